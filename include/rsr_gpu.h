@@ -1,0 +1,193 @@
+/*
+ * rsr_gpu.h -- C ABI of the B200 fitness-evaluation engine for rsr.
+ *
+ * The engine replaces rsr's CPU evaluator (src/engine/eval/evaluator.rs) behind
+ * plain pointers and sizes.  Every entry point returns an rsr_status; 0 is
+ * success and rsr_last_error() describes the last failure on the calling
+ * thread.  All host buffers are caller-owned and only read (or written, for
+ * outputs) during the call; nothing is retained unless stated.
+ *
+ * Program format (the reference's compiled Program, src/engine/expr/program.rs:18-23):
+ *   code[i]        one word per Instruction: opcode | operand << 8.  Opcodes
+ *                  follow the variant order of compose_engine!
+ *                  (src/engine/domain.rs:46-63) then BasicOpCode
+ *                  (src/domains/basic/mod.rs:9-20) then LinalgOpCode
+ *                  (src/domains/linalg/mod.rs:9-51).  The operand is the
+ *                  feature offset of LoadVar* or the constant index of
+ *                  LoadConst*.
+ *   const_kinds[c] Scalar variant of constant c (src/engine/eval/scalar.rs:4-12):
+ *                  0 Float, 1 Int, 2 Bool, 3 Vec2, 4 Vec3, 5 Mat2, 6 Mat3.
+ *   params         the flattened constants, Parameterized::flatten_params
+ *                  order (src/engine/expr/program.rs:100-145).
+ *
+ * Dataset format (src/engine/data/dataset.rs:18-34): feature_flat holds
+ * num_batches*num_features groups of 8 floats (f32x8), group b*F+f carrying
+ * feature f of points 8b..8b+7; target_batches holds num_batches groups of 8.
+ * Padded lanes are evaluated and counted, the divisor is num_samples, exactly
+ * as compute_mse does (evaluator.rs:159-173).
+ */
+#ifndef RSR_GPU_H
+#define RSR_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RSR_API __attribute__((visibility("default")))
+#else
+#define RSR_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum rsr_status {
+    RSR_OK = 0,
+    RSR_EINVAL = 1,      /* bad argument or handle */
+    RSR_EPROGRAM = 2,    /* malformed program: unknown opcode, stack underflow,
+                            more than 32 slots on a stack, index out of range */
+    RSR_ENOMEM = 3,      /* device or host allocation failed */
+    RSR_ENODEV = 4,      /* no usable sm_100 device */
+    RSR_ECUDA = 5,       /* CUDA runtime error */
+    RSR_ETIMEDOUT = 6,   /* a bounded wait expired */
+    RSR_ENOTFOUND = 7,   /* unknown dataset handle or ticket */
+    RSR_EBUSY = 8,       /* admission refused (memory budget or queue full) */
+    RSR_ECANCELED = 9    /* job cancelled or server shut down */
+} rsr_status;
+
+typedef struct rsr_ctx rsr_ctx;
+typedef uint64_t rsr_dataset;
+
+typedef struct rsr_program {
+    const uint32_t *code;
+    uint32_t len;
+    const uint8_t *const_kinds;
+    uint32_t n_consts;
+    const float *params;
+    uint32_t n_params;
+} rsr_program;
+
+/* A population packed into concatenated arrays; *_off have n_programs+1
+ * entries (element offsets). */
+typedef struct rsr_population {
+    uint32_t n_programs;
+    const uint32_t *code;
+    const uint64_t *code_off;
+    const uint8_t *const_kinds;
+    const uint64_t *kind_off;
+    const float *params;
+    const uint64_t *param_off;
+} rsr_population;
+
+/* Kernel selection for evaluation calls. */
+typedef enum rsr_kernel {
+    RSR_KERNEL_AUTO = 0,     /* register-stack batched kernel where a program fits, slot-file kernel otherwise */
+    RSR_KERNEL_PLAIN = 1,    /* slot-file interpreter, one program per warp, single launch */
+    RSR_KERNEL_BATCHED = 2   /* register-stack persistent kernel (programs that do not fit fall back to PLAIN) */
+} rsr_kernel;
+
+typedef struct rsr_options {
+    uint32_t struct_size;        /* sizeof(rsr_options) */
+    int32_t kernel;              /* rsr_kernel */
+    int32_t points_per_thread;   /* 0 = autotuned; else 1, 2, 4 or 8 */
+    int32_t programs_per_warp;   /* 0 = autotuned; else 1..8 */
+    int32_t use_graphs;          /* replay prepared batches through CUDA graphs */
+    uint64_t mem_budget_bytes;   /* 0 = 90% of free device memory at creation */
+    const char *tune_cache_path; /* autotuner cache (JSON); NULL = in memory only */
+} rsr_options;
+
+/* ------------------------------------------------------------- context */
+RSR_API void rsr_options_default(rsr_options *opts);
+RSR_API int rsr_ctx_create(int device, const rsr_options *opts, rsr_ctx **out);
+RSR_API int rsr_ctx_destroy(rsr_ctx *ctx);
+RSR_API const char *rsr_last_error(void);
+RSR_API const char *rsr_version(void);
+
+/* ------------------------------------------------------------ datasets */
+/* Upload a Dataset (dataset.rs:18-34 fields) and keep it resident.  Replaces
+ * the per-call &Dataset borrow of compute_mse (evaluator.rs:153). */
+RSR_API int rsr_dataset_upload(rsr_ctx *ctx, const float *feature_flat, const float *target_batches,
+                       uint32_t num_features, uint64_t num_batches, uint64_t num_samples, rsr_dataset *out);
+/* Same dataset given as columns: features[f*n + i], targets[i], i < n; padded
+ * to a multiple of 8 with zeros as Dataset::new does (dataset.rs:96-154). */
+RSR_API int rsr_dataset_upload_columns(rsr_ctx *ctx, const float *features, const float *targets, uint32_t num_features,
+                               uint64_t n, rsr_dataset *out);
+RSR_API int rsr_dataset_release(rsr_ctx *ctx, rsr_dataset ds);
+RSR_API int rsr_dataset_info(rsr_ctx *ctx, rsr_dataset ds, uint32_t *num_features, uint64_t *num_batches,
+                     uint64_t *num_samples);
+
+/* ------------------------------------------------- reference drop-ins */
+/* evaluator::compute_mse (src/engine/eval/evaluator.rs:153-174). */
+RSR_API int rsr_compute_mse(rsr_ctx *ctx, const rsr_program *prog, rsr_dataset ds, float *mse);
+/* evaluator::compute_mse_with_gradient (evaluator.rs:177-224): mse and
+ * grad[32], d(MSE)/d(flat parameter k) for k < min(param_count, 32), zeros
+ * elsewhere; non-finite MSE gives (f32::MAX, zeros). */
+RSR_API int rsr_compute_mse_with_gradient(rsr_ctx *ctx, const rsr_program *prog, rsr_dataset ds, float *mse, float *grad);
+/* evaluator::eval_simd (evaluator.rs:20-150) applied to every batch of the
+ * dataset: out[num_batches*8] predictions, padded lanes included. */
+RSR_API int rsr_eval_points(rsr_ctx *ctx, const rsr_program *prog, rsr_dataset ds, float *out);
+
+/* ------------------------------------------------------------- batched */
+/* compute_mse for a whole population against one dataset (ds_per_program
+ * NULL) or against ds_per_program[i]. */
+RSR_API int rsr_eval_mse_batch(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const rsr_dataset *ds_per_program,
+                       int kernel, float *mse_out);
+/* compute_mse_with_gradient for a population: mse_out[n], grad_out[n*32]. */
+RSR_API int rsr_eval_mse_grad_batch(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds,
+                            const rsr_dataset *ds_per_program, float *mse_out, float *grad_out);
+/* eval_simd over every batch for each program: out[i*num_batches*8 + j]. */
+RSR_API int rsr_eval_points_batch(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, int kernel, float *out);
+
+/* -------------------------------------------------- prepared batches */
+/* A population encoded and uploaded once, then run many times with inputs
+ * resident on the device (the timed unit of the benchmark).  run() enqueues
+ * the kernels on the context's stream (graph replay when enabled) and
+ * returns without waiting; results() waits and copies mse back. */
+typedef struct rsr_batch rsr_batch;
+RSR_API int rsr_batch_prepare(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const rsr_dataset *ds_per_program,
+                      int kernel, int with_gradient, rsr_batch **out);
+RSR_API int rsr_batch_run(rsr_ctx *ctx, rsr_batch *b);
+RSR_API int rsr_batch_results(rsr_ctx *ctx, rsr_batch *b, float *mse_out, float *grad_out);
+/* Device time in milliseconds of the last run's kernels (CUDA events on the
+ * launching stream), split into the evaluation kernels and the finalize. */
+RSR_API int rsr_batch_last_timing(rsr_ctx *ctx, rsr_batch *b, float *eval_ms, float *total_ms);
+/* Describes the prepared launch: kernel names used, points per thread,
+ * programs per warp, number of work items, programs on the fallback path. */
+RSR_API int rsr_batch_describe(rsr_ctx *ctx, rsr_batch *b, char *buf, size_t buf_len);
+RSR_API int rsr_batch_destroy(rsr_ctx *ctx, rsr_batch *b);
+
+/* Number of this library's kernel launches issued on the context since
+ * creation (device-side work the host enqueued). */
+RSR_API uint64_t rsr_ctx_launch_count(rsr_ctx *ctx);
+/* Bytes copied host->device and device->host by the last evaluation call. */
+RSR_API int rsr_ctx_last_transfer(rsr_ctx *ctx, uint64_t *h2d_bytes, uint64_t *d2h_bytes);
+/* Write bytes of zeros over a device scratch buffer larger than L2. */
+RSR_API int rsr_flush_l2(rsr_ctx *ctx);
+RSR_API int rsr_synchronize(rsr_ctx *ctx);
+/* Measured FP32 throughput of this device in unfused lane-operations per
+ * second (independent multiply and add chains): the roofline denominator of
+ * the interpreter kernels. */
+RSR_API int rsr_measure_fp32_peak(rsr_ctx *ctx, double *lane_ops_per_s);
+
+/* ------------------------------------------------------ host encoder */
+/* Validation against a feature count (0 = skip feature-range checks); does
+ * not touch the device.  Returns RSR_OK or RSR_EPROGRAM. */
+RSR_API int rsr_validate_program(const rsr_program *prog, uint32_t num_features);
+/* Analysis summary used by the tests: max depth per typed stack
+ * (F, V2, V3, M2, M3) in the reference's own evaluation order and after
+ * reordering, and whether the register-stack kernel accepts the program. */
+typedef struct rsr_program_info {
+    uint32_t depth_ref[5];
+    uint32_t depth_fast[5];
+    uint32_t n_uops_fast;
+    uint32_t n_uops_plain;
+    int32_t fast_profile;        /* -1 when only the slot-file kernel applies */
+    uint32_t flops_per_point;    /* algorithmic FP32 lane-ops incl. the MSE epilogue */
+} rsr_program_info;
+RSR_API int rsr_program_analyze(const rsr_program *prog, uint32_t num_features, rsr_program_info *info);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RSR_GPU_H */

@@ -1,0 +1,56 @@
+// encoder.h -- host-side analysis of reference programs and emission of the
+// two device encodings described in uops.h.
+#pragma once
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "uops.h"
+
+namespace rsr {
+
+// Static properties of each reference opcode: operand stacks in
+// expected_types order (basic/mod.rs:209-217, linalg/mod.rs:375-432) and the
+// result stack (-1: none).
+struct OpSig {
+    int n_in;
+    int in[3];
+    int out;
+    int flops;  // unfused FP32 lane-ops
+};
+const OpSig &op_sig(int opcode);
+int load_stack(int opcode);       // stack a LoadVar*/LoadConst* pushes to, -1 for B/I loads
+bool is_load(int opcode);
+bool is_const_load(int opcode);
+int kind_width(int kind);         // flat params per Scalar variant (program.rs:84-98)
+int const_kind_for_load(int opcode);
+
+struct EncodedProgram {
+    // common
+    uint32_t n_params = 0;
+    std::vector<float> consts;            // flat parameters (kernel constant pool)
+    uint32_t flops_per_point = 0;         // incl. MSE epilogue
+    bool differentiable = true;
+    bool result_zero = false;             // stack_f[0] is never written
+    int depth_ref[N_STACKS] = {0, 0, 0, 0, 0};
+    // slot form
+    std::vector<uint32_t> slot_code;      // 3 words per instruction
+    uint32_t n_slots = 0;
+    bool needs_zero_init = false;
+    // register form
+    int profile = -1;                     // -1: register kernel not applicable
+    int depth_fast[N_STACKS] = {0, 0, 0, 0, 0};
+    std::vector<uint32_t> reg_code;
+    // adjoint (slot form with one slot range per value, never reused)
+    std::vector<uint32_t> tape_code;      // 3 words per instruction, SSA slots
+    uint32_t n_tape_slots = 0;
+};
+
+// Validates and encodes.  num_features == 0 skips feature-range checks.
+// Returns 0 or an rsr_status code, with a message in *err.
+int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uint32_t n_consts,
+                   const float *params, uint32_t n_params, uint32_t num_features, EncodedProgram *out,
+                   std::string *err);
+
+}  // namespace rsr

@@ -1,0 +1,34 @@
+// kernels.h -- host-callable launchers of the device kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "kernels_common.cuh"
+
+namespace rsr {
+
+constexpr int kPlainThreads = 128;  // 4 warps per block, one work item per warp
+constexpr int kRegThreads = 128;
+constexpr int kGradThreads = 64;
+
+cudaError_t launch_plain(const LaunchArgs &a, int P, uint32_t warps_per_block, size_t smem, cudaStream_t st);
+size_t plain_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t slots, int P);
+cudaError_t launch_aosoa_to_soa(const float *ff, const float *tb, float *x, float *y, uint32_t nf, uint64_t nbatch,
+                                uint64_t stride, int num_sms, cudaStream_t st);
+cudaError_t measure_fp32_peak(int num_sms, cudaStream_t st, double *lane_ops_per_s);
+cudaError_t launch_finalize_mse(const ProgDesc *progs, const DatasetDesc *ds, const double *partials, uint32_t n,
+                                float *out, cudaStream_t st);
+
+// register-stack kernel (kernels_reg.cu)
+cudaError_t launch_reg(const LaunchArgs &a, int profile, int P, uint32_t grid, cudaStream_t st);
+size_t reg_smem_per_warp(uint32_t code_words, uint32_t const_floats);
+int reg_max_blocks_per_sm(int profile, int P);
+
+// adjoint kernel (kernels_grad.cu)
+cudaError_t launch_grad(const LaunchArgs &a, uint32_t warps_per_block, size_t smem, cudaStream_t st);
+size_t grad_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t tape_slots);
+cudaError_t launch_finalize_grad(const ProgDesc *progs, const DatasetDesc *ds, const double *partials, uint32_t n,
+                                 float *mse_out, float *grad_out, cudaStream_t st);
+
+}  // namespace rsr

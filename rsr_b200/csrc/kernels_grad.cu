@@ -1,0 +1,418 @@
+// kernels_grad.cu -- reverse-mode adjoint kernel: MSE and d(MSE)/d(constants)
+// of a program in one forward and one reverse sweep per tile of points.
+//
+// Replaces compute_mse_with_gradient (src/engine/eval/evaluator.rs:177-224),
+// which runs one dual-number forward pass per flat parameter
+// (eval_simd_dual, evaluator.rs:228-388).  The tape is the program's SSA slot
+// file (every live value has its own slots) in shared memory, recorded for
+// one tile of 32*P points and consumed by the reverse sweep right away: the
+// whole population x points x length tape is never stored, it is recomputed
+// tile by tile.
+//
+// Reverse rules follow the forward rules of src/engine/eval/autodiff.rs; for
+// InverseM2/M3, whose dual dispatch is a no-op in the reference
+// (src/domains/linalg/mod.rs:643,687), the adjoint is the exact one,
+// dA = -A^-T G A^-T, and zero on the singular branch (|det| < 1e-9), whose
+// value is a constant identity.
+#include <cuda_runtime.h>
+#include <float.h>
+
+#include "kernels.h"
+#include "kernels_common.cuh"
+
+namespace rsr {
+
+__host__ __device__ __forceinline__ uint32_t align4g(uint32_t v) { return (v + 3u) & ~3u; }
+constexpr uint32_t kGradParams = 32;
+
+template <int P>
+struct TapeCtx {
+    Vf<P> *val;   // [slot][lane]
+    Vf<P> *adj;   // [slot][lane]
+    const float *consts;
+    const float *x;
+    uint64_t stride, p0;
+    int lane;
+    __device__ __forceinline__ Vf<P> V(uint32_t s) const { return val[s * 32 + lane]; }
+    __device__ __forceinline__ void SV(uint32_t s, const Vf<P> &v) const { val[s * 32 + lane] = v; }
+    __device__ __forceinline__ Vf<P> A(uint32_t s) const { return adj[s * 32 + lane]; }
+    __device__ __forceinline__ void AddA(uint32_t s, const Vf<P> &v) const {
+        Vf<P> &r = adj[s * 32 + lane];
+        r = r + v;
+    }
+    __device__ __forceinline__ Vf<P> X(uint32_t f) const { return load_pts<P>(x + f * stride + p0); }
+};
+
+// Forward value of one tape instruction (same semantics as the slot kernel).
+template <int P>
+__device__ __forceinline__ void tape_forward(const TapeCtx<P> &t, uint32_t w0, uint32_t w1, uint32_t w2) {
+    const uint32_t op = w0 & 0xFFu, aux = w0 >> 8;
+    const uint32_t o = w1 & 0xFFFFu, i0 = w1 >> 16, i1 = w2 & 0xFFFFu, i2 = w2 >> 16;
+    Vf<P> A[9], B[9], R[9];
+    auto Ln = [&](Vf<P> *d, uint32_t s, int n) { for (int i = 0; i < n; ++i) d[i] = t.V(s + i); };
+    auto Sn = [&](uint32_t s, const Vf<P> *v, int n) { for (int i = 0; i < n; ++i) t.SV(s + i, v[i]); };
+    switch (op) {
+        case SLOT_NOP: {  // stale constant slot: copy of the aliased value, or zero
+            const uint32_t w = aux >> 1;
+            for (uint32_t i = 0; i < w; ++i) t.SV(o + i, (aux & 1u) ? t.V(i0 + i) : splat<P>(0.0f));
+            break;
+        }
+        case LOAD_VAR_F: t.SV(o, t.X(aux)); break;
+        case LOAD_VAR_V2: for (int i = 0; i < 2; ++i) t.SV(o + i, t.X(aux + i)); break;
+        case LOAD_VAR_V3: for (int i = 0; i < 3; ++i) t.SV(o + i, t.X(aux + i)); break;
+        case LOAD_VAR_M2: for (int i = 0; i < 4; ++i) t.SV(o + i, t.X(aux + i)); break;
+        case LOAD_VAR_M3: for (int i = 0; i < 9; ++i) t.SV(o + i, t.X(aux + i)); break;
+        case LOAD_CONST_F: t.SV(o, splat<P>(t.consts[aux])); break;
+        case LOAD_CONST_V2: for (int i = 0; i < 2; ++i) t.SV(o + i, splat<P>(t.consts[aux + i])); break;
+        case LOAD_CONST_V3: for (int i = 0; i < 3; ++i) t.SV(o + i, splat<P>(t.consts[aux + i])); break;
+        case LOAD_CONST_M2: for (int i = 0; i < 4; ++i) t.SV(o + i, splat<P>(t.consts[aux + i])); break;
+        case LOAD_CONST_M3: for (int i = 0; i < 9; ++i) t.SV(o + i, splat<P>(t.consts[aux + i])); break;
+        case ADD_F: t.SV(o, t.V(i0) + t.V(i1)); break;
+        case SUB_F: t.SV(o, t.V(i0) - t.V(i1)); break;
+        case MUL_F: t.SV(o, t.V(i0) * t.V(i1)); break;
+        case DIV_F: t.SV(o, t.V(i0) / t.V(i1)); break;
+        case SIN_F: t.SV(o, vsin(t.V(i0))); break;
+        case COS_F: t.SV(o, vcos(t.V(i0))); break;
+        case EXP_F: t.SV(o, vexp(t.V(i0))); break;
+        case SQR_F: { Vf<P> a = t.V(i0); t.SV(o, a * a); break; }
+        case SQRT_F: t.SV(o, vsqrt(t.V(i0))); break;
+        case LN_F: t.SV(o, vlog(t.V(i0))); break;
+        case MAKE_VEC2: A[0] = t.V(i0); A[1] = t.V(i1); Sn(o, A, 2); break;
+        case MAKE_VEC3: A[0] = t.V(i0); A[1] = t.V(i1); A[2] = t.V(i2); Sn(o, A, 3); break;
+        case GET_X_V2: case GET_X_V3: t.SV(o, t.V(i0)); break;
+        case GET_Y_V2: case GET_Y_V3: t.SV(o, t.V(i0 + 1)); break;
+        case GET_Z_V3: t.SV(o, t.V(i0 + 2)); break;
+        case ADD_V2: case ADD_V3: case ADD_M2: case ADD_M3: {
+            const int w = op == ADD_V2 ? 2 : op == ADD_V3 ? 3 : op == ADD_M2 ? 4 : 9;
+            Ln(A, i0, w); Ln(B, i1, w); for (int i = 0; i < w; ++i) R[i] = A[i] + B[i]; Sn(o, R, w); break;
+        }
+        case SUB_V2: case SUB_V3: case SUB_M2: case SUB_M3: {
+            const int w = op == SUB_V2 ? 2 : op == SUB_V3 ? 3 : op == SUB_M2 ? 4 : 9;
+            Ln(A, i0, w); Ln(B, i1, w); for (int i = 0; i < w; ++i) R[i] = A[i] - B[i]; Sn(o, R, w); break;
+        }
+        case SCALE_V2: case SCALE_V3: case SCALE_M2: case SCALE_M3: {
+            const int w = op == SCALE_V2 ? 2 : op == SCALE_V3 ? 3 : op == SCALE_M2 ? 4 : 9;
+            const Vf<P> s = t.V(i0);
+            Ln(A, i1, w); for (int i = 0; i < w; ++i) R[i] = A[i] * s; Sn(o, R, w); break;
+        }
+        case DOT_V2: Ln(A, i0, 2); Ln(B, i1, 2); t.SV(o, dot2(A, B)); break;
+        case DOT_V3: Ln(A, i0, 3); Ln(B, i1, 3); t.SV(o, dot3(A, B)); break;
+        case NORM_V2: Ln(A, i0, 2); t.SV(o, norm2(A)); break;
+        case NORM_V3: Ln(A, i0, 3); t.SV(o, norm3(A)); break;
+        case CROSS_V3: Ln(A, i0, 3); Ln(B, i1, 3); cross3(A, B, R); Sn(o, R, 3); break;
+        case MAKE_MAT2: Ln(A, i0, 2); Ln(A + 2, i1, 2); Sn(o, A, 4); break;
+        case MUL_M2: Ln(A, i0, 4); Ln(B, i1, 4); mul_m2(A, B, R); Sn(o, R, 4); break;
+        case MUL_M2V2: Ln(A, i0, 4); Ln(B, i1, 2); mul_m2v2(A, B, R); Sn(o, R, 2); break;
+        case DET_M2: Ln(A, i0, 4); t.SV(o, det_m2(A)); break;
+        case TRACE_M2: Ln(A, i0, 4); t.SV(o, trace_m2(A)); break;
+        case TRANSPOSE_M2: Ln(A, i0, 4); transpose_m2(A, R); Sn(o, R, 4); break;
+        case INVERSE_M2: Ln(A, i0, 4); inverse_m2(A, R); Sn(o, R, 4); break;
+        case MAKE_MAT3: Ln(A, i0, 3); Ln(A + 3, i1, 3); Ln(A + 6, i2, 3); Sn(o, A, 9); break;
+        case MUL_M3: Ln(A, i0, 9); Ln(B, i1, 9); mul_m3(A, B, R); Sn(o, R, 9); break;
+        case MUL_M3V3: Ln(A, i0, 9); Ln(B, i1, 3); mul_m3v3(A, B, R); Sn(o, R, 3); break;
+        case DET_M3: Ln(A, i0, 9); t.SV(o, det_m3(A)); break;
+        case TRACE_M3: Ln(A, i0, 9); t.SV(o, trace_m3(A)); break;
+        case TRANSPOSE_M3: Ln(A, i0, 9); transpose_m3(A, R); Sn(o, R, 9); break;
+        case INVERSE_M3: Ln(A, i0, 9); inverse_m3(A, R); Sn(o, R, 9); break;
+        default: break;
+    }
+}
+
+// dA = -O^T G O^T for O = A^-1 (N x N, column-major), zero where singular.
+template <int P, int N>
+__device__ __forceinline__ void inverse_adjoint(const TapeCtx<P> &t, uint32_t o, uint32_t i0) {
+    Vf<P> O[N * N], G[N * N], H[N * N], M[N * N];
+    for (int i = 0; i < N * N; ++i) { O[i] = t.V(o + i); G[i] = t.A(o + i); M[i] = t.V(i0 + i); }
+    Vf<P> det;
+    if constexpr (N == 2) det = det_m2(M); else det = det_m3(M);
+    // H = O^T G : H(i,l) = sum_k O(k,i) G(k,l)
+    for (int i = 0; i < N; ++i)
+        for (int l = 0; l < N; ++l) {
+            Vf<P> s = splat<P>(0.0f);
+            for (int k = 0; k < N; ++k) s = s + O[N * i + k] * G[N * l + k];
+            H[N * l + i] = s;
+        }
+    // dA(i,j) = -sum_l H(i,l) O(j,l)
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j) {
+            Vf<P> s = splat<P>(0.0f);
+            for (int l = 0; l < N; ++l) s = s + H[N * l + i] * O[N * l + j];
+            Vf<P> d;
+#pragma unroll
+            for (int k = 0; k < P; ++k) d.v[k] = fabsf(det.v[k]) < 1e-9f ? 0.0f : -s.v[k];
+            t.AddA(i0 + N * j + i, d);
+        }
+}
+
+// Reverse sweep of one tape instruction.  gacc: this lane's f32 gradient
+// contributions of the tile (summed over its P points).
+template <int P>
+__device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, uint32_t w0, uint32_t w1, uint32_t w2,
+                                             float *gacc_lane) {
+    const uint32_t op = w0 & 0xFFu, aux = w0 >> 8;
+    const uint32_t o = w1 & 0xFFFFu, i0 = w1 >> 16, i1 = w2 & 0xFFFFu, i2 = w2 >> 16;
+    switch (op) {
+        case SLOT_NOP:
+            if (aux & 1u) for (uint32_t i = 0; i < (aux >> 1); ++i) t.AddA(i0 + i, t.A(o + i));
+            break;
+        case LOAD_VAR_F: case LOAD_VAR_V2: case LOAD_VAR_V3: case LOAD_VAR_M2: case LOAD_VAR_M3: break;
+        case LOAD_CONST_F: case LOAD_CONST_V2: case LOAD_CONST_V3: case LOAD_CONST_M2: case LOAD_CONST_M3: {
+            const int w = op == LOAD_CONST_F ? 1 : op == LOAD_CONST_V2 ? 2 : op == LOAD_CONST_V3 ? 3
+                        : op == LOAD_CONST_M2 ? 4 : 9;
+            for (int i = 0; i < w; ++i) {
+                if (aux + i >= kGradParams) break;
+                const Vf<P> g = t.A(o + i);
+                float s = 0.0f;
+#pragma unroll
+                for (int k = 0; k < P; ++k) s = s + g.v[k];
+                gacc_lane[(aux + i) * 32] += s;
+            }
+            break;
+        }
+        case ADD_F: { const Vf<P> g = t.A(o); t.AddA(i0, g); t.AddA(i1, g); break; }
+        case SUB_F: { const Vf<P> g = t.A(o); t.AddA(i0, g); t.AddA(i1, -g); break; }
+        case MUL_F: { const Vf<P> g = t.A(o); t.AddA(i0, g * t.V(i1)); t.AddA(i1, g * t.V(i0)); break; }
+        case DIV_F: {
+            const Vf<P> q = t.A(o) / t.V(i1);
+            t.AddA(i0, q);
+            t.AddA(i1, -(q * t.V(o)));
+            break;
+        }
+        case SIN_F: t.AddA(i0, t.A(o) * vcos(t.V(i0))); break;
+        case COS_F: t.AddA(i0, t.A(o) * (-vsin(t.V(i0)))); break;
+        case EXP_F: t.AddA(i0, t.A(o) * t.V(o)); break;
+        case SQR_F: t.AddA(i0, t.A(o) * (splat<P>(2.0f) * t.V(i0))); break;
+        case SQRT_F: t.AddA(i0, t.A(o) / (splat<P>(2.0f) * t.V(o))); break;
+        case LN_F: t.AddA(i0, t.A(o) / t.V(i0)); break;
+        case MAKE_VEC2: t.AddA(i0, t.A(o)); t.AddA(i1, t.A(o + 1)); break;
+        case MAKE_VEC3: t.AddA(i0, t.A(o)); t.AddA(i1, t.A(o + 1)); t.AddA(i2, t.A(o + 2)); break;
+        case GET_X_V2: case GET_X_V3: t.AddA(i0, t.A(o)); break;
+        case GET_Y_V2: case GET_Y_V3: t.AddA(i0 + 1, t.A(o)); break;
+        case GET_Z_V3: t.AddA(i0 + 2, t.A(o)); break;
+        case ADD_V2: case ADD_V3: case ADD_M2: case ADD_M3: case SUB_V2: case SUB_V3: case SUB_M2: case SUB_M3: {
+            const bool sub = op == SUB_V2 || op == SUB_V3 || op == SUB_M2 || op == SUB_M3;
+            const int w = (op == ADD_V2 || op == SUB_V2) ? 2 : (op == ADD_V3 || op == SUB_V3) ? 3
+                        : (op == ADD_M2 || op == SUB_M2) ? 4 : 9;
+            for (int i = 0; i < w; ++i) {
+                const Vf<P> g = t.A(o + i);
+                t.AddA(i0 + i, g);
+                t.AddA(i1 + i, sub ? -g : g);
+            }
+            break;
+        }
+        case SCALE_V2: case SCALE_V3: case SCALE_M2: case SCALE_M3: {
+            const int w = op == SCALE_V2 ? 2 : op == SCALE_V3 ? 3 : op == SCALE_M2 ? 4 : 9;
+            const Vf<P> s = t.V(i0);
+            Vf<P> ds = splat<P>(0.0f);
+            for (int i = 0; i < w; ++i) {
+                const Vf<P> g = t.A(o + i);
+                ds = ds + g * t.V(i1 + i);
+                t.AddA(i1 + i, g * s);
+            }
+            t.AddA(i0, ds);
+            break;
+        }
+        case DOT_V2: case DOT_V3: {
+            const int w = op == DOT_V2 ? 2 : 3;
+            const Vf<P> g = t.A(o);
+            for (int i = 0; i < w; ++i) {
+                const Vf<P> a = t.V(i0 + i), b = t.V(i1 + i);
+                t.AddA(i0 + i, g * b);
+                t.AddA(i1 + i, g * a);
+            }
+            break;
+        }
+        case NORM_V2: case NORM_V3: {
+            const int w = op == NORM_V2 ? 2 : 3;
+            const Vf<P> q = t.A(o) / t.V(o);
+            for (int i = 0; i < w; ++i) t.AddA(i0 + i, q * t.V(i0 + i));
+            break;
+        }
+        case CROSS_V3: {  // o = a x b: da += b x g, db += g x a
+            Vf<P> a[3], b[3], g[3], da[3], db[3];
+            for (int i = 0; i < 3; ++i) { a[i] = t.V(i0 + i); b[i] = t.V(i1 + i); g[i] = t.A(o + i); }
+            cross3(b, g, da);
+            cross3(g, a, db);
+            for (int i = 0; i < 3; ++i) { t.AddA(i0 + i, da[i]); t.AddA(i1 + i, db[i]); }
+            break;
+        }
+        case MAKE_MAT2:
+            t.AddA(i0, t.A(o)); t.AddA(i0 + 1, t.A(o + 1)); t.AddA(i1, t.A(o + 2)); t.AddA(i1 + 1, t.A(o + 3));
+            break;
+        case MAKE_MAT3:
+            for (int i = 0; i < 3; ++i) { t.AddA(i0 + i, t.A(o + i)); t.AddA(i1 + i, t.A(o + 3 + i)); t.AddA(i2 + i, t.A(o + 6 + i)); }
+            break;
+        case MUL_M2: case MUL_M3: {  // O = A B: dA = G B^T, dB = A^T G
+            const int N = op == MUL_M2 ? 2 : 3;
+            Vf<P> Am[9], Bm[9], G[9];
+            for (int i = 0; i < N * N; ++i) { Am[i] = t.V(i0 + i); Bm[i] = t.V(i1 + i); G[i] = t.A(o + i); }
+            for (int r = 0; r < N; ++r)
+                for (int c = 0; c < N; ++c) {
+                    Vf<P> da = splat<P>(0.0f), db = splat<P>(0.0f);
+                    for (int j = 0; j < N; ++j) {
+                        da = da + G[N * j + r] * Bm[N * j + c];   // G(r,j) B(c,j)
+                        db = db + Am[N * r + j] * G[N * c + j];   // A(j,r) G(j,c)
+                    }
+                    t.AddA(i0 + N * c + r, da);
+                    t.AddA(i1 + N * c + r, db);
+                }
+            break;
+        }
+        case MUL_M2V2: case MUL_M3V3: {  // o = M v: dM(r,c) += g_r v_c, dv_c += sum_r M(r,c) g_r
+            const int N = op == MUL_M2V2 ? 2 : 3;
+            Vf<P> g[3], v[3];
+            for (int i = 0; i < N; ++i) { g[i] = t.A(o + i); v[i] = t.V(i1 + i); }
+            for (int c = 0; c < N; ++c) {
+                Vf<P> dv = splat<P>(0.0f);
+                for (int r = 0; r < N; ++r) {
+                    t.AddA(i0 + N * c + r, g[r] * v[c]);
+                    dv = dv + t.V(i0 + N * c + r) * g[r];
+                }
+                t.AddA(i1 + c, dv);
+            }
+            break;
+        }
+        case DET_M2: {
+            const Vf<P> g = t.A(o);
+            t.AddA(i0, g * t.V(i0 + 3));
+            t.AddA(i0 + 3, g * t.V(i0));
+            t.AddA(i0 + 1, -(g * t.V(i0 + 2)));
+            t.AddA(i0 + 2, -(g * t.V(i0 + 1)));
+            break;
+        }
+        case DET_M3: {  // d det / d m(r,c) = cofactor C(r,c)
+            const Vf<P> g = t.A(o);
+            Vf<P> m[9];
+            for (int i = 0; i < 9; ++i) m[i] = t.V(i0 + i);
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) {
+                    const int r1 = (r + 1) % 3, r2 = (r + 2) % 3, c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+                    const Vf<P> cof = m[3 * c1 + r1] * m[3 * c2 + r2] - m[3 * c2 + r1] * m[3 * c1 + r2];
+                    t.AddA(i0 + 3 * c + r, g * cof);
+                }
+            break;
+        }
+        case TRACE_M2: { const Vf<P> g = t.A(o); t.AddA(i0, g); t.AddA(i0 + 3, g); break; }
+        case TRACE_M3: { const Vf<P> g = t.A(o); t.AddA(i0, g); t.AddA(i0 + 4, g); t.AddA(i0 + 8, g); break; }
+        case TRANSPOSE_M2: case TRANSPOSE_M3: {
+            const int N = op == TRANSPOSE_M2 ? 2 : 3;
+            for (int r = 0; r < N; ++r)
+                for (int c = 0; c < N; ++c) t.AddA(i0 + N * r + c, t.A(o + N * c + r));
+            break;
+        }
+        case INVERSE_M2: inverse_adjoint<P, 2>(t, o, i0); break;
+        case INVERSE_M3: inverse_adjoint<P, 3>(t, o, i0); break;
+        default: break;
+    }
+}
+
+template <int P>
+__global__ void __launch_bounds__(kGradThreads) grad_kernel(const LaunchArgs a) {
+    extern __shared__ __align__(16) float smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t item_id = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (item_id >= a.n_items) return;
+    const uint32_t cw = align4g(a.smem_code_words), cf = align4g(a.smem_const_floats);
+    const uint32_t region = cw + cf + kGradParams * 32u + 2u * a.smem_slots * 32u * P;
+    float *base = smem + (size_t)warp * region;
+    uint32_t *scode = reinterpret_cast<uint32_t *>(base);
+    float *sconst = base + cw;
+    float *gacc = sconst + cf;  // [param][lane] f32, per tile
+    Vf<P> *val = reinterpret_cast<Vf<P> *>(gacc + kGradParams * 32u);
+    Vf<P> *adj = val + (size_t)a.smem_slots * 32u;
+
+    const WorkItem it = a.items[item_id];
+    const ProgDesc pd = a.progs[it.prog_begin];
+    const DatasetDesc ds = a.datasets[pd.dataset];
+    for (uint32_t i = lane; i < pd.uop_len; i += 32) scode[i] = __ldg(a.code + pd.uop_off + i);
+    for (uint32_t i = lane; i < pd.n_consts; i += 32) sconst[i] = __ldg(a.consts + pd.const_off + i);
+    __syncwarp();
+    const uint32_t result = scode[0];
+    const uint32_t *code = scode + 1;
+    const uint32_t n_nodes = (pd.uop_len - 1) / 3;
+    TapeCtx<P> t{val, adj, sconst, ds.x, ds.stride, 0, lane};
+    Kahan sse;
+    double gsum[kGradParams];
+#pragma unroll
+    for (int k = 0; k < (int)kGradParams; ++k) gsum[k] = 0.0;
+    const uint32_t np = min(pd.n_consts, kGradParams);
+    for (uint32_t tile = it.tile_begin; tile < it.tile_end; ++tile) {
+        t.p0 = (uint64_t)tile * (32u * P) + (uint64_t)lane * P;
+        for (uint32_t k = 0; k < np; ++k) gacc[k * 32 + lane] = 0.0f;
+        // forward sweep, adjoints cleared on the way
+        for (uint32_t i = 0; i < n_nodes; ++i) tape_forward<P>(t, code[3 * i], code[3 * i + 1], code[3 * i + 2]);
+        for (uint32_t s = 0; s < pd.n_tape; ++s) adj[s * 32 + lane] = splat<P>(0.0f);
+        const Vf<P> pred = result == 0xFFFFFFFFu ? splat<P>(0.0f) : t.V(result);
+        const Vf<P> y = load_pts<P>(ds.y + t.p0);
+        Vf<P> seed;
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            const bool valid = t.p0 + k < ds.n_eval;
+            const float d = pred.v[k] - y.v[k];
+            if (valid) sse.add(d * d);
+            seed.v[k] = valid ? 2.0f * d : 0.0f;  // d(diff^2)/d pred, as in evaluator.rs:207
+        }
+        if (result == 0xFFFFFFFFu) continue;
+        t.AddA(result, seed);
+        // reverse sweep
+        for (uint32_t i = n_nodes; i-- > 0;)
+            tape_reverse<P>(t, code[3 * i], code[3 * i + 1], code[3 * i + 2], gacc + lane);
+#pragma unroll
+        for (int k = 0; k < (int)kGradParams; ++k)
+            if ((uint32_t)k < np) gsum[k] += (double)gacc[k * 32 + lane];
+    }
+    double *out = a.partials + (size_t)(pd.part_off + it.chunk) * (1 + kGradParams);
+    const double s = warp_sum(sse.value());
+    if (lane == 0) out[0] = s;
+#pragma unroll
+    for (int k = 0; k < (int)kGradParams; ++k) {
+        const double g = warp_sum(gsum[k]);
+        if (lane == 0) out[1 + k] = g;
+    }
+}
+
+// compute_mse_with_gradient epilogue (evaluator.rs:211-223).
+__global__ void finalize_grad_kernel(const ProgDesc *progs, const DatasetDesc *datasets, const double *partials,
+                                     uint32_t n_progs, float *mse_out, float *grad_out) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n_progs) return;
+    const ProgDesc pd = progs[p];
+    const double n = (double)datasets[pd.dataset].num_samples;
+    double s = 0.0, g[kGradParams];
+    for (int k = 0; k < (int)kGradParams; ++k) g[k] = 0.0;
+    for (uint32_t c = 0; c < pd.n_parts; ++c) {
+        const double *q = partials + (size_t)(pd.part_off + c) * (1 + kGradParams);
+        s += q[0];
+        for (int k = 0; k < (int)kGradParams; ++k) g[k] += q[1 + k];
+    }
+    float m = (float)(s / n);
+    const bool bad = !(s <= (double)FLT_MAX) || !isfinite(m);
+    mse_out[p] = bad ? FLT_MAX : m;
+    const uint32_t np = min(pd.n_consts, kGradParams);
+    for (uint32_t k = 0; k < kGradParams; ++k) grad_out[(size_t)p * kGradParams + k] = (bad || k >= np) ? 0.0f : (float)(g[k] / n);
+}
+
+template <int P>
+static cudaError_t launch_grad_p(const LaunchArgs &a, uint32_t wpb, size_t smem, cudaStream_t st) {
+    auto k = grad_kernel<P>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k<<<(a.n_items + wpb - 1) / wpb, wpb * 32, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grad(const LaunchArgs &a, uint32_t wpb, size_t smem, cudaStream_t st) {
+    return a.progs_per_warp >= 2 ? launch_grad_p<2>(a, wpb, smem, st) : launch_grad_p<1>(a, wpb, smem, st);
+}
+
+size_t grad_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t tape_slots) {
+    return ((size_t)align4g(code_words) + align4g(const_floats) + kGradParams * 32u + 2u * (size_t)tape_slots * 32u) * 4u;
+}
+
+cudaError_t launch_finalize_grad(const ProgDesc *progs, const DatasetDesc *ds, const double *partials, uint32_t n,
+                                 float *mse_out, float *grad_out, cudaStream_t st) {
+    finalize_grad_kernel<<<(n + 127) / 128, 128, 0, st>>>(progs, ds, partials, n, mse_out, grad_out);
+    return cudaGetLastError();
+}
+
+}  // namespace rsr

@@ -1,0 +1,844 @@
+// runtime.cu -- contexts, resident datasets, launch planning and the C ABI
+// entry points of include/rsr_gpu.h.
+#include <cuda_runtime.h>
+#include <float.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "runtime.h"
+
+namespace rsr {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+int fail(int code, const std::string &msg) {
+    set_error(msg);
+    return code;
+}
+int cuda_fail(cudaError_t e, const char *what) {
+    return fail(e == cudaErrorMemoryAllocation ? RSR_ENOMEM : RSR_ECUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+cudaError_t DevBuf::reserve(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    release();
+    size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        cap = 0;
+        return e;
+    }
+    cap = want;
+    return cudaSuccess;
+}
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+}
+
+static constexpr uint64_t kChunkPoints = 4096;   // points per work-item chunk (all P)
+static constexpr uint64_t kStrideAlign = 1024;   // dataset column padding
+static constexpr int kGradSlotDoubles = 33;      // sse + 32 gradient sums
+
+static uint64_t round_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
+static int log2_bucket(uint64_t n) {
+    int b = 0;
+    while ((1ull << (b + 1)) <= n) ++b;
+    return b;
+}
+
+// Default launch shape of the register kernel per profile: points per
+// thread and programs per warp.
+static TuneChoice default_choice(int profile) {
+    switch (profile) {
+        case P_F: return {4, 4};
+        case P_FV3: return {2, 4};
+        case P_FV2M2: return {2, 4};
+        case P_FV3M3: return {1, 4};
+        default: return {1, 4};
+    }
+}
+
+static TuneChoice choice_for(rsr_ctx *ctx, int profile, uint64_t n_eval) {
+    TuneChoice c = default_choice(profile);
+    auto it = ctx->tune.find({profile, log2_bucket(n_eval)});
+    if (it != ctx->tune.end()) c = it->second;
+    if (ctx->opts.points_per_thread > 0) c.P = ctx->opts.points_per_thread;
+    if (ctx->opts.programs_per_warp > 0) c.G = ctx->opts.programs_per_warp;
+    // variants that exist (kernels_reg.cu)
+    int maxP = profile == P_F ? 8 : (profile == P_FV3M3 || profile == P_ALL) ? 2 : 4;
+    if (c.P > maxP) c.P = maxP;
+    if (c.P != 1 && c.P != 2 && c.P != 4 && c.P != 8) c.P = 1;
+    c.G = std::max(1, std::min(c.G, 8));
+    return c;
+}
+
+static uint32_t align4h(uint32_t v) { return (v + 3u) & ~3u; }
+
+int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_prog, uint64_t ds_all, int kernel,
+               bool gradient, int mode, Plan *plan) {
+    Plan &P = *plan;
+    P = Plan();
+    P.gradient = gradient;
+    P.mode = mode;
+    const uint32_t n = pop.n_programs;
+    if (n == 0) return RSR_OK;
+    if (!pop.code_off || !pop.kind_off || !pop.param_off) return fail(RSR_EINVAL, "population offsets are null");
+    // datasets
+    std::map<uint64_t, uint32_t> ds_index;
+    std::vector<uint32_t> prog_ds(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        uint64_t h = ds_per_prog ? ds_per_prog[i] : ds_all;
+        auto f = ds_index.find(h);
+        if (f == ds_index.end()) {
+            auto it = ctx->datasets.find(h);
+            if (it == ctx->datasets.end()) return fail(RSR_ENOTFOUND, "unknown dataset handle " + std::to_string(h));
+            uint32_t idx = (uint32_t)P.datasets.size();
+            P.datasets.push_back(it->second->desc());
+            P.ds_handles.push_back(h);
+            f = ds_index.emplace(h, idx).first;
+        }
+        prog_ds[i] = f->second;
+    }
+    // encode
+    std::vector<EncodedProgram> enc(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint64_t c0 = pop.code_off[i], c1 = pop.code_off[i + 1];
+        const uint64_t k0 = pop.kind_off[i], k1 = pop.kind_off[i + 1];
+        const uint64_t p0 = pop.param_off[i], p1 = pop.param_off[i + 1];
+        if (c1 < c0 || k1 < k0 || p1 < p0) return fail(RSR_EINVAL, "population offsets decrease at " + std::to_string(i));
+        std::string err;
+        int rc = encode_program(pop.code + c0, (uint32_t)(c1 - c0), pop.const_kinds + k0, (uint32_t)(k1 - k0),
+                                pop.params + p0, (uint32_t)(p1 - p0), P.datasets[prog_ds[i]].num_features, &enc[i],
+                                &err);
+        if (rc != RSR_OK) return fail(rc, "program " + std::to_string(i) + ": " + err);
+    }
+    // path per program: -2 adjoint, -1 plain, >= 0 register profile
+    std::vector<int> path(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (gradient) path[i] = -2;
+        else if (kernel == RSR_KERNEL_PLAIN || enc[i].profile < 0) path[i] = -1;
+        else path[i] = enc[i].profile;
+    }
+    // group programs by (path, dataset), each group sorted by descending code length
+    std::vector<uint32_t> order(n);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+        if (path[a] != path[b]) return path[a] < path[b];
+        if (prog_ds[a] != prog_ds[b]) return prog_ds[a] < prog_ds[b];
+        return enc[a].reg_code.size() + enc[a].slot_code.size() > enc[b].reg_code.size() + enc[b].slot_code.size();
+    });
+    P.progs.resize(n);
+    P.orig = order;
+    uint32_t part = 0;
+    for (uint32_t li = 0; li < n; ++li) {
+        const uint32_t i = order[li];
+        const EncodedProgram &E = enc[i];
+        const std::vector<uint32_t> &code = path[i] == -2 ? E.tape_code : path[i] == -1 ? E.slot_code : E.reg_code;
+        ProgDesc d{};
+        d.uop_off = (uint32_t)P.code.size();
+        d.uop_len = (uint32_t)code.size();
+        d.const_off = (uint32_t)P.consts.size();
+        d.n_consts = (uint32_t)E.consts.size();
+        d.n_slots = E.n_slots;
+        d.flags = (E.result_zero ? PF_RESULT_ZERO : 0u) | (E.needs_zero_init ? PF_NEEDS_ZERO_INIT : 0u) |
+                  (E.differentiable ? PF_DIFFERENTIABLE : 0u);
+        d.dataset = prog_ds[i];
+        const uint64_t n_eval = P.datasets[d.dataset].n_eval;
+        d.n_parts = (uint32_t)std::max<uint64_t>(1, (n_eval + kChunkPoints - 1) / kChunkPoints);
+        d.part_off = part;
+        d.n_tape = E.n_tape_slots;
+        part += d.n_parts;
+        P.code.insert(P.code.end(), code.begin(), code.end());
+        P.consts.insert(P.consts.end(), E.consts.begin(), E.consts.end());
+        P.progs[li] = d;
+        P.flops += (uint64_t)E.flops_per_point * n_eval;
+        P.program_points += n_eval;
+    }
+    P.n_partials = part * (gradient ? kGradSlotDoubles : 1);
+    // work items, one group per (path) run
+    uint32_t li = 0;
+    while (li < n) {
+        const int pth = path[order[li]];
+        uint32_t end = li;
+        while (end < n && path[order[end]] == pth) ++end;
+        Group g;
+        g.kind = pth == -2 ? 2 : pth == -1 ? 0 : 1;
+        g.profile = pth >= 0 ? pth : -1;
+        g.item_begin = (uint32_t)P.items.size();
+        if (g.kind == 1) {
+            // P and G are per profile and dataset size; one launch uses one P,
+            // the largest dataset's choice.
+            uint64_t max_eval = 0;
+            for (uint32_t j = li; j < end; ++j) max_eval = std::max(max_eval, P.datasets[P.progs[j].dataset].n_eval);
+            TuneChoice c = choice_for(ctx, g.profile, max_eval);
+            g.P = c.P;
+            g.G = c.G;
+            P.n_reg += end - li;
+        } else if (g.kind == 0) {
+            g.G = 1;
+            P.n_plain += end - li;
+        } else {
+            g.G = 1;
+        }
+        // tile size and per-warp staging requirements
+        uint32_t j = li;
+        std::vector<std::pair<uint64_t, WorkItem>> items;
+        while (j < end) {
+            uint32_t k = j + 1;
+            const uint32_t ds = P.progs[j].dataset;
+            while (k < end && k - j < (uint32_t)g.G && P.progs[k].dataset == ds) ++k;
+            uint32_t cw = 0, cf = 0, sl = 0, len_sum = 0;
+            for (uint32_t q = j; q < k; ++q) {
+                cw += P.progs[q].uop_len + 1;
+                cf += P.progs[q].n_consts;
+                sl = std::max(sl, g.kind == 2 ? P.progs[q].n_tape : P.progs[q].n_slots);
+                len_sum += P.progs[q].uop_len;
+            }
+            g.code_words = std::max(g.code_words, cw);
+            g.const_floats = std::max(g.const_floats, cf);
+            g.slots = std::max(g.slots, sl);
+            items.emplace_back(len_sum, WorkItem{j, k - j, 0, 0, 0, 0});
+            j = k;
+        }
+        // points per thread of slot-file kernels: largest that fits the smem budget
+        if (g.kind != 1) {
+            const size_t budget = 110 * 1024;
+            int Pp = g.kind == 2 ? 2 : 4;
+            while (Pp > 1) {
+                size_t per = g.kind == 2 ? grad_smem_per_warp(g.code_words, g.const_floats, g.slots)
+                                         : plain_smem_per_warp(g.code_words, g.const_floats, g.slots, Pp);
+                if (g.kind == 2) per += (size_t)g.slots * 32u * 4u * (Pp - 1) * 2u;
+                if (per <= budget) break;
+                Pp >>= 1;
+            }
+            g.P = Pp;
+        }
+        // expand chunks
+        std::vector<std::pair<uint64_t, WorkItem>> chunks;
+        const uint64_t tile_pts = 32ull * g.P;
+        for (auto &pr : items) {
+            const WorkItem &w = pr.second;
+            const uint64_t n_eval = P.datasets[P.progs[w.prog_begin].dataset].n_eval;
+            const uint64_t n_tiles = (n_eval + tile_pts - 1) / tile_pts;
+            const uint64_t tpc = kChunkPoints / tile_pts;
+            for (uint64_t c = 0, t = 0; t < n_tiles; ++c, t += tpc) {
+                WorkItem it = w;
+                it.tile_begin = (uint32_t)t;
+                it.tile_end = (uint32_t)std::min(n_tiles, t + tpc);
+                it.chunk = (uint32_t)c;
+                chunks.emplace_back(pr.first * (it.tile_end - it.tile_begin), it);
+            }
+        }
+        // longest first (persistent kernels pull items in this order)
+        std::stable_sort(chunks.begin(), chunks.end(),
+                         [](const auto &a, const auto &b) { return a.first > b.first; });
+        for (auto &c : chunks) P.items.push_back(c.second);
+        g.n_items = (uint32_t)P.items.size() - g.item_begin;
+        for (uint32_t q = li; q < end; ++q) {
+            const EncodedProgram &E = enc[order[q]];
+            const uint64_t ne = P.datasets[P.progs[q].dataset].n_eval;
+            g.flops += (uint64_t)E.flops_per_point * ne;
+            g.program_points += ne;
+        }
+        P.groups.push_back(g);
+        li = end;
+    }
+    return RSR_OK;
+}
+
+// Pinned staging buffer of the context.
+static int ensure_pinned(rsr_ctx *ctx, size_t bytes) {
+    if (bytes <= ctx->pinned_cap) return RSR_OK;
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_cap = 0;
+    size_t want = std::max<size_t>(bytes, 1 << 20);
+    cudaError_t e = cudaHostAlloc(&ctx->pinned, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaHostAlloc");
+    ctx->pinned_cap = want;
+    return RSR_OK;
+}
+
+int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st) {
+    const size_t n = plan.progs.size();
+    auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+    const size_t o_progs = 0;
+    const size_t o_ds = o_progs + al(n * sizeof(ProgDesc));
+    const size_t o_items = o_ds + al(plan.datasets.size() * sizeof(DatasetDesc));
+    const size_t o_code = o_items + al(plan.items.size() * sizeof(WorkItem));
+    const size_t o_consts = o_code + al((plan.code.size() + 1) * sizeof(uint32_t));
+    const size_t total = o_consts + al((plan.consts.size() + 1) * sizeof(float));
+    cudaError_t e;
+    if ((e = dev->pool.reserve(total)) != cudaSuccess) return cuda_fail(e, "plan pool");
+    if ((e = dev->partials.reserve(std::max<size_t>(plan.n_partials, 1) * sizeof(double))) != cudaSuccess)
+        return cuda_fail(e, "partials");
+    const size_t out_floats = plan.mode == MODE_POINTS ? n * plan.points_stride : n * (plan.gradient ? 33 : 1);
+    if ((e = dev->out.reserve(std::max<size_t>(out_floats, 1) * sizeof(float))) != cudaSuccess)
+        return cuda_fail(e, "outputs");
+    if ((e = dev->counters.reserve(std::max<size_t>(plan.groups.size(), 1) * sizeof(uint32_t) + 64)) != cudaSuccess)
+        return cuda_fail(e, "counters");
+    int rc = ensure_pinned(ctx, total);
+    if (rc) return rc;
+    // the pinned buffer is shared: wait for earlier copies out of it
+    cudaStreamSynchronize(st);
+    char *h = (char *)ctx->pinned;
+    memcpy(h + o_progs, plan.progs.data(), n * sizeof(ProgDesc));
+    memcpy(h + o_ds, plan.datasets.data(), plan.datasets.size() * sizeof(DatasetDesc));
+    memcpy(h + o_items, plan.items.data(), plan.items.size() * sizeof(WorkItem));
+    memcpy(h + o_code, plan.code.data(), plan.code.size() * sizeof(uint32_t));
+    memcpy(h + o_consts, plan.consts.data(), plan.consts.size() * sizeof(float));
+    if ((e = cudaMemcpyAsync(dev->pool.p, h, total, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return cuda_fail(e, "plan upload");
+    ctx->last_h2d = total;
+    char *d = (char *)dev->pool.p;
+    LaunchArgs &a = dev->base;
+    a = LaunchArgs{};
+    a.progs = (const ProgDesc *)(d + o_progs);
+    a.datasets = (const DatasetDesc *)(d + o_ds);
+    a.items = (const WorkItem *)(d + o_items);
+    a.code = (const uint32_t *)(d + o_code);
+    a.consts = (const float *)(d + o_consts);
+    a.partials = (double *)dev->partials.p;
+    a.mode = (uint32_t)plan.mode;
+    a.points_stride = plan.points_stride;
+    a.points_out = plan.mode == MODE_POINTS ? (float *)dev->out.p : nullptr;
+    dev->mse = (float *)dev->out.p;
+    dev->grad = plan.gradient ? (float *)dev->out.p + n : nullptr;
+    return RSR_OK;
+}
+
+int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st, cudaEvent_t ev_mid,
+                 cudaEvent_t *group_events) {
+    const uint32_t n = (uint32_t)plan.progs.size();
+    if (n == 0) {
+        if (ev_mid) cudaEventRecord(ev_mid, st);
+        return RSR_OK;
+    }
+    cudaError_t e;
+    uint32_t *counters = (uint32_t *)dev->counters.p;
+    if ((e = cudaMemsetAsync(counters, 0, plan.groups.size() * sizeof(uint32_t), st)) != cudaSuccess)
+        return cuda_fail(e, "counter reset");
+    for (size_t gi = 0; gi < plan.groups.size(); ++gi) {
+        const Group &g = plan.groups[gi];
+        if (g.n_items == 0) continue;
+        LaunchArgs a = dev->base;
+        a.items = dev->base.items + g.item_begin;
+        a.n_items = g.n_items;
+        a.item_counter = counters + gi;
+        a.smem_code_words = g.code_words;
+        a.smem_const_floats = g.const_floats;
+        a.smem_slots = g.slots;
+        a.progs_per_warp = g.G;
+        if (group_events) cudaEventRecord(group_events[2 * gi], st);
+        if (g.kind == 0) {
+            const size_t per = plain_smem_per_warp(g.code_words, g.const_floats, g.slots, g.P);
+            uint32_t wpb = (uint32_t)std::max<size_t>(1, std::min<size_t>(kPlainThreads / 32, (200 * 1024) / per));
+            e = launch_plain(a, g.P, wpb, per * wpb, st);
+        } else if (g.kind == 1) {
+            int bps = std::max(1, reg_max_blocks_per_sm(g.profile, g.P));
+            uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)bps * ctx->num_sms,
+                                                         (g.n_items + (kRegThreads / 32) - 1) / (kRegThreads / 32));
+            e = launch_reg(a, g.profile, g.P, std::max(1u, grid), st);
+        } else {
+            size_t per = grad_smem_per_warp(g.code_words, g.const_floats, g.slots);
+            per += (size_t)g.slots * 32u * 4u * (g.P - 1) * 2u;
+            uint32_t wpb = (uint32_t)std::max<size_t>(1, std::min<size_t>(kGradThreads / 32, (200 * 1024) / per));
+            a.progs_per_warp = (uint32_t)g.P;  // adjoint kernel reads P from here
+            e = launch_grad(a, wpb, per * wpb, st);
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+        if (group_events) cudaEventRecord(group_events[2 * gi + 1], st);
+        ctx->launches++;
+    }
+    if (ev_mid) cudaEventRecord(ev_mid, st);
+    if (plan.mode == MODE_MSE) {
+        if (plan.gradient)
+            e = launch_finalize_grad(dev->base.progs, dev->base.datasets, dev->base.partials, n, dev->mse, dev->grad, st);
+        else
+            e = launch_finalize_mse(dev->base.progs, dev->base.datasets, dev->base.partials, n, dev->mse, st);
+        if (e != cudaSuccess) return cuda_fail(e, "finalize launch");
+        ctx->launches++;
+    }
+    return RSR_OK;
+}
+
+// Copy results back in caller order.
+static int fetch_results(rsr_ctx *ctx, const Plan &plan, DevicePlan &dev, cudaStream_t st, float *mse_out,
+                         float *grad_out, float *points_out) {
+    const size_t n = plan.progs.size();
+    if (n == 0) return RSR_OK;
+    cudaError_t e;
+    if (plan.mode == MODE_POINTS) {
+        const size_t per = plan.points_stride;
+        std::vector<float> tmp(n * per);
+        if ((e = cudaMemcpyAsync(tmp.data(), dev.out.p, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost, st)))
+            return cuda_fail(e, "points download");
+        if ((e = cudaStreamSynchronize(st))) return cuda_fail(e, "evaluation");
+        ctx->last_d2h = tmp.size() * sizeof(float);
+        for (size_t li = 0; li < n; ++li) memcpy(points_out + (size_t)plan.orig[li] * per, tmp.data() + li * per, per * sizeof(float));
+        return RSR_OK;
+    }
+    const size_t nf = n * (plan.gradient ? 33 : 1);
+    std::vector<float> tmp(nf);
+    if ((e = cudaMemcpyAsync(tmp.data(), dev.out.p, nf * sizeof(float), cudaMemcpyDeviceToHost, st)))
+        return cuda_fail(e, "result download");
+    if ((e = cudaStreamSynchronize(st))) return cuda_fail(e, "evaluation");
+    ctx->last_d2h = nf * sizeof(float);
+    for (size_t li = 0; li < n; ++li) {
+        if (mse_out) mse_out[plan.orig[li]] = tmp[li];
+        if (grad_out && plan.gradient) memcpy(grad_out + (size_t)plan.orig[li] * 32, tmp.data() + n + li * 32, 32 * sizeof(float));
+    }
+    (void)ctx;
+    return RSR_OK;
+}
+
+static rsr_population single_pop(const rsr_program *p, uint64_t offs[6]) {
+    offs[0] = 0; offs[1] = p->len; offs[2] = 0; offs[3] = p->n_consts; offs[4] = 0; offs[5] = p->n_params;
+    rsr_population pop{};
+    pop.n_programs = 1;
+    pop.code = p->code;
+    pop.code_off = offs;
+    pop.const_kinds = p->const_kinds;
+    pop.kind_off = offs + 2;
+    pop.params = p->params;
+    pop.param_off = offs + 4;
+    return pop;
+}
+
+static int run_oneshot(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *dsp, uint64_t ds, int kernel,
+                       bool gradient, int mode, float *mse, float *grad, float *points) {
+    Plan plan;
+    int rc = build_plan(ctx, pop, dsp, ds, kernel, gradient, mode, &plan);
+    if (rc) return rc;
+    if (mode == MODE_POINTS) {
+        plan.points_stride = plan.datasets.empty() ? 0 : plan.datasets[0].n_eval;
+    }
+    if ((rc = upload_plan(ctx, plan, &ctx->scratch, ctx->stream))) return rc;
+    if ((rc = enqueue_plan(ctx, plan, &ctx->scratch, ctx->stream, nullptr))) return rc;
+    return fetch_results(ctx, plan, ctx->scratch, ctx->stream, mse, grad, points);
+}
+
+}  // namespace rsr
+
+using namespace rsr;
+
+// ====================================================================== ABI
+extern "C" {
+
+const char *rsr_last_error(void) { return g_last_error.c_str(); }
+const char *rsr_version(void) { return "rsr-b200 0.1 (sm_100a)"; }
+
+void rsr_options_default(rsr_options *o) {
+    if (!o) return;
+    memset(o, 0, sizeof(*o));
+    o->struct_size = sizeof(rsr_options);
+    o->kernel = RSR_KERNEL_AUTO;
+    o->use_graphs = 1;
+}
+
+int rsr_ctx_create(int device, const rsr_options *opts, rsr_ctx **out) {
+    if (!out) return fail(RSR_EINVAL, "out is null");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return fail(RSR_ENODEV, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(RSR_EINVAL, "device index out of range");
+    cudaDeviceProp prop;
+    if ((e = cudaGetDeviceProperties(&prop, device)) != cudaSuccess) return cuda_fail(e, "device properties");
+    if (prop.major != 10) return fail(RSR_ENODEV, std::string("sm_100 device required, found ") + prop.name);
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    auto *ctx = new rsr_ctx();
+    ctx->device = device;
+    ctx->num_sms = prop.multiProcessorCount;
+    rsr_options_default(&ctx->opts);
+    if (opts) memcpy(&ctx->opts, opts, std::min<size_t>(sizeof(rsr_options), opts->struct_size ? opts->struct_size : sizeof(rsr_options)));
+    if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        delete ctx;
+        return cuda_fail(e, "stream");
+    }
+    for (auto &ev : ctx->ev) cudaEventCreate(&ev);
+    if (ctx->opts.mem_budget_bytes == 0) {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        ctx->opts.mem_budget_bytes = (uint64_t)(fr * 0.9);
+    }
+    *out = ctx;
+    return RSR_OK;
+}
+
+int rsr_ctx_destroy(rsr_ctx *ctx) {
+    if (!ctx) return RSR_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto &kv : ctx->datasets) {
+        cudaFree(kv.second->x);
+        cudaFree(kv.second->y);
+    }
+    ctx->scratch.pool.release();
+    ctx->scratch.partials.release();
+    ctx->scratch.out.release();
+    ctx->scratch.counters.release();
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    if (ctx->l2buf) cudaFree(ctx->l2buf);
+    for (auto &ev : ctx->ev) if (ev) cudaEventDestroy(ev);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return RSR_OK;
+}
+
+static int upload_soa(rsr_ctx *ctx, const float *ff, const float *tb, bool aosoa, uint32_t nf, uint64_t nbatch,
+                      uint64_t nsamples, rsr_dataset *out) {
+    if (!out) return fail(RSR_EINVAL, "out is null");
+    if (nbatch == 0 || nsamples == 0 || nsamples > nbatch * 8 || nsamples <= (nbatch - 1) * 8)
+        return fail(RSR_EINVAL, "num_samples must satisfy 8*(num_batches-1) < num_samples <= 8*num_batches");
+    if (nf > 255) return fail(RSR_EINVAL, "at most 255 features (LoadVar operands are u8)");
+    if ((nf && !ff) || !tb) return fail(RSR_EINVAL, "feature or target pointer is null");
+    const uint64_t n_eval = nbatch * 8;
+    const uint64_t stride = round_up(n_eval, kStrideAlign);
+    const size_t xbytes = (size_t)stride * std::max<uint32_t>(nf, 1) * sizeof(float);
+    const size_t ybytes = (size_t)stride * sizeof(float);
+    if (ctx->mem_in_use + xbytes + ybytes > ctx->opts.mem_budget_bytes)
+        return fail(RSR_ENOMEM, "dataset exceeds the context's memory budget");
+    auto rec = std::make_unique<DatasetRec>();
+    cudaError_t e;
+    if ((e = cudaMalloc(&rec->x, xbytes)) != cudaSuccess) return cuda_fail(e, "dataset features");
+    if ((e = cudaMalloc(&rec->y, ybytes)) != cudaSuccess) { cudaFree(rec->x); return cuda_fail(e, "dataset targets"); }
+    cudaMemsetAsync(rec->x, 0, xbytes, ctx->stream);
+    cudaMemsetAsync(rec->y, 0, ybytes, ctx->stream);
+    rec->num_features = nf;
+    rec->num_batches = nbatch;
+    rec->num_samples = nsamples;
+    rec->stride = stride;
+    rec->bytes = xbytes + ybytes;
+    if (aosoa) {
+        // raw AoSoA upload, transposed on the device
+        const size_t rawx = (size_t)nbatch * nf * 8 * sizeof(float), rawy = (size_t)nbatch * 8 * sizeof(float);
+        void *tmp = nullptr;
+        if ((e = cudaMalloc(&tmp, rawx + rawy)) != cudaSuccess) {
+            cudaFree(rec->x); cudaFree(rec->y);
+            return cuda_fail(e, "dataset staging");
+        }
+        if (rawx) cudaMemcpyAsync(tmp, ff, rawx, cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync((char *)tmp + rawx, tb, rawy, cudaMemcpyHostToDevice, ctx->stream);
+        e = launch_aosoa_to_soa((const float *)tmp, (const float *)((char *)tmp + rawx), rec->x, rec->y, nf, nbatch,
+                                stride, ctx->num_sms, ctx->stream);
+        ctx->launches++;
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(tmp);
+    } else {
+        // columns: features[f*n + i] with n = nsamples, zero padded
+        for (uint32_t f = 0; f < nf; ++f)
+            cudaMemcpyAsync(rec->x + (size_t)f * stride, ff + (size_t)f * nsamples, nsamples * sizeof(float),
+                            cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync(rec->y, tb, nsamples * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+        e = cudaStreamSynchronize(ctx->stream);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        cudaFree(rec->x); cudaFree(rec->y);
+        return cuda_fail(e, "dataset upload");
+    }
+    ctx->mem_in_use += rec->bytes;
+    uint64_t h = ctx->next_handle++;
+    ctx->datasets.emplace(h, std::move(rec));
+    *out = h;
+    return RSR_OK;
+}
+
+int rsr_dataset_upload(rsr_ctx *ctx, const float *feature_flat, const float *target_batches, uint32_t num_features,
+                       uint64_t num_batches, uint64_t num_samples, rsr_dataset *out) {
+    if (!ctx) return fail(RSR_EINVAL, "ctx is null");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return upload_soa(ctx, feature_flat, target_batches, true, num_features, num_batches, num_samples, out);
+}
+
+int rsr_dataset_upload_columns(rsr_ctx *ctx, const float *features, const float *targets, uint32_t num_features,
+                               uint64_t n, rsr_dataset *out) {
+    if (!ctx) return fail(RSR_EINVAL, "ctx is null");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return upload_soa(ctx, features, targets, false, num_features, (n + 7) / 8, n, out);
+}
+
+int rsr_dataset_release(rsr_ctx *ctx, rsr_dataset ds) {
+    if (!ctx) return fail(RSR_EINVAL, "ctx is null");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    auto it = ctx->datasets.find(ds);
+    if (it == ctx->datasets.end()) return fail(RSR_ENOTFOUND, "unknown dataset handle");
+    if (it->second->refs.load() > 0) return fail(RSR_EBUSY, "dataset is referenced by a prepared batch or a job");
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(it->second->x);
+    cudaFree(it->second->y);
+    ctx->mem_in_use -= it->second->bytes;
+    ctx->datasets.erase(it);
+    return RSR_OK;
+}
+
+int rsr_dataset_info(rsr_ctx *ctx, rsr_dataset ds, uint32_t *nf, uint64_t *nb, uint64_t *ns) {
+    if (!ctx) return fail(RSR_EINVAL, "ctx is null");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    auto it = ctx->datasets.find(ds);
+    if (it == ctx->datasets.end()) return fail(RSR_ENOTFOUND, "unknown dataset handle");
+    if (nf) *nf = it->second->num_features;
+    if (nb) *nb = it->second->num_batches;
+    if (ns) *ns = it->second->num_samples;
+    return RSR_OK;
+}
+
+int rsr_compute_mse(rsr_ctx *ctx, const rsr_program *prog, rsr_dataset ds, float *mse) {
+    if (!ctx || !prog || !mse) return fail(RSR_EINVAL, "null argument");
+    uint64_t offs[6];
+    rsr_population pop = single_pop(prog, offs);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return run_oneshot(ctx, pop, nullptr, ds, ctx->opts.kernel, false, MODE_MSE, mse, nullptr, nullptr);
+}
+
+int rsr_compute_mse_with_gradient(rsr_ctx *ctx, const rsr_program *prog, rsr_dataset ds, float *mse, float *grad) {
+    if (!ctx || !prog || !mse || !grad) return fail(RSR_EINVAL, "null argument");
+    uint64_t offs[6];
+    rsr_population pop = single_pop(prog, offs);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return run_oneshot(ctx, pop, nullptr, ds, RSR_KERNEL_AUTO, true, MODE_MSE, mse, grad, nullptr);
+}
+
+int rsr_eval_points(rsr_ctx *ctx, const rsr_program *prog, rsr_dataset ds, float *out) {
+    if (!ctx || !prog || !out) return fail(RSR_EINVAL, "null argument");
+    uint64_t offs[6];
+    rsr_population pop = single_pop(prog, offs);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return run_oneshot(ctx, pop, nullptr, ds, ctx->opts.kernel, false, MODE_POINTS, nullptr, nullptr, out);
+}
+
+int rsr_eval_mse_batch(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const rsr_dataset *dsp, int kernel,
+                       float *mse_out) {
+    if (!ctx || !pop || (!mse_out && pop->n_programs)) return fail(RSR_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return run_oneshot(ctx, *pop, dsp, ds, kernel, false, MODE_MSE, mse_out, nullptr, nullptr);
+}
+
+int rsr_eval_mse_grad_batch(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const rsr_dataset *dsp,
+                            float *mse_out, float *grad_out) {
+    if (!ctx || !pop || ((!mse_out || !grad_out) && pop->n_programs)) return fail(RSR_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return run_oneshot(ctx, *pop, dsp, ds, RSR_KERNEL_AUTO, true, MODE_MSE, mse_out, grad_out, nullptr);
+}
+
+int rsr_eval_points_batch(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, int kernel, float *out) {
+    if (!ctx || !pop || (!out && pop->n_programs)) return fail(RSR_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return run_oneshot(ctx, *pop, nullptr, ds, kernel, false, MODE_POINTS, nullptr, nullptr, out);
+}
+
+// ------------------------------------------------------------ prepared
+int rsr_batch_prepare(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const rsr_dataset *dsp, int kernel,
+                      int with_gradient, rsr_batch **out) {
+    if (!ctx || !pop || !out) return fail(RSR_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    auto *b = new rsr_batch();
+    int rc = build_plan(ctx, *pop, dsp, ds, kernel, with_gradient != 0, MODE_MSE, &b->plan);
+    if (!rc) rc = upload_plan(ctx, b->plan, &b->dev, ctx->stream);
+    if (!rc && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "prepare");
+    if (rc) {
+        delete b;
+        return rc;
+    }
+    for (uint64_t h : b->plan.ds_handles) ctx->datasets[h]->refs++;
+    for (auto &ev : b->ev) cudaEventCreate(&ev);
+    b->pool_bytes = ctx->last_h2d;
+    b->gev.resize(2 * b->plan.groups.size());
+    for (auto &ev : b->gev) cudaEventCreate(&ev);
+    b->group_ms.assign(b->plan.groups.size(), 0.0f);
+    *out = b;
+    return RSR_OK;
+}
+
+int rsr_batch_run(rsr_ctx *ctx, rsr_batch *b) {
+    if (!ctx || !b) return fail(RSR_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaError_t e;
+    if (ctx->opts.use_graphs) {
+        if (!b->graph_ready) {
+            cudaGraph_t g;
+            if ((e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+                return cuda_fail(e, "graph capture");
+            uint64_t before = ctx->launches.load();
+            int rc = enqueue_plan(ctx, b->plan, &b->dev, ctx->stream, nullptr);
+            e = cudaStreamEndCapture(ctx->stream, &g);
+            if (rc) return rc;
+            if (e != cudaSuccess) return cuda_fail(e, "graph capture");
+            if ((e = cudaGraphInstantiate(&b->graph, g, 0)) != cudaSuccess) return cuda_fail(e, "graph instantiate");
+            cudaGraphDestroy(g);
+            b->graph_ready = true;
+            ctx->launches = before;  // counted at replay
+        }
+        cudaEventRecord(b->ev[0], ctx->stream);
+        if ((e = cudaGraphLaunch(b->graph, ctx->stream)) != cudaSuccess) return cuda_fail(e, "graph launch");
+        uint64_t nl = 0;
+        for (auto &g : b->plan.groups) nl += g.n_items ? 1 : 0;
+        ctx->launches += nl + (b->plan.progs.empty() ? 0 : 1);
+        cudaEventRecord(b->ev[2], ctx->stream);
+        return RSR_OK;
+    }
+    cudaEventRecord(b->ev[0], ctx->stream);
+    int rc = enqueue_plan(ctx, b->plan, &b->dev, ctx->stream, b->ev[1], b->gev.data());
+    if (rc) return rc;
+    cudaEventRecord(b->ev[2], ctx->stream);
+    return RSR_OK;
+}
+
+int rsr_batch_results(rsr_ctx *ctx, rsr_batch *b, float *mse_out, float *grad_out) {
+    if (!ctx || !b) return fail(RSR_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    int rc = fetch_results(ctx, b->plan, b->dev, ctx->stream, mse_out, grad_out, nullptr);
+    if (rc) return rc;
+    float t = 0.0f;
+    if (cudaEventElapsedTime(&t, b->ev[0], b->ev[2]) == cudaSuccess) b->total_ms = t;
+    if (!ctx->opts.use_graphs && cudaEventElapsedTime(&t, b->ev[0], b->ev[1]) == cudaSuccess) b->eval_ms = t;
+    else b->eval_ms = b->total_ms;
+    return RSR_OK;
+}
+
+int rsr_batch_last_timing(rsr_ctx *ctx, rsr_batch *b, float *eval_ms, float *total_ms) {
+    if (!ctx || !b) return fail(RSR_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaEventSynchronize(b->ev[2]);
+    if (e != cudaSuccess) return cuda_fail(e, "timing");
+    float t = 0.0f;
+    if (cudaEventElapsedTime(&t, b->ev[0], b->ev[2]) == cudaSuccess) b->total_ms = t;
+    b->eval_ms = b->total_ms;
+    if (!ctx->opts.use_graphs && cudaEventElapsedTime(&t, b->ev[0], b->ev[1]) == cudaSuccess) b->eval_ms = t;
+    if (!ctx->opts.use_graphs)
+        for (size_t g = 0; g < b->plan.groups.size(); ++g)
+            if (b->plan.groups[g].n_items && cudaEventElapsedTime(&t, b->gev[2 * g], b->gev[2 * g + 1]) == cudaSuccess)
+                b->group_ms[g] = t;
+    if (eval_ms) *eval_ms = b->eval_ms;
+    if (total_ms) *total_ms = b->total_ms;
+    return RSR_OK;
+}
+
+int rsr_batch_describe(rsr_ctx *ctx, rsr_batch *b, char *buf, size_t len) {
+    if (!ctx || !b || !buf || !len) return fail(RSR_EINVAL, "null argument");
+    std::string s = "{\"programs\": " + std::to_string(b->plan.progs.size()) +
+                    ", \"register_kernel_programs\": " + std::to_string(b->plan.n_reg) +
+                    ", \"slot_kernel_programs\": " + std::to_string(b->plan.n_plain) +
+                    ", \"work_items\": " + std::to_string(b->plan.items.size()) +
+                    ", \"flops\": " + std::to_string(b->plan.flops) +
+                    ", \"program_points\": " + std::to_string(b->plan.program_points) + ", \"groups\": [";
+    for (size_t i = 0; i < b->plan.groups.size(); ++i) {
+        const Group &g = b->plan.groups[i];
+        const char *kn = g.kind == 0 ? "slot" : g.kind == 1 ? "register" : "adjoint";
+        s += (i ? ", " : "") + std::string("{\"kernel\": \"") + kn + "\", \"profile\": " + std::to_string(g.profile) +
+             ", \"points_per_thread\": " + std::to_string(g.P) + ", \"programs_per_warp\": " + std::to_string(g.G) +
+             ", \"items\": " + std::to_string(g.n_items) + ", \"flops\": " + std::to_string(g.flops) +
+             ", \"program_points\": " + std::to_string(g.program_points) + ", \"last_ms\": " +
+             std::to_string(b->group_ms.size() > i ? b->group_ms[i] : 0.0f) + "}";
+    }
+    s += "], \"upload_bytes\": " + std::to_string(b->pool_bytes) + "}";
+    snprintf(buf, len, "%s", s.c_str());
+    return RSR_OK;
+}
+
+int rsr_batch_destroy(rsr_ctx *ctx, rsr_batch *b) {
+    if (!ctx || !b) return RSR_OK;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (uint64_t h : b->plan.ds_handles) {
+        auto it = ctx->datasets.find(h);
+        if (it != ctx->datasets.end()) it->second->refs--;
+    }
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (auto &ev : b->ev) if (ev) cudaEventDestroy(ev);
+    for (auto &ev : b->gev) if (ev) cudaEventDestroy(ev);
+    delete b;
+    return RSR_OK;
+}
+
+uint64_t rsr_ctx_launch_count(rsr_ctx *ctx) { return ctx ? ctx->launches.load() : 0; }
+
+int rsr_ctx_last_transfer(rsr_ctx *ctx, uint64_t *h2d_bytes, uint64_t *d2h_bytes) {
+    if (!ctx) return fail(RSR_EINVAL, "ctx is null");
+    if (h2d_bytes) *h2d_bytes = ctx->last_h2d;
+    if (d2h_bytes) *d2h_bytes = ctx->last_d2h;
+    return RSR_OK;
+}
+
+int rsr_flush_l2(rsr_ctx *ctx) {
+    if (!ctx) return fail(RSR_EINVAL, "ctx is null");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (!ctx->l2buf) {
+        ctx->l2bytes = 256ull << 20;
+        cudaError_t e = cudaMalloc(&ctx->l2buf, ctx->l2bytes);
+        if (e != cudaSuccess) return cuda_fail(e, "L2 flush buffer");
+    }
+    cudaError_t e = cudaMemsetAsync(ctx->l2buf, ctx->launches.load() & 0xFF, ctx->l2bytes, ctx->stream);
+    return e == cudaSuccess ? RSR_OK : cuda_fail(e, "L2 flush");
+}
+
+int rsr_synchronize(rsr_ctx *ctx) {
+    if (!ctx) return fail(RSR_EINVAL, "ctx is null");
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? RSR_OK : cuda_fail(e, "synchronize");
+}
+
+int rsr_measure_fp32_peak(rsr_ctx *ctx, double *lane_ops_per_s) {
+    if (!ctx || !lane_ops_per_s) return fail(RSR_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaError_t e = measure_fp32_peak(ctx->num_sms, ctx->stream, lane_ops_per_s);
+    ctx->launches += 2;
+    return e == cudaSuccess ? RSR_OK : cuda_fail(e, "fp32 peak");
+}
+
+int rsr_validate_program(const rsr_program *prog, uint32_t num_features) {
+    if (!prog) return fail(RSR_EINVAL, "prog is null");
+    EncodedProgram E;
+    std::string err;
+    int rc = encode_program(prog->code, prog->len, prog->const_kinds, prog->n_consts, prog->params, prog->n_params,
+                            num_features, &E, &err);
+    if (rc) return fail(rc, err);
+    return RSR_OK;
+}
+
+int rsr_program_analyze(const rsr_program *prog, uint32_t num_features, rsr_program_info *info) {
+    if (!prog || !info) return fail(RSR_EINVAL, "null argument");
+    EncodedProgram E;
+    std::string err;
+    int rc = encode_program(prog->code, prog->len, prog->const_kinds, prog->n_consts, prog->params, prog->n_params,
+                            num_features, &E, &err);
+    if (rc) return fail(rc, err);
+    for (int t = 0; t < N_STACKS; ++t) {
+        info->depth_ref[t] = (uint32_t)E.depth_ref[t];
+        info->depth_fast[t] = (uint32_t)E.depth_fast[t];
+    }
+    info->n_uops_fast = (uint32_t)E.reg_code.size();
+    info->n_uops_plain = (uint32_t)E.slot_code.size() / 3;
+    info->fast_profile = E.profile;
+    info->flops_per_point = E.flops_per_point;
+    return RSR_OK;
+}
+
+}  // extern "C"

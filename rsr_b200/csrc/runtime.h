@@ -1,0 +1,143 @@
+// runtime.h -- host-side engine state behind the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/rsr_gpu.h"
+#include "encoder.h"
+#include "kernels.h"
+#include "uops.h"
+
+namespace rsr {
+
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+// Grow-only device allocation.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t reserve(size_t bytes);
+    void release();
+    ~DevBuf() { release(); }
+};
+
+struct DatasetRec {
+    float *x = nullptr;   // features, SoA, stride points per feature
+    float *y = nullptr;
+    uint32_t num_features = 0;
+    uint64_t num_batches = 0, num_samples = 0, stride = 0;
+    size_t bytes = 0;
+    std::atomic<int> refs{0};  // prepared batches and in-flight jobs holding it
+    DatasetDesc desc() const {
+        DatasetDesc d{};
+        d.x = x; d.y = y; d.stride = stride; d.n_eval = num_batches * 8; d.num_samples = num_samples;
+        d.num_features = num_features;
+        return d;
+    }
+};
+
+// Tuned launch shape for one (kernel profile, dataset size class).
+struct TuneChoice {
+    int P = 0;
+    int G = 0;
+};
+
+// One kernel launch inside a plan.
+struct Group {
+    int kind = 0;        // 0 plain, 1 register, 2 adjoint
+    int profile = -1;
+    int P = 4;
+    int G = 1;
+    uint32_t item_begin = 0, n_items = 0;  // into the plan's item array
+    uint32_t code_words = 0, const_floats = 0, slots = 0;  // per-warp staging maxima
+    uint32_t grid = 0;
+    size_t smem = 0;
+    uint32_t warps_per_block = 0;
+    uint64_t flops = 0;           // algorithmic FP32 lane-ops of one run
+    uint64_t program_points = 0;
+};
+
+// A population encoded and laid out for the device: what one launch of the
+// engine needs besides the datasets.
+struct Plan {
+    std::vector<ProgDesc> progs;            // launch order
+    std::vector<uint32_t> orig;             // launch index -> caller index
+    std::vector<DatasetDesc> datasets;      // launch dataset table
+    std::vector<uint64_t> ds_handles;
+    std::vector<WorkItem> items;
+    std::vector<uint32_t> code;
+    std::vector<float> consts;
+    std::vector<Group> groups;
+    uint32_t n_partials = 0;                // doubles (gradient: 33 per slot)
+    bool gradient = false;
+    int mode = MODE_MSE;
+    uint64_t points_stride = 0;
+    uint64_t flops = 0;                     // algorithmic lane-ops of one run
+    uint64_t program_points = 0;
+    uint32_t n_plain = 0, n_reg = 0;
+};
+
+// Device copy of a plan plus the buffers one run writes.
+struct DevicePlan {
+    DevBuf pool;        // progs | datasets | items | code | consts
+    DevBuf partials;
+    DevBuf out;         // mse (n floats) [+ grad (n*32 floats)]
+    DevBuf counters;    // one item counter per group
+    DevBuf status;
+    LaunchArgs base{};
+    float *mse = nullptr, *grad = nullptr;
+};
+
+}  // namespace rsr
+
+struct rsr_ctx {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    rsr_options opts{};
+    std::mutex mu;
+    std::map<uint64_t, std::unique_ptr<rsr::DatasetRec>> datasets;
+    uint64_t next_handle = 1;
+    uint64_t mem_in_use = 0;
+    std::map<std::pair<int, int>, rsr::TuneChoice> tune;  // (profile, log2 points) -> choice
+    rsr::DevicePlan scratch;   // for one-shot calls
+    void *pinned = nullptr;
+    size_t pinned_cap = 0;
+    void *l2buf = nullptr;
+    size_t l2bytes = 0;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    std::atomic<uint64_t> launches{0};
+    uint64_t last_h2d = 0, last_d2h = 0;   // bytes copied by the last evaluation call
+};
+
+struct rsr_batch {
+    rsr::Plan plan;
+    rsr::DevicePlan dev;
+    cudaGraphExec_t graph = nullptr;
+    bool graph_ready = false;
+    float eval_ms = 0.0f, total_ms = 0.0f;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    std::vector<cudaEvent_t> gev;          // per-group kernel events (runs without graphs)
+    std::vector<float> group_ms;
+    uint64_t pool_bytes = 0;
+};
+
+namespace rsr {
+// Planning and execution (runtime.cu), shared with the serving loop.
+int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_prog, uint64_t ds_all, int kernel,
+               bool gradient, int mode, Plan *plan);
+int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st);
+// group_events: optional, 2 per group (before/after its kernel); not used
+// while capturing a graph.
+int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st, cudaEvent_t ev_mid,
+                 cudaEvent_t *group_events = nullptr);
+}  // namespace rsr
