@@ -199,6 +199,7 @@ def run_engine(args):
         return float(t.item())
 
     # ---------------------------------------------------- batched (resident)
+    tune = eng.autotune(pk, dd, reps=2)
     b = eng.prepare(pk, dd, kernel=N.KERNEL_AUTO)
     for _ in range(args.warmup):
         eng.flush_l2()
@@ -230,6 +231,7 @@ def run_engine(args):
     # per-kernel time of the dominant kernel (same batch, events per kernel, no graph)
     eng2 = Engine(device=local, use_graphs=False)
     dd2 = eng2.upload(ds)
+    eng2.autotune(pk, dd2, reps=2)
     b2 = eng2.prepare(pk, dd2, kernel=N.KERNEL_AUTO)
     gms = []
     for i in range(max(3, min(args.steps, 20)) + 3):
@@ -302,6 +304,7 @@ def run_engine(args):
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "wall_s_timed": t_wall,
+            "autotune": tune["chosen"],
             "programs_on_register_kernel": desc["register_kernel_programs"],
             "programs_on_slot_kernel": desc["slot_kernel_programs"],
         }

@@ -95,7 +95,11 @@ typedef struct rsr_options {
     int32_t use_graphs;          /* replay prepared batches through CUDA graphs */
     uint64_t mem_budget_bytes;   /* 0 = 90% of free device memory at creation */
     const char *tune_cache_path; /* autotuner cache (JSON); NULL = in memory only */
+    uint32_t flags;              /* RSR_OPT_* */
 } rsr_options;
+
+/* rsr_options.flags */
+#define RSR_OPT_NO_LOAD_FUSION 1u   /* register kernel: keep loads as separate micro-ops */
 
 /* ------------------------------------------------------------- context */
 RSR_API void rsr_options_default(rsr_options *opts);
@@ -157,6 +161,13 @@ RSR_API int rsr_batch_last_timing(rsr_ctx *ctx, rsr_batch *b, float *eval_ms, fl
 RSR_API int rsr_batch_describe(rsr_ctx *ctx, rsr_batch *b, char *buf, size_t buf_len);
 RSR_API int rsr_batch_destroy(rsr_ctx *ctx, rsr_batch *b);
 
+/* Autotuner: times the register kernel's launch shapes (points per thread
+ * 2/4/8, programs per warp 1/2/4/8) on this population and keeps the
+ * fastest per kernel profile and dataset size class for later calls on the
+ * context.  report (optional) receives the timings as JSON. */
+RSR_API int rsr_autotune(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const rsr_dataset *ds_per_program,
+                         int reps, char *report, size_t report_len);
+
 /* Number of this library's kernel launches issued on the context since
  * creation (device-side work the host enqueued). */
 RSR_API uint64_t rsr_ctx_launch_count(rsr_ctx *ctx);
@@ -186,6 +197,12 @@ typedef struct rsr_program_info {
     uint32_t flops_per_point;    /* algorithmic FP32 lane-ops incl. the MSE epilogue */
 } rsr_program_info;
 RSR_API int rsr_program_analyze(const rsr_program *prog, uint32_t num_features, rsr_program_info *info);
+/* Device encoding of a program, for diagnostics and tests: form 0 = slot
+ * form (3 words per instruction), 1 = accumulator form (one word per
+ * micro-op), 2 = tape form (adjoint).  Writes up to cap words and the full
+ * length to *len. */
+RSR_API int rsr_program_encoding(const rsr_program *prog, uint32_t num_features, int form, uint32_t *out,
+                                 uint32_t cap, uint32_t *len);
 
 #ifdef __cplusplus
 }

@@ -16,6 +16,7 @@ RSR_OK, RSR_EINVAL, RSR_EPROGRAM, RSR_ENOMEM, RSR_ENODEV, RSR_ECUDA, RSR_ETIMEDO
 STATUS_NAMES = ["OK", "EINVAL", "EPROGRAM", "ENOMEM", "ENODEV", "ECUDA", "ETIMEDOUT", "ENOTFOUND", "EBUSY",
                 "ECANCELED"]
 KERNEL_AUTO, KERNEL_PLAIN, KERNEL_BATCHED = 0, 1, 2
+OPT_NO_LOAD_FUSION = 1
 
 
 class RsrError(RuntimeError):
@@ -39,7 +40,7 @@ class Population(C.Structure):
 class Options(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("kernel", C.c_int32), ("points_per_thread", C.c_int32),
                 ("programs_per_warp", C.c_int32), ("use_graphs", C.c_int32), ("mem_budget_bytes", C.c_uint64),
-                ("tune_cache_path", C.c_char_p)]
+                ("tune_cache_path", C.c_char_p), ("flags", C.c_uint32)]
 
 
 class ProgramInfo(C.Structure):
@@ -81,10 +82,14 @@ _SIGS = {
     "rsr_ctx_launch_count": (C.c_uint64, [C.c_void_p]),
     "rsr_ctx_last_transfer": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "rsr_flush_l2": (C.c_int, [C.c_void_p]),
+    "rsr_autotune": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_int, C.c_char_p,
+                               C.c_size_t]),
     "rsr_synchronize": (C.c_int, [C.c_void_p]),
     "rsr_measure_fp32_peak": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "rsr_validate_program": (C.c_int, [C.POINTER(Program), C.c_uint32]),
     "rsr_program_analyze": (C.c_int, [C.POINTER(Program), C.c_uint32, C.POINTER(ProgramInfo)]),
+    "rsr_program_encoding": (C.c_int, [C.POINTER(Program), C.c_uint32, C.c_int, C.c_void_p, C.c_uint32,
+                                       C.POINTER(C.c_uint32)]),
 }
 
 

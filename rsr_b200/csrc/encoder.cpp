@@ -99,7 +99,7 @@ int const_kind_for_load(int opcode) {
 
 namespace {
 
-// ------------------------------------------------------- register form
+// ---------------------------------------------------- accumulator form
 enum OpClass { C_LOAD, C_BIN, C_DOT, C_SCALE, C_MULMV, C_UNARY_F, C_GET, C_NORM, C_DET, C_TRACE, C_MAT_UN, C_MAKE };
 
 OpClass op_class(int op) {
@@ -121,241 +121,250 @@ OpClass op_class(int op) {
     }
 }
 
-struct Plan {
-    int fused = -1;        // operand index taken from a feature/constant directly
-    int order[3] = {0, 1, 2};
-    int n_kids = 0;        // stack operands in evaluation order (operand indices)
-    std::array<int, N_STACKS> need{};
-};
+// (binary-op index within its type's block, index of the reversed form)
+struct BinIdx { int op, rop; };
+BinIdx bin_index(int opcode) {
+    switch (opcode) {
+        case ADD_F: return {0, 0};  case SUB_F: return {1, 2};  case MUL_F: return {3, 3};  case DIV_F: return {4, 5};
+        case ADD_V2: return {0, 0}; case SUB_V2: return {1, 2};
+        case ADD_V3: return {0, 0}; case SUB_V3: return {1, 2}; case CROSS_V3: return {3, 4};
+        case ADD_M2: case ADD_M3: return {0, 0};
+        case SUB_M2: case SUB_M3: return {1, 2};
+        case MUL_M2: case MUL_M3: return {3, 4};
+        default: return {0, 0};
+    }
+}
 
-class RegEmitter {
+class AccEmitter {
    public:
-    RegEmitter(const std::vector<Node> &nodes) : nodes_(nodes), plans_(nodes.size()) {}
+    explicit AccEmitter(const std::vector<Node> &nodes)
+        : nodes_(nodes), writes_(nodes.size(), 0), size_(nodes.size(), 0) {}
 
-    bool plan(int id) {  // fills plans_ bottom-up; false if unsupported
+    bool analyze(int id) {  // accumulator write sets and subtree sizes; false if unsupported
         const Node &n = nodes_[id];
-        Plan &p = plans_[id];
         if (is_load(n.opcode)) {
             if (n.stale) return false;
-            p.need.fill(0);
-            p.need[n.out] = 1;
+            writes_[id] = 1u << n.out;
+            size_[id] = 1;
+            types_ |= 1u << n.out;
             return true;
         }
-        for (int i = 0; i < n.n_in; ++i)
-            if (!plan(n.in[i])) return false;
-        OpClass c = op_class(n.opcode);
-        // choose a fused (leaf) operand
-        if (c == C_BIN || c == C_DOT) {
-            if (leaf(nodes_[n.in[1]])) p.fused = 1;
-            else if (leaf(nodes_[n.in[0]])) p.fused = 0;
-        } else if (c == C_SCALE || c == C_MULMV) {
-            if (leaf(nodes_[n.in[0]])) p.fused = 0;
+        uint32_t w = 1u << n.out;
+        int sz = 1;
+        for (int i = 0; i < n.n_in; ++i) {
+            if (!analyze(n.in[i])) return false;
+            w |= writes_[n.in[i]];
+            sz += size_[n.in[i]];
         }
-        int kids[3], nk = 0;
-        for (int i = 0; i < n.n_in; ++i)
-            if (i != p.fused) kids[nk++] = i;
-        p.n_kids = nk;
-        // best evaluation order of the stack operands
-        int perm[3] = {0, 1, 2};
-        int best_cost = 1 << 30;
-        std::array<int, N_STACKS> best_need{};
-        int best_order[3] = {0, 1, 2};
-        do {
-            std::array<int, N_STACKS> cur{}, peak{};
-            for (int j = 0; j < nk; ++j) {
-                int k = n.in[kids[perm[j]]];
-                const auto &kn = plans_[k].need;
-                for (int t = 0; t < N_STACKS; ++t) peak[t] = std::max(peak[t], cur[t] + kn[t]);
-                cur[nodes_[k].out] += 1;
-            }
-            if (n.out >= 0) {
-                int consumed = 0;
-                for (int j = 0; j < nk; ++j) consumed += nodes_[n.in[kids[j]]].out == n.out;
-                peak[n.out] = std::max(peak[n.out], cur[n.out] - consumed + 1);
-            }
-            int cost = 0;
-            for (int t = 0; t < N_STACKS; ++t) cost += peak[t] * kStackWidth[t];
-            if (cost < best_cost) {
-                best_cost = cost;
-                best_need = peak;
-                for (int j = 0; j < nk; ++j) best_order[j] = kids[perm[j]];
-            }
-        } while (std::next_permutation(perm, perm + nk));
-        p.need = best_need;
-        for (int j = 0; j < nk; ++j) p.order[j] = best_order[j];
+        writes_[id] = w;
+        size_[id] = sz;
+        types_ |= w;
         return true;
     }
 
-    // Emits the subtree of `id`; leaves its value on top of its stack.
+    // Emits the subtree of `id`; leaves its value in the accumulator of its type.
     void gen(int id) {
         const Node &n = nodes_[id];
-        const Plan &p = plans_[id];
-        if (is_load(n.opcode)) {
-            int t = n.out;
-            static const int ldx[N_STACKS] = {U_F_LDX, U_V2_LDX, U_V3_LDX, U_M2_LDX, U_M3_LDX};
-            static const int ldc[N_STACKS] = {U_F_LDC, U_V2_LDC, U_V3_LDC, U_M2_LDC, U_M3_LDC};
-            emit(is_const_load(n.opcode) ? ldc[t] : ldx[t], push(t), n.arg);
+        const int op = n.opcode;
+        if (is_load(op)) {
+            emit(kBlockBase[n.out] + (is_const_load(op) ? KV_LDC : KV_LDX), n.arg);
             return;
         }
-        int pos[3] = {-1, -1, -1};
-        for (int j = 0; j < p.n_kids; ++j) {
-            int i = p.order[j];
-            gen(n.in[i]);
-            pos[i] = sp_[nodes_[n.in[i]].out] - 1;
-        }
-        // pop the stack operands
-        for (int i = 0; i < n.n_in; ++i)
-            if (i != p.fused) sp_[nodes_[n.in[i]].out] -= 1;
-        const Node *fz = p.fused >= 0 ? &nodes_[n.in[p.fused]] : nullptr;
-        bool fzc = fz && is_const_load(fz->opcode);
-        uint32_t farg = fz ? fz->arg : 0;
-        int op = n.opcode;
+        const Node *in[3] = {n.n_in > 0 ? &nodes_[n.in[0]] : nullptr, n.n_in > 1 ? &nodes_[n.in[1]] : nullptr,
+                             n.n_in > 2 ? &nodes_[n.in[2]] : nullptr};
         switch (op_class(op)) {
             case C_BIN: {
-                int t = n.out;
-                int r = sp_[t];
-                int kind = bin_kind(op, p.fused, fzc, pos, r);
-                emit(kind, r, farg);
-                push(t);
+                const int t = n.out, base = kBlockBase[t] + KV_BIN;
+                const BinIdx b = bin_index(op);
+                const bool la = leaf(*in[0]), lb = leaf(*in[1]);
+                if (lb) {                       // acc = a op leaf
+                    gen(n.in[0]);
+                    emit(base + 3 * b.op + src_of(*in[1]), in[1]->arg);
+                } else if (la) {                // acc = leaf op b
+                    gen(n.in[1]);
+                    emit(base + 3 * b.rop + src_of(*in[0]), in[0]->arg);
+                } else if (size_[n.in[1]] > size_[n.in[0]]) {  // b first: acc = a op S[b]
+                    gen(n.in[1]);
+                    const int slot = push(t);
+                    gen(n.in[0]);
+                    emit(base + 3 * b.op + SRC_S, slot);
+                    pop(t);
+                } else {                        // a first: acc = S[a] op b
+                    gen(n.in[0]);
+                    const int slot = push(t);
+                    gen(n.in[1]);
+                    emit(base + 3 * b.rop + SRC_S, slot);
+                    pop(t);
+                }
                 break;
             }
             case C_DOT: {
-                int t = nodes_[n.in[0]].out;
-                int base = t == SV2 ? U_V2_DOT_T : U_V3_DOT_T;
-                if (p.fused < 0) emit(base, std::min(pos[0], pos[1]), 0);
-                else emit(base + (fzc ? 2 : 1), pos[1 - p.fused], farg);
-                use_t(1);
-                emit(U_F_FROM_T0, push(SF), 0);
-                break;
-            }
-            case C_SCALE: {
-                int t = n.out;
-                static const int sc[N_STACKS] = {0, U_V2_SCALE_T, U_V3_SCALE_T, U_M2_SCALE_T, U_M3_SCALE_T};
-                if (p.fused == 0) {
-                    emit(sc[t] + (fzc ? 2 : 1), pos[1], farg);
-                } else {
-                    emit(U_F_TO_T0, pos[0], 0);
-                    use_t(1);
-                    emit(sc[t], pos[1], 0);
+                const int t = in[0]->out, nb = kBinOps[t];
+                const int base = kBlockBase[t] + kv_dot(nb);
+                if (leaf(*in[1])) { gen(n.in[0]); emit(base + src_of(*in[1]), in[1]->arg); }
+                else if (leaf(*in[0])) { gen(n.in[1]); emit(base + src_of(*in[0]), in[0]->arg); }
+                else {
+                    gen(n.in[0]);
+                    const int slot = push(t);
+                    gen(n.in[1]);
+                    emit(base + SRC_S, slot);
+                    pop(t);
                 }
-                push(t);
                 break;
             }
-            case C_MULMV: {
-                int tv = n.out;
-                int base = tv == SV2 ? U_V2_MULM_T : U_V3_MULM_T;
-                if (p.fused == 0) {
-                    emit(base + (fzc ? 2 : 1), pos[1], farg);
-                } else {
-                    emit(tv == SV2 ? U_M2_TO_T : U_M3_TO_T, pos[0], 0);
-                    use_t(tv == SV2 ? 4 : 9);
-                    emit(base, pos[1], 0);
+            case C_SCALE: {  // in[0] scalar, in[1] vector/matrix
+                const int t = n.out;
+                const int base = kBlockBase[t] + (t == SM2 || t == SM3 ? (int)KM_SCALE : kv_scale(kBinOps[t]));
+                cross_type(n, base, SF, t);
+                break;
+            }
+            case C_MULMV: {  // in[0] matrix, in[1] vector
+                const int t = n.out, tm = in[0]->out;
+                const int w = t == SV2 ? 2 : 3;
+                cross_type(n, kBlockBase[t] + kv_mulm(kBinOps[t], w), tm, t);
+                break;
+            }
+            case C_UNARY_F:
+                gen(n.in[0]);
+                emit(K_F_UN + (op - SIN_F), 0);
+                break;
+            case C_NORM: case C_GET: {
+                const int t = in[0]->out, nb = kBinOps[t];
+                gen(n.in[0]);
+                int k = kv_norm(nb);
+                if (op == GET_X_V2 || op == GET_X_V3) k += 1;
+                if (op == GET_Y_V2 || op == GET_Y_V3) k += 2;
+                if (op == GET_Z_V3) k += 3;
+                emit(kBlockBase[t] + k, 0);
+                break;
+            }
+            case C_DET: case C_TRACE: case C_MAT_UN: {
+                const int t = in[0]->out;
+                gen(n.in[0]);
+                int k = op == DET_M2 || op == DET_M3 ? KM_DET : op == TRACE_M2 || op == TRACE_M3 ? KM_TRACE
+                      : op == TRANSPOSE_M2 || op == TRANSPOSE_M3 ? KM_TRANSPOSE : KM_INVERSE;
+                emit(kBlockBase[t] + k, 0);
+                break;
+            }
+            case C_MAKE: {  // operands pushed in order, the last stays in its accumulator
+                const int tin = in[0]->out, t = n.out;
+                int first = -1;
+                for (int i = 0; i + 1 < n.n_in; ++i) {
+                    gen(n.in[i]);
+                    const int slot = push(tin);
+                    if (i == 0) first = slot;
                 }
-                push(tv);
-                break;
-            }
-            case C_UNARY_F: {
-                static const int k[] = {U_F_SIN, U_F_COS, U_F_EXP, U_F_SQR, U_F_SQRT, U_F_LN};
-                emit(k[op - SIN_F], pos[0], 0);
-                push(SF);
-                break;
-            }
-            case C_GET: {
-                int kind = op == GET_X_V2 ? U_V2_GETX_T : op == GET_Y_V2 ? U_V2_GETY_T
-                         : op == GET_X_V3 ? U_V3_GETX_T : op == GET_Y_V3 ? U_V3_GETY_T : U_V3_GETZ_T;
-                emit(kind, pos[0], 0);
-                use_t(1);
-                emit(U_F_FROM_T0, push(SF), 0);
-                break;
-            }
-            case C_NORM:
-                emit(op == NORM_V2 ? U_V2_NORM_T : U_V3_NORM_T, pos[0], 0);
-                use_t(1);
-                emit(U_F_FROM_T0, push(SF), 0);
-                break;
-            case C_DET: case C_TRACE: {
-                int kind = op == DET_M2 ? U_M2_DET_T : op == DET_M3 ? U_M3_DET_T
-                         : op == TRACE_M2 ? U_M2_TRACE_T : U_M3_TRACE_T;
-                emit(kind, pos[0], 0);
-                use_t(1);
-                emit(U_F_FROM_T0, push(SF), 0);
-                break;
-            }
-            case C_MAT_UN: {
-                int kind = op == TRANSPOSE_M2 ? U_M2_TRANSPOSE : op == TRANSPOSE_M3 ? U_M3_TRANSPOSE
-                         : op == INVERSE_M2 ? U_M2_INVERSE : U_M3_INVERSE;
-                emit(kind, pos[0], 0);
-                push(n.out);
-                break;
-            }
-            case C_MAKE: {
-                if (op == MAKE_VEC2 || op == MAKE_VEC3) {
-                    static const int tt[3] = {U_F_TO_T0, U_F_TO_T1, U_F_TO_T2};
-                    for (int i = 0; i < n.n_in; ++i) emit(tt[i], pos[i], 0);
-                    use_t(n.n_in);
-                    emit(op == MAKE_VEC2 ? U_V2_FROM_T : U_V3_FROM_T, push(n.out), 0);
-                } else if (op == MAKE_MAT2) {
-                    emit(U_V2_TO_T0, pos[0], 0);
-                    emit(U_V2_TO_T2, pos[1], 0);
-                    use_t(4);
-                    emit(U_M2_FROM_T, push(SM2), 0);
-                } else {
-                    emit(U_V3_TO_T0, pos[0], 0);
-                    emit(U_V3_TO_T3, pos[1], 0);
-                    emit(U_V3_TO_T6, pos[2], 0);
-                    use_t(9);
-                    emit(U_M3_FROM_T, push(SM3), 0);
-                }
+                gen(n.in[n.n_in - 1]);
+                const int k = t == SM2 || t == SM3 ? (int)KM_MAKE : kv_make(kBinOps[t], t == SV2 ? 2 : 3);
+                emit(kBlockBase[t] + k, (uint32_t)first);
+                for (int i = 0; i + 1 < n.n_in; ++i) pop(tin);
                 break;
             }
             case C_LOAD: break;
         }
     }
 
-    const Plan &plan_of(int id) const { return plans_[id]; }
     std::vector<uint32_t> code;
     int max_sp[N_STACKS] = {0, 0, 0, 0, 0};
-    int max_t = 0;
+    uint32_t types_ = 0;  // accumulator types used
 
    private:
-    int push(int t) {
-        int p = sp_[t]++;
-        max_sp[t] = std::max(max_sp[t], sp_[t]);
-        return p;
-    }
-    void use_t(int n) { max_t = std::max(max_t, n); }
-    void emit(int kind, int slot, uint32_t arg) { code.push_back(uop_word(kind, slot, arg)); }
-
-    static int bin_kind(int op, int fused, bool fzc, const int *pos, int r) {
-        // base kinds: {stack-stack, reversed, X, reversed X, C, reversed C}
-        struct K { int s, rs, x, rx, c, rc; };
-        K k{};
-        switch (op) {
-            case ADD_F: k = {U_F_ADD, U_F_ADD, U_F_ADDX, U_F_ADDX, U_F_ADDC, U_F_ADDC}; break;
-            case MUL_F: k = {U_F_MUL, U_F_MUL, U_F_MULX, U_F_MULX, U_F_MULC, U_F_MULC}; break;
-            case SUB_F: k = {U_F_SUB, U_F_RSUB, U_F_SUBX, U_F_RSUBX, U_F_SUBC, U_F_RSUBC}; break;
-            case DIV_F: k = {U_F_DIV, U_F_RDIV, U_F_DIVX, U_F_RDIVX, U_F_DIVC, U_F_RDIVC}; break;
-            case ADD_V2: k = {U_V2_ADD, U_V2_ADD, U_V2_ADDX, U_V2_ADDX, U_V2_ADDC, U_V2_ADDC}; break;
-            case SUB_V2: k = {U_V2_SUB, U_V2_RSUB, U_V2_SUBX, U_V2_RSUBX, U_V2_SUBC, U_V2_RSUBC}; break;
-            case ADD_V3: k = {U_V3_ADD, U_V3_ADD, U_V3_ADDX, U_V3_ADDX, U_V3_ADDC, U_V3_ADDC}; break;
-            case SUB_V3: k = {U_V3_SUB, U_V3_RSUB, U_V3_SUBX, U_V3_RSUBX, U_V3_SUBC, U_V3_RSUBC}; break;
-            case CROSS_V3: k = {U_V3_CROSS, U_V3_RCROSS, U_V3_CROSSX, U_V3_RCROSSX, U_V3_CROSSC, U_V3_RCROSSC}; break;
-            case ADD_M2: k = {U_M2_ADD, U_M2_ADD, U_M2_ADDX, U_M2_ADDX, U_M2_ADDC, U_M2_ADDC}; break;
-            case SUB_M2: k = {U_M2_SUB, U_M2_RSUB, U_M2_SUBX, U_M2_RSUBX, U_M2_SUBC, U_M2_RSUBC}; break;
-            case MUL_M2: k = {U_M2_MUL, U_M2_RMUL, U_M2_MULX, U_M2_RMULX, U_M2_MULC, U_M2_RMULC}; break;
-            case ADD_M3: k = {U_M3_ADD, U_M3_ADD, U_M3_ADDX, U_M3_ADDX, U_M3_ADDC, U_M3_ADDC}; break;
-            case SUB_M3: k = {U_M3_SUB, U_M3_RSUB, U_M3_SUBX, U_M3_RSUBX, U_M3_SUBC, U_M3_RSUBC}; break;
-            case MUL_M3: k = {U_M3_MUL, U_M3_RMUL, U_M3_MULX, U_M3_RMULX, U_M3_MULC, U_M3_RMULC}; break;
+    // Ops whose second operand has another type (Scale: scalar, MulMV:
+    // matrix): the operand of the result type is evaluated last; the other
+    // one is fused if it is a leaf, kept in its accumulator if the result
+    // subtree does not overwrite it, pushed to its stack otherwise.
+    // base + {0 A, 1 X, 2 C, 3 S}.
+    void cross_type(const Node &n, int base, int tother, int t) {
+        const Node &o = nodes_[n.in[0]];
+        if (leaf(o)) {
+            gen(n.in[1]);
+            emit(base + 1 + src_of(o), o.arg);
+            return;
         }
-        if (fused == 1) return fzc ? k.c : k.x;   // stack[r] = stack[r] op leaf
-        if (fused == 0) return fzc ? k.rc : k.rx; // stack[r] = leaf op stack[r]
-        return pos[0] == r ? k.s : k.rs;          // operands at r, r+1
+        gen(n.in[0]);
+        if (writes_[n.in[1]] & (1u << tother)) {
+            const int slot = push(tother);
+            gen(n.in[1]);
+            emit(base + 3, slot);
+            pop(tother);
+        } else {
+            gen(n.in[1]);
+            emit(base + 0, 0);
+        }
+        (void)t;
     }
+    static int src_of(const Node &leafn) { return is_const_load(leafn.opcode) ? SRC_C : SRC_X; }
+    int push(int t) {
+        const int slot = sp_[t]++;
+        max_sp[t] = std::max(max_sp[t], sp_[t]);
+        emit(kBlockBase[t] + KV_PUSH, (uint32_t)slot);
+        return slot;
+    }
+    void pop(int t) { sp_[t]--; }
+    void emit(int kind, uint32_t arg) { code.push_back(uop_word((uint32_t)kind, arg)); }
 
     const std::vector<Node> &nodes_;
-    std::vector<Plan> plans_;
+    std::vector<uint32_t> writes_;
+    std::vector<int> size_;
     int sp_[N_STACKS] = {0, 0, 0, 0, 0};
 };
+
+// Peephole pass over the accumulator form: a PUSH directly followed by a
+// load becomes part of the load, and a load directly followed by a unary op
+// on the loaded value becomes the load's post-op.
+int kind_block(int kind) { return kind >= K_M3 ? SM3 : kind >= K_M2 ? SM2 : kind >= K_V3 ? SV3 : kind >= K_V2 ? SV2 : SF; }
+
+int post_op_of(int kind, int t) {
+    const int k = kind - kBlockBase[t];
+    if (t == SF) return (k >= K_F_UN - K_F && k < K_F_END - K_F) ? k - (K_F_UN - K_F) + 1 : 0;
+    if (t == SV2 || t == SV3) {
+        const int kn = kv_norm(kBinOps[t]), w = kStackWidth[t];
+        return (k >= kn && k <= kn + w) ? k - kn + 1 : 0;
+    }
+    if (k == KM_DET) return 1;
+    if (k == KM_TRACE) return 2;
+    if (k == KM_TRANSPOSE) return 3;
+    if (k == KM_INVERSE) return 4;
+    return 0;
+}
+
+bool is_unary_kind(int kind, int t) { return post_op_of(kind, t) != 0; }
+
+void fuse_loads(std::vector<uint32_t> *code) {
+    const std::vector<uint32_t> &c = *code;
+    // 1. a load directly followed by a unary op on the loaded value
+    std::vector<uint32_t> out;
+    for (size_t i = 0; i < c.size(); ++i) {
+        const int kind = (int)(c[i] & 0xFFu);
+        const int t = kind_block(kind), k = kind - kBlockBase[t];
+        if ((k == KV_LDX || k == KV_LDC) && i + 1 < c.size()) {
+            const int kn = (int)(c[i + 1] & 0xFFu);
+            if (kind_block(kn) == t && is_unary_kind(kn, t)) {
+                out.push_back(uop_word((uint32_t)kn, unary_load_arg(c[i] >> 8, k == KV_LDX ? 1u : 2u)));
+                ++i;
+                continue;
+            }
+        }
+        out.push_back(c[i]);
+    }
+    // 2. a PUSH directly followed by a load
+    std::vector<uint32_t> fin;
+    for (size_t i = 0; i < out.size(); ++i) {
+        const int kind = (int)(out[i] & 0xFFu);
+        const int t = kind_block(kind), k = kind - kBlockBase[t];
+        if (k == KV_PUSH && i + 1 < out.size()) {
+            const int kn = (int)(out[i + 1] & 0xFFu), tn = kind_block(kn), kk = kn - kBlockBase[tn];
+            if (kk == KV_LDX || kk == KV_LDC) {
+                fin.push_back(uop_word((uint32_t)kind, push_load_arg(out[i] >> 8, (uint32_t)tn + 1u,
+                                                                     kk == KV_LDC ? 1u : 0u, out[i + 1] >> 8)));
+                ++i;
+                continue;
+            }
+        }
+        fin.push_back(out[i]);
+    }
+    *code = std::move(fin);
+}
 
 void set_err(std::string *err, const std::string &m) {
     if (err) *err = m;
@@ -365,7 +374,7 @@ void set_err(std::string *err, const std::string &m) {
 
 int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uint32_t n_consts,
                    const float *params, uint32_t n_params, uint32_t num_features, EncodedProgram *out,
-                   std::string *err) {
+                   std::string *err, bool fuse) {
     EncodedProgram &E = *out;
     E = EncodedProgram();
     if (len > 0 && !code) { set_err(err, "code is null"); return RSR_EINVAL; }
@@ -527,18 +536,19 @@ int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uin
         }
     }
 
-    // ---- register form
-    if (root >= 0 && !has_stale_live) {
-        RegEmitter em(nodes);
-        if (em.plan(root)) {
+    // ---- accumulator form
+    if (root >= 0 && !has_stale_live && n_params < (1u << kLdOffsetBits)) {
+        AccEmitter em(nodes);
+        if (em.analyze(root)) {
             em.gen(root);
-            const auto &need = em.plan_of(root).need;
-            for (int t = 0; t < N_STACKS; ++t) E.depth_fast[t] = std::max(need[t], em.max_sp[t]);
-            for (int p = 0; p < N_PROFILES; ++p) {
-                bool ok = em.max_t <= kProfiles[p].n_transfer;
-                for (int t = 0; t < N_STACKS; ++t) ok = ok && E.depth_fast[t] <= kProfiles[p].cap[t];
-                if (ok) { E.profile = p; break; }
+            if (fuse) fuse_loads(&em.code);
+            bool fits = true;
+            for (int t = 0; t < N_STACKS; ++t) {
+                E.depth_fast[t] = em.max_sp[t];
+                fits = fits && em.max_sp[t] <= kMaxAccStack;
             }
+            for (int p = 0; fits && p < N_PROFILES; ++p)
+                if ((em.types_ & ~kProfileTypes[p]) == 0) { E.profile = p; break; }
             if (E.profile >= 0) E.reg_code = std::move(em.code);
         }
     }

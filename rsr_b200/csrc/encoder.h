@@ -51,6 +51,6 @@ struct EncodedProgram {
 // Returns 0 or an rsr_status code, with a message in *err.
 int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uint32_t n_consts,
                    const float *params, uint32_t n_params, uint32_t num_features, EncodedProgram *out,
-                   std::string *err);
+                   std::string *err, bool fuse_loads = true);
 
 }  // namespace rsr

@@ -22,8 +22,10 @@ cudaError_t launch_finalize_mse(const ProgDesc *progs, const DatasetDesc *ds, co
 
 // register-stack kernel (kernels_reg.cu)
 cudaError_t launch_reg(const LaunchArgs &a, int profile, int P, uint32_t grid, cudaStream_t st);
-size_t reg_smem_per_warp(uint32_t code_words, uint32_t const_floats);
-int reg_max_blocks_per_sm(int profile, int P);
+void reg_layout(uint32_t code_words, uint32_t const_floats, const uint32_t *stack_depth, int P,
+                uint32_t *stack_off, uint32_t *acc_off, uint32_t *region_floats);
+int reg_max_p(int profile);
+int reg_max_blocks_per_sm(int profile, int P, size_t smem);
 
 // adjoint kernel (kernels_grad.cu)
 cudaError_t launch_grad(const LaunchArgs &a, uint32_t warps_per_block, size_t smem, cudaStream_t st);

@@ -28,6 +28,10 @@ struct LaunchArgs {
     uint32_t smem_const_floats;
     uint32_t smem_slots;      // per warp (slot-file kernels)
     uint32_t progs_per_warp;
+    // register kernel: per-warp shared-memory layout (floats)
+    uint32_t region_floats;
+    uint32_t acc_off;
+    uint32_t stack_off[N_STACKS];
 };
 
 // Kahan-compensated single-precision running sum (one per lane).

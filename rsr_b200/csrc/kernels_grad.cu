@@ -32,6 +32,7 @@ struct TapeCtx {
     const float *consts;
     const float *x;
     uint64_t stride, p0;
+    uint64_t n_eval;   // points counted (num_batches * 8)
     int lane;
     __device__ __forceinline__ Vf<P> V(uint32_t s) const { return val[s * 32 + lane]; }
     __device__ __forceinline__ void SV(uint32_t s, const Vf<P> &v) const { val[s * 32 + lane] = v; }
@@ -164,7 +165,8 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, uint32_t w0, u
                 const Vf<P> g = t.A(o + i);
                 float s = 0.0f;
 #pragma unroll
-                for (int k = 0; k < P; ++k) s = s + g.v[k];
+                for (int k = 0; k < P; ++k)  // points past the dataset's end may carry 0*inf = NaN adjoints
+                    if (t.p0 + k < t.n_eval) s = s + g.v[k];
                 gacc_lane[(aux + i) * 32] += s;
             }
             break;
@@ -330,7 +332,7 @@ __global__ void __launch_bounds__(kGradThreads) grad_kernel(const LaunchArgs a) 
     const uint32_t result = scode[0];
     const uint32_t *code = scode + 1;
     const uint32_t n_nodes = (pd.uop_len - 1) / 3;
-    TapeCtx<P> t{val, adj, sconst, ds.x, ds.stride, 0, lane};
+    TapeCtx<P> t{val, adj, sconst, ds.x, ds.stride, 0, ds.n_eval, lane};
     Kahan sse;
     double gsum[kGradParams];
 #pragma unroll

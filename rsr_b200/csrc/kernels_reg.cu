@@ -1,18 +1,17 @@
-// kernels_reg.cu -- the register-stack interpreter (batched persistent
-// kernel).
+// kernels_reg.cu -- the batched register kernel: an accumulator machine.
 //
-// Each typed stack of the reference VM (state.rs:12-37) is an array of
-// P-point values held in registers.  A register cannot be indexed at run
-// time, so the stack position is part of the dispatch: every micro-op word
-// selects one (kind, position) case of a dense switch, and each case is
-// straight-line code on fixed registers.  The encoder keeps positions small
-// by evaluating subtrees in the order that needs the fewest slots, which
-// leaves every value bit-identical to the reference's.
+// Each value type of the reference VM (state.rs:12-37) has one accumulator
+// register set holding P data points per lane: A_F, A_V2[2], A_V3[3],
+// A_M2[4], A_M3[9].  Micro-ops (uops.h, accumulator form) combine an
+// accumulator with a feature, a constant, a value spilled to a per-type
+// stack in shared memory (slot fixed by the encoder), or another type's
+// accumulator, so dispatch is on the micro-op kind alone (about 140 cases,
+// one code block each) and values never leave registers except for spills.
 //
-// The kernel is persistent: warps pull work items (a group of programs on a
-// chunk of point tiles) from a global counter, so uneven program lengths and
-// uneven dataset sizes balance across the GPU.  All programs of an item run
-// on each tile while its features are hot in L1.
+// The kernel is persistent: warps pull work items (up to 8 programs sharing a
+// dataset, on a chunk of point tiles) from a global counter, so uneven
+// program lengths and dataset sizes balance across the 148 SMs; all programs
+// of an item run on each tile while its features are hot in L1.
 #include <cuda_runtime.h>
 
 #include "kernels.h"
@@ -20,283 +19,273 @@
 
 namespace rsr {
 
-template <int N> struct AtLeast1 { static constexpr int v = N > 0 ? N : 1; };
+template <int PROF>
+struct Types {
+    static constexpr uint32_t T = kProfileTypes[PROF];
+    static constexpr bool V2 = (T >> SV2) & 1u, V3 = (T >> SV3) & 1u, M2 = (T >> SM2) & 1u, M3 = (T >> SM3) & 1u;
+};
 
 template <int PROF, int P>
-struct RegState {
-    static constexpr int DF = kProfiles[PROF].cap[SF];
-    static constexpr int DV2 = kProfiles[PROF].cap[SV2];
-    static constexpr int DV3 = kProfiles[PROF].cap[SV3];
-    static constexpr int DM2 = kProfiles[PROF].cap[SM2];
-    static constexpr int DM3 = kProfiles[PROF].cap[SM3];
-    static constexpr int NT = kProfiles[PROF].n_transfer;
-    Vf<P> F[AtLeast1<DF>::v];
-    Vf<P> V2[AtLeast1<DV2>::v][2];
-    Vf<P> V3[AtLeast1<DV3>::v][3];
-    Vf<P> M2[AtLeast1<DM2>::v][4];
-    Vf<P> M3[AtLeast1<DM3>::v][9];
-    Vf<P> T[AtLeast1<NT>::v];
+struct Acc {
+    Vf<P> F[1];
+    Vf<P> V2[Types<PROF>::V2 ? 2 : 1];
+    Vf<P> V3[Types<PROF>::V3 ? 3 : 1];
+    Vf<P> M2[Types<PROF>::M2 ? 4 : 1];
+    Vf<P> M3[Types<PROF>::M3 ? 9 : 1];
 };
 
 template <int P>
-struct RegIO {
+struct AccIO {
     const float *x;
     uint64_t stride;
     uint64_t p0;
     const float *consts;
+    Vf<P> *stk[N_STACKS];  // per-type shared-memory stacks of this warp: [(slot*W + c)*32 + lane]
+    int lane;
     __device__ __forceinline__ Vf<P> X(uint32_t f) const { return load_pts<P>(x + f * stride + p0); }
     __device__ __forceinline__ Vf<P> C(uint32_t i) const { return splat<P>(consts[i]); }
-    __device__ __forceinline__ void Xn(Vf<P> *d, uint32_t f, int n) const {
-#pragma unroll
-        for (int i = 0; i < n; ++i) d[i] = X(f + i);
-    }
-    __device__ __forceinline__ void Cn(Vf<P> *d, uint32_t c, int n) const {
-#pragma unroll
-        for (int i = 0; i < n; ++i) d[i] = C(c + i);
-    }
+    template <int W>
+    __device__ __forceinline__ Vf<P> &S(int t, uint32_t slot, int c) const { return stk[t][(slot * W + c) * 32 + lane]; }
 };
 
-template <int P, int W>
-__device__ __forceinline__ void vcopy(Vf<P> *d, const Vf<P> *s) {
-#pragma unroll
-    for (int i = 0; i < W; ++i) d[i] = s[i];
+template <int PROF, int P, int t>
+__device__ __forceinline__ Vf<P> *acc_of(Acc<PROF, P> &a) {
+    if constexpr (t == SF) return a.F;
+    else if constexpr (t == SV2) return a.V2;
+    else if constexpr (t == SV3) return a.V3;
+    else if constexpr (t == SM2) return a.M2;
+    else return a.M3;
 }
 
-// Same-stack binary operations of width W: a = a op b, op selected by OPK:
-// 0 add, 1 sub, 2 reversed sub (b - a), 3 cross, 4 reversed cross,
-// 5 mat-mul (M2 if W == 4, M3 if W == 9), 6 reversed mat-mul.
-template <int P, int W, int OPK>
-__device__ __forceinline__ void bin_op(Vf<P> *a, const Vf<P> *b) {
-    if constexpr (OPK == 0) {
+// Second operand of width W from a feature, a constant or a stack slot of type t.
+template <int P, int W, int SRC>
+__device__ __forceinline__ void fetch(Vf<P> *b, const AccIO<P> &io, int t, uint32_t arg) {
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+        if constexpr (SRC == SRC_X) b[c] = io.X(arg + c);
+        else if constexpr (SRC == SRC_C) b[c] = io.C(arg + c);
+        else b[c] = io.template S<W>(t, arg, c);
+    }
+}
+
+// a = a op b (or b op a for the R-forms), op an AccBin code.
+template <int P, int W, int OP>
+__device__ __forceinline__ void apply_bin(Vf<P> *a, const Vf<P> *b) {
+    if constexpr (OP == BIN_ADD) {
 #pragma unroll
         for (int i = 0; i < W; ++i) a[i] = a[i] + b[i];
-    } else if constexpr (OPK == 1) {
+    } else if constexpr (OP == BIN_SUB) {
 #pragma unroll
         for (int i = 0; i < W; ++i) a[i] = a[i] - b[i];
-    } else if constexpr (OPK == 2) {
+    } else if constexpr (OP == BIN_RSUB) {
 #pragma unroll
         for (int i = 0; i < W; ++i) a[i] = b[i] - a[i];
-    } else if constexpr (OPK == 3) {
+    } else if constexpr (OP == BIN_MUL) {
+        a[0] = a[0] * b[0];
+    } else if constexpr (OP == BIN_DIV) {
+        a[0] = a[0] / b[0];
+    } else if constexpr (OP == BIN_RDIV) {
+        a[0] = b[0] / a[0];
+    } else if constexpr (OP == BIN_CROSS) {
         cross3(a, b, a);
-    } else if constexpr (OPK == 4) {
+    } else if constexpr (OP == BIN_RCROSS) {
         cross3(b, a, a);
-    } else if constexpr (OPK == 5) {
+    } else if constexpr (OP == BIN_MMUL) {
         if constexpr (W == 4) mul_m2(a, b, a); else mul_m3(a, b, a);
     } else {
         if constexpr (W == 4) mul_m2(b, a, a); else mul_m3(b, a, a);
     }
 }
 
-// One register micro-op (kind K at stack position S).
-template <int PROF, int P, int K, int S>
-__device__ __forceinline__ void uop(RegState<PROF, P> &st, const RegIO<P> &io, uint32_t arg) {
-    using St = RegState<PROF, P>;
-    constexpr int DF = St::DF, DV2 = St::DV2, DV3 = St::DV3, DM2 = St::DM2, DM3 = St::DM3, NT = St::NT;
-    // ------------------------------------------------------------ F stack
-    if constexpr (K <= U_F_LN) {
-        if constexpr (S < DF) {
-            Vf<P> &a = st.F[S];
-            if constexpr (K == U_F_LDX) a = io.X(arg);
-            else if constexpr (K == U_F_LDC) a = io.C(arg);
-            else if constexpr (K == U_F_FROM_T0) a = st.T[0];
-            else if constexpr (K == U_F_TO_T0) st.T[0] = a;
-            else if constexpr (K == U_F_TO_T1) { if constexpr (NT > 1) st.T[1] = a; }
-            else if constexpr (K == U_F_TO_T2) { if constexpr (NT > 2) st.T[2] = a; }
-            else if constexpr (K >= U_F_ADD && K <= U_F_RDIV) {
-                if constexpr (S + 1 < DF) {
-                    const Vf<P> &b = st.F[S + 1];
-                    if constexpr (K == U_F_ADD) a = a + b;
-                    else if constexpr (K == U_F_SUB) a = a - b;
-                    else if constexpr (K == U_F_RSUB) a = b - a;
-                    else if constexpr (K == U_F_MUL) a = a * b;
-                    else if constexpr (K == U_F_DIV) a = a / b;
-                    else a = b / a;
-                }
-            } else if constexpr (K >= U_F_ADDX && K <= U_F_RDIVC) {
-                constexpr int k6 = (K - U_F_ADDX) % 6;
-                const Vf<P> b = (K <= U_F_RDIVX) ? io.X(arg) : io.C(arg);
-                if constexpr (k6 == 0) a = a + b;
-                else if constexpr (k6 == 1) a = a - b;
-                else if constexpr (k6 == 2) a = b - a;
-                else if constexpr (k6 == 3) a = a * b;
-                else if constexpr (k6 == 4) a = a / b;
-                else a = b / a;
-            } else if constexpr (K == U_F_SIN) a = vsin(a);
-            else if constexpr (K == U_F_COS) a = vcos(a);
-            else if constexpr (K == U_F_EXP) a = vexp(a);
-            else if constexpr (K == U_F_SQR) a = a * a;
-            else if constexpr (K == U_F_SQRT) a = vsqrt(a);
-            else if constexpr (K == U_F_LN) a = vlog(a);
-        }
+template <int t, int j>
+__host__ __device__ constexpr int bin_code() {
+    if constexpr (t == SF) {
+        return j == 0 ? BIN_ADD : j == 1 ? BIN_SUB : j == 2 ? BIN_RSUB : j == 3 ? BIN_MUL : j == 4 ? BIN_DIV : BIN_RDIV;
+    } else if constexpr (t == SV2) {
+        return j == 0 ? BIN_ADD : j == 1 ? BIN_SUB : BIN_RSUB;
+    } else if constexpr (t == SV3) {
+        return j == 0 ? BIN_ADD : j == 1 ? BIN_SUB : j == 2 ? BIN_RSUB : j == 3 ? BIN_CROSS : BIN_RCROSS;
+    } else {
+        return j == 0 ? BIN_ADD : j == 1 ? BIN_SUB : j == 2 ? BIN_RSUB : j == 3 ? BIN_MMUL : BIN_RMMUL;
     }
-    // ----------------------------------------------------------- V2 stack
-    else if constexpr (K >= U_V2_LDX && K <= U_V2_MULMC) {
-        if constexpr (S < DV2) {
-            Vf<P> *a = st.V2[S];
-            if constexpr (K == U_V2_LDX) io.Xn(a, arg, 2);
-            else if constexpr (K == U_V2_LDC) io.Cn(a, arg, 2);
-            else if constexpr (K == U_V2_FROM_T) { if constexpr (NT >= 2) vcopy<P, 2>(a, st.T); }
-            else if constexpr (K == U_V2_TO_T0) { if constexpr (NT >= 2) vcopy<P, 2>(st.T, a); }
-            else if constexpr (K == U_V2_TO_T2) { if constexpr (NT >= 4) vcopy<P, 2>(st.T + 2, a); }
-            else if constexpr (K >= U_V2_ADD && K <= U_V2_RSUB) {
-                if constexpr (S + 1 < DV2) bin_op<P, 2, K - U_V2_ADD>(a, st.V2[S + 1]);
-            } else if constexpr (K >= U_V2_ADDX && K <= U_V2_RSUBC) {
-                Vf<P> b[2];
-                if constexpr (K <= U_V2_RSUBX) io.Xn(b, arg, 2); else io.Cn(b, arg, 2);
-                bin_op<P, 2, (K - U_V2_ADDX) % 3>(a, b);
-            } else if constexpr (K == U_V2_SCALE_T || K == U_V2_SCALE_X || K == U_V2_SCALE_C) {
-                const Vf<P> s = K == U_V2_SCALE_T ? st.T[0] : K == U_V2_SCALE_X ? io.X(arg) : io.C(arg);
-                a[0] = a[0] * s; a[1] = a[1] * s;
-            } else if constexpr (K == U_V2_DOT_T) {
-                if constexpr (S + 1 < DV2) st.T[0] = dot2(a, st.V2[S + 1]);
-            } else if constexpr (K == U_V2_DOTX_T || K == U_V2_DOTC_T) {
-                Vf<P> b[2];
-                if constexpr (K == U_V2_DOTX_T) io.Xn(b, arg, 2); else io.Cn(b, arg, 2);
-                st.T[0] = dot2(a, b);
-            } else if constexpr (K == U_V2_NORM_T) st.T[0] = norm2(a);
-            else if constexpr (K == U_V2_GETX_T) st.T[0] = a[0];
-            else if constexpr (K == U_V2_GETY_T) st.T[0] = a[1];
-            else if constexpr (K == U_V2_MULM_T) { if constexpr (NT >= 4) mul_m2v2(st.T, a, a); }
-            else if constexpr (K == U_V2_MULMX || K == U_V2_MULMC) {
-                Vf<P> m[4];
-                if constexpr (K == U_V2_MULMX) io.Xn(m, arg, 4); else io.Cn(m, arg, 4);
-                mul_m2v2(m, a, a);
-            }
-        }
+}
+
+// Load a feature (or a constant) into the accumulator of runtime type t
+// (one of the profile's): the load fused after a PUSH.
+template <int PROF, int P, int t>
+__device__ __forceinline__ void load_t(Acc<PROF, P> &a, const AccIO<P> &io, uint32_t is_const, uint32_t off) {
+    if constexpr (((kProfileTypes[PROF] >> t) & 1u) != 0u) {
+        constexpr int W = kStackWidth[t];
+        Vf<P> *A = acc_of<PROF, P, t>(a);
+        if (is_const) fetch<P, W, SRC_C>(A, io, t, off);
+        else fetch<P, W, SRC_X>(A, io, t, off);
     }
-    // ----------------------------------------------------------- V3 stack
-    else if constexpr (K >= U_V3_LDX && K <= U_V3_MULMC) {
-        if constexpr (S < DV3) {
-            Vf<P> *a = st.V3[S];
-            if constexpr (K == U_V3_LDX) io.Xn(a, arg, 3);
-            else if constexpr (K == U_V3_LDC) io.Cn(a, arg, 3);
-            else if constexpr (K == U_V3_FROM_T) { if constexpr (NT >= 3) vcopy<P, 3>(a, st.T); }
-            else if constexpr (K == U_V3_TO_T0) { if constexpr (NT >= 3) vcopy<P, 3>(st.T, a); }
-            else if constexpr (K == U_V3_TO_T3) { if constexpr (NT >= 6) vcopy<P, 3>(st.T + 3, a); }
-            else if constexpr (K == U_V3_TO_T6) { if constexpr (NT >= 9) vcopy<P, 3>(st.T + 6, a); }
-            else if constexpr (K >= U_V3_ADD && K <= U_V3_RCROSS) {
-                if constexpr (S + 1 < DV3) bin_op<P, 3, K - U_V3_ADD>(a, st.V3[S + 1]);
-            } else if constexpr (K >= U_V3_ADDX && K <= U_V3_RCROSSC) {
-                Vf<P> b[3];
-                if constexpr (K <= U_V3_RCROSSX) io.Xn(b, arg, 3); else io.Cn(b, arg, 3);
-                bin_op<P, 3, (K - U_V3_ADDX) % 5>(a, b);
-            } else if constexpr (K == U_V3_SCALE_T || K == U_V3_SCALE_X || K == U_V3_SCALE_C) {
-                const Vf<P> s = K == U_V3_SCALE_T ? st.T[0] : K == U_V3_SCALE_X ? io.X(arg) : io.C(arg);
-                a[0] = a[0] * s; a[1] = a[1] * s; a[2] = a[2] * s;
-            } else if constexpr (K == U_V3_DOT_T) {
-                if constexpr (S + 1 < DV3) st.T[0] = dot3(a, st.V3[S + 1]);
-            } else if constexpr (K == U_V3_DOTX_T || K == U_V3_DOTC_T) {
-                Vf<P> b[3];
-                if constexpr (K == U_V3_DOTX_T) io.Xn(b, arg, 3); else io.Cn(b, arg, 3);
-                st.T[0] = dot3(a, b);
-            } else if constexpr (K == U_V3_NORM_T) st.T[0] = norm3(a);
-            else if constexpr (K == U_V3_GETX_T) st.T[0] = a[0];
-            else if constexpr (K == U_V3_GETY_T) st.T[0] = a[1];
-            else if constexpr (K == U_V3_GETZ_T) st.T[0] = a[2];
-            else if constexpr (K == U_V3_MULM_T) { if constexpr (NT >= 9) mul_m3v3(st.T, a, a); }
-            else if constexpr (K == U_V3_MULMX || K == U_V3_MULMC) {
-                Vf<P> m[9];
-                if constexpr (K == U_V3_MULMX) io.Xn(m, arg, 9); else io.Cn(m, arg, 9);
-                mul_m3v3(m, a, a);
-            }
-        }
+}
+template <int PROF, int P>
+__device__ __forceinline__ void load_any(Acc<PROF, P> &a, const AccIO<P> &io, uint32_t t, uint32_t is_const,
+                                         uint32_t off) {
+    switch (t) {
+        case SF: load_t<PROF, P, SF>(a, io, is_const, off); break;
+        case SV2: load_t<PROF, P, SV2>(a, io, is_const, off); break;
+        case SV3: load_t<PROF, P, SV3>(a, io, is_const, off); break;
+        case SM2: load_t<PROF, P, SM2>(a, io, is_const, off); break;
+        default: load_t<PROF, P, SM3>(a, io, is_const, off); break;
     }
-    // ------------------------------------------------------- M2 / M3 stacks
-    else if constexpr (K >= U_M2_LDX && K <= U_M3_INVERSE) {
-        constexpr bool is3 = K >= U_M3_LDX;
-        constexpr int W = is3 ? 9 : 4;
-        constexpr int D = is3 ? DM3 : DM2;
-        constexpr int k = K - (is3 ? U_M3_LDX : U_M2_LDX);  // offset within the M block
-        if constexpr (S < D) {
-            Vf<P> *a;
-            if constexpr (is3) a = st.M3[S]; else a = st.M2[S];
-            if constexpr (k == 0) io.Xn(a, arg, W);
-            else if constexpr (k == 1) io.Cn(a, arg, W);
-            else if constexpr (k == 2) { if constexpr (NT >= W) vcopy<P, W>(a, st.T); }
-            else if constexpr (k == 3) { if constexpr (NT >= W) vcopy<P, W>(st.T, a); }
-            else if constexpr (k >= 4 && k <= 8) {  // ADD SUB RSUB MUL RMUL (stack)
-                if constexpr (S + 1 < D) {
-                    Vf<P> *b;
-                    if constexpr (is3) b = st.M3[S + 1]; else b = st.M2[S + 1];
-                    constexpr int opk = k == 4 ? 0 : k == 5 ? 1 : k == 6 ? 2 : k == 7 ? 5 : 6;
-                    bin_op<P, W, opk>(a, b);
-                }
-            } else if constexpr (k >= 9 && k <= 18) {  // X and C forms
-                Vf<P> b[W];
-                if constexpr (k <= 13) io.Xn(b, arg, W); else io.Cn(b, arg, W);
-                constexpr int j = (k - 9) % 5;
-                constexpr int opk = j == 0 ? 0 : j == 1 ? 1 : j == 2 ? 2 : j == 3 ? 5 : 6;
-                bin_op<P, W, opk>(a, b);
-            } else if constexpr (k >= 19 && k <= 21) {  // SCALE_T / X / C
-                const Vf<P> s = k == 19 ? st.T[0] : k == 20 ? io.X(arg) : io.C(arg);
+}
+
+// Optional operand load in front of a unary op (uops.h, unary_load_arg).
+template <int P, int W>
+__device__ __forceinline__ void unary_prefix(Vf<P> *A, const AccIO<P> &io, int t, uint32_t arg) {
+    const uint32_t src1 = (arg >> 12) & 3u;
+    if (src1 == 1u) fetch<P, W, SRC_X>(A, io, t, arg & 0xFFFu);
+    else if (src1 == 2u) fetch<P, W, SRC_C>(A, io, t, arg & 0xFFFu);
+}
+
+// One accumulator micro-op of kind K.
+template <int PROF, int P, int K>
+__device__ __forceinline__ void acc_op(Acc<PROF, P> &a, const AccIO<P> &io, uint32_t arg) {
+    constexpr int t = K >= K_M3 ? SM3 : K >= K_M2 ? SM2 : K >= K_V3 ? SV3 : K >= K_V2 ? SV2 : SF;
+    if constexpr (((kProfileTypes[PROF] >> t) & 1u) != 0u) {
+        constexpr int W = kStackWidth[t];
+        constexpr int k = K - kBlockBase[t];
+        constexpr int nb = kBinOps[t];
+        Vf<P> *A = acc_of<PROF, P, t>(a);
+        if constexpr (k == KV_LDX) {
+            fetch<P, W, SRC_X>(A, io, t, arg);
+        } else if constexpr (k == KV_LDC) {
+            fetch<P, W, SRC_C>(A, io, t, arg);
+        } else if constexpr (k == KV_PUSH) {
+            const uint32_t slot = arg & 15u, lt = (arg >> 4) & 7u;
 #pragma unroll
-                for (int i = 0; i < W; ++i) a[i] = a[i] * s;
-            } else if constexpr (k == 22) {
-                if constexpr (is3) st.T[0] = det_m3(a); else st.T[0] = det_m2(a);
-            } else if constexpr (k == 23) {
-                if constexpr (is3) st.T[0] = trace_m3(a); else st.T[0] = trace_m2(a);
-            } else if constexpr (k == 24) {
-                if constexpr (is3) transpose_m3(a, a); else transpose_m2(a, a);
-            } else if constexpr (k == 25) {
-                if constexpr (is3) inverse_m3(a, a); else inverse_m2(a, a);
+            for (int c = 0; c < W; ++c) io.template S<W>(t, slot, c) = A[c];
+            if (lt) load_any<PROF, P>(a, io, lt - 1u, (arg >> 7) & 1u, arg >> 8);
+        } else if constexpr (k >= KV_BIN && k < KV_BIN + 3 * nb) {
+            constexpr int j = (k - KV_BIN) / 3, src = (k - KV_BIN) % 3;
+            Vf<P> b[W];
+            fetch<P, W, src>(b, io, t, arg);
+            apply_bin<P, W, bin_code<t, j>()>(A, b);
+        } else if constexpr (t == SF) {
+            constexpr int u = k - (K_F_UN - K_F);
+            unary_prefix<P, 1>(A, io, t, arg);
+            if constexpr (u == 0) A[0] = vsin(A[0]);
+            else if constexpr (u == 1) A[0] = vcos(A[0]);
+            else if constexpr (u == 2) A[0] = vexp(A[0]);
+            else if constexpr (u == 3) A[0] = A[0] * A[0];
+            else if constexpr (u == 4) A[0] = vsqrt(A[0]);
+            else if constexpr (u == 5) A[0] = vlog(A[0]);
+        } else if constexpr (t == SV2 || t == SV3) {
+            constexpr int ks = kv_scale(nb), kd = kv_dot(nb), kn = kv_norm(nb), km = kv_mulm(nb, W),
+                          kk = kv_make(nb, W);
+            if constexpr (k >= ks && k < ks + 4) {                // SCALE {A X C S}
+                Vf<P> s;
+                if constexpr (k == ks) s = a.F[0];
+                else if constexpr (k == ks + 1) s = io.X(arg);
+                else if constexpr (k == ks + 2) s = io.C(arg);
+                else s = io.template S<1>(SF, arg, 0);
+#pragma unroll
+                for (int c = 0; c < W; ++c) A[c] = A[c] * s;
+            } else if constexpr (k >= kd && k < kd + 3) {         // DOT {X C S} -> A_F
+                Vf<P> b[W];
+                fetch<P, W, k - kd>(b, io, t, arg);
+                if constexpr (W == 2) a.F[0] = dot2(A, b); else a.F[0] = dot3(A, b);
+            } else if constexpr (k == kn) {                       // NORM -> A_F
+                unary_prefix<P, W>(A, io, t, arg);
+                if constexpr (W == 2) a.F[0] = norm2(A); else a.F[0] = norm3(A);
+            } else if constexpr (k > kn && k <= kn + W) {         // GET x/y/z -> A_F
+                unary_prefix<P, W>(A, io, t, arg);
+                a.F[0] = A[k - kn - 1];
+            } else if constexpr (k >= km && k < km + 4) {         // MULM {A X C S}: A = M * A
+                constexpr int tm = W == 2 ? SM2 : SM3;
+                constexpr int MW = W * W;
+                if constexpr (((kProfileTypes[PROF] >> tm) & 1u) != 0u || k != km) {
+                    Vf<P> m[MW];
+                    if constexpr (k == km) {
+                        if constexpr (((kProfileTypes[PROF] >> tm) & 1u) != 0u) {
+                            Vf<P> *M = acc_of<PROF, P, tm>(a);
+#pragma unroll
+                            for (int c = 0; c < MW; ++c) m[c] = M[c];
+                        }
+                    } else if constexpr (k == km + 1) {
+                        fetch<P, MW, SRC_X>(m, io, tm, arg);
+                    } else if constexpr (k == km + 2) {
+                        fetch<P, MW, SRC_C>(m, io, tm, arg);
+                    } else {
+                        fetch<P, MW, SRC_S>(m, io, tm, arg);
+                    }
+                    if constexpr (W == 2) mul_m2v2(m, A, A); else mul_m3v3(m, A, A);
+                }
+            } else if constexpr (k == kk) {                       // MAKE from F stack + A_F
+#pragma unroll
+                for (int c = 0; c + 1 < W; ++c) A[c] = io.template S<1>(SF, arg + c, 0);
+                A[W - 1] = a.F[0];
+            }
+        } else {  // M2 / M3
+            constexpr int N = W == 4 ? 2 : 3;
+            constexpr int tv = W == 4 ? SV2 : SV3;
+            if constexpr (k >= KM_SCALE && k < KM_SCALE + 4) {
+                Vf<P> s;
+                if constexpr (k == KM_SCALE) s = a.F[0];
+                else if constexpr (k == KM_SCALE + 1) s = io.X(arg);
+                else if constexpr (k == KM_SCALE + 2) s = io.C(arg);
+                else s = io.template S<1>(SF, arg, 0);
+#pragma unroll
+                for (int c = 0; c < W; ++c) A[c] = A[c] * s;
+            } else if constexpr (k == KM_DET) {
+                unary_prefix<P, W>(A, io, t, arg);
+                if constexpr (N == 2) a.F[0] = det_m2(A); else a.F[0] = det_m3(A);
+            } else if constexpr (k == KM_TRACE) {
+                unary_prefix<P, W>(A, io, t, arg);
+                if constexpr (N == 2) a.F[0] = trace_m2(A); else a.F[0] = trace_m3(A);
+            } else if constexpr (k == KM_TRANSPOSE) {
+                unary_prefix<P, W>(A, io, t, arg);
+                if constexpr (N == 2) transpose_m2(A, A); else transpose_m3(A, A);
+            } else if constexpr (k == KM_INVERSE) {
+                unary_prefix<P, W>(A, io, t, arg);
+                if constexpr (N == 2) inverse_m2(A, A); else inverse_m3(A, A);
+            } else if constexpr (k == KM_MAKE) {                  // columns: stack slots + A_V
+                if constexpr (((kProfileTypes[PROF] >> tv) & 1u) != 0u) {
+                    Vf<P> *V = acc_of<PROF, P, tv>(a);
+#pragma unroll
+                    for (int col = 0; col + 1 < N; ++col)
+#pragma unroll
+                        for (int r = 0; r < N; ++r) A[N * col + r] = io.template S<N>(tv, arg + col, r);
+#pragma unroll
+                    for (int r = 0; r < N; ++r) A[N * (N - 1) + r] = V[r];
+                }
             }
         }
     }
 }
 
-#define RSR_C(K, S) case ((K) << 3) | (S): uop<PROF, P, (K), (S)>(st, io, arg); break;
-#define RSR_K(K) RSR_C(K, 0) RSR_C(K, 1) RSR_C(K, 2) RSR_C(K, 3) RSR_C(K, 4) RSR_C(K, 5) RSR_C(K, 6) RSR_C(K, 7)
+#define RSR_C(K) case (K): acc_op<PROF, P, (K)>(a, io, arg); break;
+#define RSR_C4(K) RSR_C(K) RSR_C(K + 1) RSR_C(K + 2) RSR_C(K + 3)
+#define RSR_C9(K) RSR_C4(K) RSR_C4(K + 4) RSR_C(K + 8)
+#define RSR_C27(K) RSR_C9(K) RSR_C9(K + 9) RSR_C9(K + 18)
 
-// Runs one program (register form) on this lane's P points.  One flat
-// switch over (kind, position); cases of stacks the profile does not hold
-// compile to nothing.
+// Runs one program (accumulator form) on this lane's P points; the result
+// is left in A_F.
 template <int PROF, int P>
-__device__ __forceinline__ void run_program(RegState<PROF, P> &st, const RegIO<P> &io, const uint32_t *code,
+__device__ __forceinline__ void run_program(Acc<PROF, P> &a, const AccIO<P> &io, const uint32_t *code,
                                             uint32_t len) {
     uint32_t w = code[0];
     for (uint32_t pc = 0; pc < len; ++pc) {
         const uint32_t wn = code[pc + 1];
-        const uint32_t arg = w >> 11;
-        switch (w & 0x7FFu) {
-            RSR_K(U_F_LDX) RSR_K(U_F_LDC) RSR_K(U_F_FROM_T0) RSR_K(U_F_TO_T0) RSR_K(U_F_TO_T1) RSR_K(U_F_TO_T2)
-            RSR_K(U_F_ADD) RSR_K(U_F_SUB) RSR_K(U_F_RSUB) RSR_K(U_F_MUL) RSR_K(U_F_DIV) RSR_K(U_F_RDIV)
-            RSR_K(U_F_ADDX) RSR_K(U_F_SUBX) RSR_K(U_F_RSUBX) RSR_K(U_F_MULX) RSR_K(U_F_DIVX) RSR_K(U_F_RDIVX)
-            RSR_K(U_F_ADDC) RSR_K(U_F_SUBC) RSR_K(U_F_RSUBC) RSR_K(U_F_MULC) RSR_K(U_F_DIVC) RSR_K(U_F_RDIVC)
-            RSR_K(U_F_SIN) RSR_K(U_F_COS) RSR_K(U_F_EXP) RSR_K(U_F_SQR) RSR_K(U_F_SQRT) RSR_K(U_F_LN)
-            RSR_K(U_V2_LDX) RSR_K(U_V2_LDC) RSR_K(U_V2_FROM_T) RSR_K(U_V2_TO_T0) RSR_K(U_V2_TO_T2)
-            RSR_K(U_V2_ADD) RSR_K(U_V2_SUB) RSR_K(U_V2_RSUB) RSR_K(U_V2_ADDX) RSR_K(U_V2_SUBX)
-            RSR_K(U_V2_RSUBX) RSR_K(U_V2_ADDC) RSR_K(U_V2_SUBC) RSR_K(U_V2_RSUBC)
-            RSR_K(U_V2_SCALE_T) RSR_K(U_V2_SCALE_X) RSR_K(U_V2_SCALE_C)
-            RSR_K(U_V2_DOT_T) RSR_K(U_V2_DOTX_T) RSR_K(U_V2_DOTC_T) RSR_K(U_V2_NORM_T)
-            RSR_K(U_V2_GETX_T) RSR_K(U_V2_GETY_T) RSR_K(U_V2_MULM_T) RSR_K(U_V2_MULMX) RSR_K(U_V2_MULMC)
-            RSR_K(U_V3_LDX) RSR_K(U_V3_LDC) RSR_K(U_V3_FROM_T) RSR_K(U_V3_TO_T0) RSR_K(U_V3_TO_T3)
-            RSR_K(U_V3_TO_T6) RSR_K(U_V3_ADD) RSR_K(U_V3_SUB) RSR_K(U_V3_RSUB) RSR_K(U_V3_CROSS)
-            RSR_K(U_V3_RCROSS) RSR_K(U_V3_ADDX) RSR_K(U_V3_SUBX) RSR_K(U_V3_RSUBX)
-            RSR_K(U_V3_CROSSX) RSR_K(U_V3_RCROSSX) RSR_K(U_V3_ADDC) RSR_K(U_V3_SUBC)
-            RSR_K(U_V3_RSUBC) RSR_K(U_V3_CROSSC) RSR_K(U_V3_RCROSSC)
-            RSR_K(U_V3_SCALE_T) RSR_K(U_V3_SCALE_X) RSR_K(U_V3_SCALE_C)
-            RSR_K(U_V3_DOT_T) RSR_K(U_V3_DOTX_T) RSR_K(U_V3_DOTC_T) RSR_K(U_V3_NORM_T)
-            RSR_K(U_V3_GETX_T) RSR_K(U_V3_GETY_T) RSR_K(U_V3_GETZ_T)
-            RSR_K(U_V3_MULM_T) RSR_K(U_V3_MULMX) RSR_K(U_V3_MULMC)
-            RSR_K(U_M2_LDX) RSR_K(U_M2_LDC) RSR_K(U_M2_FROM_T) RSR_K(U_M2_TO_T)
-            RSR_K(U_M2_ADD) RSR_K(U_M2_SUB) RSR_K(U_M2_RSUB) RSR_K(U_M2_MUL) RSR_K(U_M2_RMUL)
-            RSR_K(U_M2_ADDX) RSR_K(U_M2_SUBX) RSR_K(U_M2_RSUBX) RSR_K(U_M2_MULX) RSR_K(U_M2_RMULX)
-            RSR_K(U_M2_ADDC) RSR_K(U_M2_SUBC) RSR_K(U_M2_RSUBC) RSR_K(U_M2_MULC) RSR_K(U_M2_RMULC)
-            RSR_K(U_M2_SCALE_T) RSR_K(U_M2_SCALE_X) RSR_K(U_M2_SCALE_C)
-            RSR_K(U_M2_DET_T) RSR_K(U_M2_TRACE_T) RSR_K(U_M2_TRANSPOSE) RSR_K(U_M2_INVERSE)
-            RSR_K(U_M3_LDX) RSR_K(U_M3_LDC) RSR_K(U_M3_FROM_T) RSR_K(U_M3_TO_T)
-            RSR_K(U_M3_ADD) RSR_K(U_M3_SUB) RSR_K(U_M3_RSUB) RSR_K(U_M3_MUL) RSR_K(U_M3_RMUL)
-            RSR_K(U_M3_ADDX) RSR_K(U_M3_SUBX) RSR_K(U_M3_RSUBX) RSR_K(U_M3_MULX) RSR_K(U_M3_RMULX)
-            RSR_K(U_M3_ADDC) RSR_K(U_M3_SUBC) RSR_K(U_M3_RSUBC) RSR_K(U_M3_MULC) RSR_K(U_M3_RMULC)
-            RSR_K(U_M3_SCALE_T) RSR_K(U_M3_SCALE_X) RSR_K(U_M3_SCALE_C)
-            RSR_K(U_M3_DET_T) RSR_K(U_M3_TRACE_T) RSR_K(U_M3_TRANSPOSE) RSR_K(U_M3_INVERSE)
+        const uint32_t arg = w >> 8;
+        switch (w & 0xFFu) {
+            RSR_C27(K_F)                     // F block: 0..26
+            RSR_C27(K_V2)                    // V2 block: 32..58
+            RSR_C27(K_V3) RSR_C4(K_V3 + 27) RSR_C(K_V3 + 31) RSR_C(K_V3 + 32) RSR_C(K_V3 + 33)  // 64..97
+            RSR_C27(K_M2)                    // 104..130
+            RSR_C27(K_M3)                    // 136..162
             default: break;
         }
         w = wn;
     }
 }
 
-#undef RSR_K
+#undef RSR_C27
+#undef RSR_C9
+#undef RSR_C4
 #undef RSR_C
 
 __host__ __device__ __forceinline__ uint32_t align4r(uint32_t v) { return (v + 3u) & ~3u; }
@@ -307,12 +296,16 @@ template <int PROF, int P>
 __global__ void __launch_bounds__(kRegThreads) reg_eval_kernel(const LaunchArgs a) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t region = align4r(a.smem_code_words) + align4r(a.smem_const_floats) + 2u * 32u * kMaxProgsPerWarp;
-    float *base = smem + (size_t)warp * region;
+    float *base = smem + (size_t)warp * a.region_floats;
     uint32_t *scode = reinterpret_cast<uint32_t *>(base);
     float *sconst = base + align4r(a.smem_code_words);
-    float *sacc = sconst + align4r(a.smem_const_floats);  // [g][2][32] Kahan state
+    float *sacc = base + a.acc_off;  // [g][2][32] Kahan state
     __shared__ uint32_t meta[kRegThreads / 32][kMaxProgsPerWarp][3];  // code off, len, const off
+
+    AccIO<P> io;
+#pragma unroll
+    for (int t = 0; t < N_STACKS; ++t) io.stk[t] = reinterpret_cast<Vf<P> *>(base + a.stack_off[t]);
+    io.lane = lane;
 
     for (;;) {
         uint32_t item_id = 0;
@@ -321,7 +314,6 @@ __global__ void __launch_bounds__(kRegThreads) reg_eval_kernel(const LaunchArgs 
         if (item_id >= a.n_items) break;
         const WorkItem it = a.items[item_id];
         const uint32_t G = it.n_progs;
-        // stage the programs of this item
         uint32_t coff = 0, koff = 0;
         for (uint32_t g = 0; g < G; ++g) {
             const ProgDesc pd = a.progs[it.prog_begin + g];
@@ -335,42 +327,42 @@ __global__ void __launch_bounds__(kRegThreads) reg_eval_kernel(const LaunchArgs 
             koff += pd.n_consts;
         }
         __syncwarp();
-        const ProgDesc pd0 = a.progs[it.prog_begin];
-        const DatasetDesc ds = a.datasets[pd0.dataset];
-        RegState<PROF, P> st;
-        RegIO<P> io{ds.x, ds.stride, 0, sconst};
+        const DatasetDesc ds = a.datasets[a.progs[it.prog_begin].dataset];
+        io.x = ds.x;
+        io.stride = ds.stride;
+        Acc<PROF, P> acc;
         for (uint32_t tile = it.tile_begin; tile < it.tile_end; ++tile) {
             io.p0 = (uint64_t)tile * (32u * P) + (uint64_t)lane * P;
             const Vf<P> y = load_pts<P>(ds.y + io.p0);
             for (uint32_t g = 0; g < G; ++g) {
                 io.consts = sconst + meta[warp][g][2];
-                run_program<PROF, P>(st, io, scode + meta[warp][g][0], meta[warp][g][1]);
-                const Vf<P> pred = st.F[0];
+                run_program<PROF, P>(acc, io, scode + meta[warp][g][0], meta[warp][g][1]);
+                const Vf<P> pred = acc.F[0];
                 if (a.mode == MODE_POINTS) {
                     store_pts<P>(a.points_out + (uint64_t)(it.prog_begin + g) * a.points_stride + io.p0, pred, io.p0,
                                  ds.n_eval);
                 } else {
-                    Kahan acc;
-                    acc.s = sacc[(g * 2) * 32 + lane];
-                    acc.c = sacc[(g * 2 + 1) * 32 + lane];
+                    Kahan k;
+                    k.s = sacc[(g * 2) * 32 + lane];
+                    k.c = sacc[(g * 2 + 1) * 32 + lane];
 #pragma unroll
-                    for (int k = 0; k < P; ++k) {
-                        if (io.p0 + k < ds.n_eval) {
-                            const float d = pred.v[k] - y.v[k];
-                            acc.add(d * d);
+                    for (int q = 0; q < P; ++q) {
+                        if (io.p0 + q < ds.n_eval) {
+                            const float d = pred.v[q] - y.v[q];
+                            k.add(d * d);
                         }
                     }
-                    sacc[(g * 2) * 32 + lane] = acc.s;
-                    sacc[(g * 2 + 1) * 32 + lane] = acc.c;
+                    sacc[(g * 2) * 32 + lane] = k.s;
+                    sacc[(g * 2 + 1) * 32 + lane] = k.c;
                 }
             }
         }
         if (a.mode == MODE_MSE) {
             for (uint32_t g = 0; g < G; ++g) {
-                Kahan acc;
-                acc.s = sacc[(g * 2) * 32 + lane];
-                acc.c = sacc[(g * 2 + 1) * 32 + lane];
-                const double s = warp_sum(acc.value());
+                Kahan k;
+                k.s = sacc[(g * 2) * 32 + lane];
+                k.c = sacc[(g * 2 + 1) * 32 + lane];
+                const double s = warp_sum(k.value());
                 if (lane == 0) a.partials[a.progs[it.prog_begin + g].part_off + it.chunk] = s;
             }
         }
@@ -379,39 +371,44 @@ __global__ void __launch_bounds__(kRegThreads) reg_eval_kernel(const LaunchArgs 
 }
 
 // ------------------------------------------------------------- launchers
+// Shared-memory layout of one warp: code | constants | stacks (per type) |
+// Kahan state.  Offsets in floats.
+void reg_layout(uint32_t code_words, uint32_t const_floats, const uint32_t *stack_depth, int P,
+                uint32_t *stack_off, uint32_t *acc_off, uint32_t *region_floats) {
+    uint32_t off = align4r(code_words) + align4r(const_floats);
+    for (int t = 0; t < N_STACKS; ++t) {
+        stack_off[t] = off;
+        off += stack_depth[t] * (uint32_t)kStackWidth[t] * 32u * (uint32_t)P;
+    }
+    *acc_off = off;
+    off += 2u * 32u * kMaxProgsPerWarp;
+    *region_floats = align4r(off);
+}
+
 template <int PROF, int P>
 static cudaError_t launch_reg_pp(const LaunchArgs &a, uint32_t grid, cudaStream_t st) {
     auto k = reg_eval_kernel<PROF, P>;
-    const size_t smem = reg_smem_per_warp(a.smem_code_words, a.smem_const_floats) * (kRegThreads / 32);
+    const size_t smem = (size_t)a.region_floats * 4u * (kRegThreads / 32);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, kRegThreads, smem, st>>>(a);
     return cudaGetLastError();
 }
 
-template <int PROF>
-static cudaError_t launch_reg_prof(const LaunchArgs &a, int P, uint32_t grid, cudaStream_t st) {
-    switch (P) {
-        case 1: return launch_reg_pp<PROF, 1>(a, grid, st);
-        case 2: return launch_reg_pp<PROF, 2>(a, grid, st);
-        default:
-            if constexpr (PROF == P_ALL) return launch_reg_pp<PROF, 2>(a, grid, st);
-            else return launch_reg_pp<PROF, 4>(a, grid, st);
-    }
-}
+// Instantiated points-per-thread values: {2, 4, 8} for the F and F+V3
+// profiles, {2, 4} for the others.
+int reg_max_p(int profile) { return profile == P_F || profile == P_FV3 ? 8 : 4; }
 
 cudaError_t launch_reg(const LaunchArgs &a, int profile, int P, uint32_t grid, cudaStream_t st) {
     switch (profile) {
-        case P_F: return P == 8 ? launch_reg_pp<P_F, 8>(a, grid, st) : launch_reg_prof<P_F>(a, P, grid, st);
-        case P_FV3: return launch_reg_prof<P_FV3>(a, P, grid, st);
-        case P_FV2M2: return launch_reg_prof<P_FV2M2>(a, P, grid, st);
-        case P_FV3M3: return launch_reg_prof<P_FV3M3>(a, P, grid, st);
-        default: return launch_reg_prof<P_ALL>(a, P, grid, st);
+        case P_F: return P >= 8 ? launch_reg_pp<P_F, 8>(a, grid, st) : P >= 4 ? launch_reg_pp<P_F, 4>(a, grid, st)
+                                                                            : launch_reg_pp<P_F, 2>(a, grid, st);
+        case P_FV3: return P >= 8 ? launch_reg_pp<P_FV3, 8>(a, grid, st) : P >= 4 ? launch_reg_pp<P_FV3, 4>(a, grid, st)
+                                                                                : launch_reg_pp<P_FV3, 2>(a, grid, st);
+        case P_FV2M2: return P >= 4 ? launch_reg_pp<P_FV2M2, 4>(a, grid, st) : launch_reg_pp<P_FV2M2, 2>(a, grid, st);
+        case P_FV3M3: return P >= 4 ? launch_reg_pp<P_FV3M3, 4>(a, grid, st) : launch_reg_pp<P_FV3M3, 2>(a, grid, st);
+        default: return P >= 4 ? launch_reg_pp<P_ALL, 4>(a, grid, st) : launch_reg_pp<P_ALL, 2>(a, grid, st);
     }
-}
-
-size_t reg_smem_per_warp(uint32_t code_words, uint32_t const_floats) {
-    return ((size_t)align4r(code_words) + align4r(const_floats) + 2u * 32u * kMaxProgsPerWarp) * 4u;
 }
 
 template <int PROF, int P>
@@ -421,14 +418,13 @@ static int occ(size_t smem) {
     return n;
 }
 
-int reg_max_blocks_per_sm(int profile, int P) {
-    const size_t smem = reg_smem_per_warp(512, 256) * (kRegThreads / 32);
+int reg_max_blocks_per_sm(int profile, int P, size_t smem) {
     switch (profile) {
-        case P_F: return P == 8 ? occ<P_F, 8>(smem) : P == 4 ? occ<P_F, 4>(smem) : P == 2 ? occ<P_F, 2>(smem) : occ<P_F, 1>(smem);
-        case P_FV3: return P >= 4 ? occ<P_FV3, 4>(smem) : P == 2 ? occ<P_FV3, 2>(smem) : occ<P_FV3, 1>(smem);
-        case P_FV2M2: return P >= 4 ? occ<P_FV2M2, 4>(smem) : P == 2 ? occ<P_FV2M2, 2>(smem) : occ<P_FV2M2, 1>(smem);
-        case P_FV3M3: return P >= 4 ? occ<P_FV3M3, 4>(smem) : P == 2 ? occ<P_FV3M3, 2>(smem) : occ<P_FV3M3, 1>(smem);
-        default: return P >= 2 ? occ<P_ALL, 2>(smem) : occ<P_ALL, 1>(smem);
+        case P_F: return P >= 8 ? occ<P_F, 8>(smem) : P >= 4 ? occ<P_F, 4>(smem) : occ<P_F, 2>(smem);
+        case P_FV3: return P >= 8 ? occ<P_FV3, 8>(smem) : P >= 4 ? occ<P_FV3, 4>(smem) : occ<P_FV3, 2>(smem);
+        case P_FV2M2: return P >= 4 ? occ<P_FV2M2, 4>(smem) : occ<P_FV2M2, 2>(smem);
+        case P_FV3M3: return P >= 4 ? occ<P_FV3M3, 4>(smem) : occ<P_FV3M3, 2>(smem);
+        default: return P >= 4 ? occ<P_ALL, 4>(smem) : occ<P_ALL, 2>(smem);
     }
 }
 

@@ -59,11 +59,9 @@ static int log2_bucket(uint64_t n) {
 // thread and programs per warp.
 static TuneChoice default_choice(int profile) {
     switch (profile) {
-        case P_F: return {4, 4};
-        case P_FV3: return {2, 4};
-        case P_FV2M2: return {2, 4};
-        case P_FV3M3: return {1, 4};
-        default: return {1, 4};
+        case P_F: return {8, 4};
+        case P_FV3: return {4, 4};
+        default: return {4, 4};
     }
 }
 
@@ -73,10 +71,11 @@ static TuneChoice choice_for(rsr_ctx *ctx, int profile, uint64_t n_eval) {
     if (it != ctx->tune.end()) c = it->second;
     if (ctx->opts.points_per_thread > 0) c.P = ctx->opts.points_per_thread;
     if (ctx->opts.programs_per_warp > 0) c.G = ctx->opts.programs_per_warp;
-    // variants that exist (kernels_reg.cu)
-    int maxP = profile == P_F ? 8 : (profile == P_FV3M3 || profile == P_ALL) ? 2 : 4;
+    if (ctx->force.P > 0) c = ctx->force;
+    // variants that exist (kernels_reg.cu): P in {2, 4, 8} up to reg_max_p
+    const int maxP = reg_max_p(profile);
     if (c.P > maxP) c.P = maxP;
-    if (c.P != 1 && c.P != 2 && c.P != 4 && c.P != 8) c.P = 1;
+    if (c.P != 2 && c.P != 4 && c.P != 8) c.P = c.P < 2 ? 2 : 4;
     c.G = std::max(1, std::min(c.G, 8));
     return c;
 }
@@ -118,7 +117,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         std::string err;
         int rc = encode_program(pop.code + c0, (uint32_t)(c1 - c0), pop.const_kinds + k0, (uint32_t)(k1 - k0),
                                 pop.params + p0, (uint32_t)(p1 - p0), P.datasets[prog_ds[i]].num_features, &enc[i],
-                                &err);
+                                &err, (ctx->opts.flags & RSR_OPT_NO_LOAD_FUSION) == 0);
         if (rc != RSR_OK) return fail(rc, "program " + std::to_string(i) + ": " + err);
     }
     // path per program: -2 adjoint, -1 plain, >= 0 register profile
@@ -202,6 +201,9 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                 cf += P.progs[q].n_consts;
                 sl = std::max(sl, g.kind == 2 ? P.progs[q].n_tape : P.progs[q].n_slots);
                 len_sum += P.progs[q].uop_len;
+                if (g.kind == 1)
+                    for (int t = 0; t < N_STACKS; ++t)
+                        g.stack_depth[t] = std::max(g.stack_depth[t], (uint32_t)enc[order[q]].depth_fast[t]);
             }
             g.code_words = std::max(g.code_words, cw);
             g.const_floats = std::max(g.const_floats, cf);
@@ -344,7 +346,9 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             uint32_t wpb = (uint32_t)std::max<size_t>(1, std::min<size_t>(kPlainThreads / 32, (200 * 1024) / per));
             e = launch_plain(a, g.P, wpb, per * wpb, st);
         } else if (g.kind == 1) {
-            int bps = std::max(1, reg_max_blocks_per_sm(g.profile, g.P));
+            reg_layout(g.code_words, g.const_floats, g.stack_depth, g.P, a.stack_off, &a.acc_off, &a.region_floats);
+            const size_t smem = (size_t)a.region_floats * 4u * (kRegThreads / 32);
+            int bps = std::max(1, reg_max_blocks_per_sm(g.profile, g.P, smem));
             uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)bps * ctx->num_sms,
                                                          (g.n_items + (kRegThreads / 32) - 1) / (kRegThreads / 32));
             e = launch_reg(a, g.profile, g.P, std::max(1u, grid), st);
@@ -804,6 +808,78 @@ int rsr_synchronize(rsr_ctx *ctx) {
     return e == cudaSuccess ? RSR_OK : cuda_fail(e, "synchronize");
 }
 
+// Autotuner: times every (points per thread, programs per warp) candidate of
+// the register kernel on this population and keeps, per kernel profile and
+// dataset size class, the fastest.  Later plans of the context use it.
+int rsr_autotune(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const rsr_dataset *dsp, int reps,
+                 char *report, size_t report_len) {
+    if (!ctx || !pop) return fail(RSR_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (reps < 1) reps = 3;
+    const int Ps[3] = {2, 4, 8}, Gs[4] = {1, 2, 4, 8};
+    struct Best { float ms = 1e30f; TuneChoice c; int bucket = 0; };
+    std::map<int, Best> best;   // profile -> best
+    std::string rep = "{\"candidates\": [";
+    bool first = true;
+    DevicePlan dev;
+    std::vector<cudaEvent_t> ev;
+    int rc = RSR_OK;
+    for (int P : Ps)
+        for (int G : Gs) {
+            ctx->force = TuneChoice{P, G};
+            Plan plan;
+            rc = build_plan(ctx, *pop, dsp, ds, RSR_KERNEL_BATCHED, false, MODE_MSE, &plan);
+            if (!rc) rc = upload_plan(ctx, plan, &dev, ctx->stream);
+            if (rc) break;
+            while (ev.size() < 2 * plan.groups.size()) {
+                cudaEvent_t e;
+                cudaEventCreate(&e);
+                ev.push_back(e);
+            }
+            std::vector<float> gmin(plan.groups.size(), 1e30f);
+            for (int r = 0; r < reps + 1 && !rc; ++r) {
+                rc = enqueue_plan(ctx, plan, &dev, ctx->stream, nullptr, ev.data());
+                if (!rc && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "autotune");
+                for (size_t g = 0; !rc && r > 0 && g < plan.groups.size(); ++g) {
+                    float t = 0.0f;
+                    if (plan.groups[g].n_items && cudaEventElapsedTime(&t, ev[2 * g], ev[2 * g + 1]) == cudaSuccess)
+                        gmin[g] = std::min(gmin[g], t);
+                }
+            }
+            if (rc) break;
+            for (size_t g = 0; g < plan.groups.size(); ++g) {
+                const Group &gr = plan.groups[g];
+                if (gr.kind != 1 || !gr.n_items) continue;
+                uint64_t max_eval = 0;
+                for (uint32_t i = gr.item_begin; i < gr.item_begin + gr.n_items; ++i)
+                    max_eval = std::max(max_eval, plan.datasets[plan.progs[plan.items[i].prog_begin].dataset].n_eval);
+                Best &b = best[gr.profile];
+                if (gmin[g] < b.ms) { b.ms = gmin[g]; b.c = TuneChoice{gr.P, gr.G}; b.bucket = log2_bucket(max_eval); }
+                rep += std::string(first ? "" : ", ") + "{\"profile\": " + std::to_string(gr.profile) +
+                       ", \"P\": " + std::to_string(gr.P) + ", \"G\": " + std::to_string(gr.G) +
+                       ", \"ms\": " + std::to_string(gmin[g]) + "}";
+                first = false;
+            }
+        }
+    ctx->force = TuneChoice{};
+    for (auto &e : ev) cudaEventDestroy(e);
+    dev.pool.release(); dev.partials.release(); dev.out.release(); dev.counters.release();
+    if (rc) return rc;
+    rep += "], \"chosen\": [";
+    first = true;
+    for (auto &kv : best) {
+        ctx->tune[{kv.first, kv.second.bucket}] = kv.second.c;
+        rep += std::string(first ? "" : ", ") + "{\"profile\": " + std::to_string(kv.first) + ", \"P\": " +
+               std::to_string(kv.second.c.P) + ", \"G\": " + std::to_string(kv.second.c.G) + ", \"ms\": " +
+               std::to_string(kv.second.ms) + "}";
+        first = false;
+    }
+    rep += "]}";
+    if (report && report_len) snprintf(report, report_len, "%s", rep.c_str());
+    return RSR_OK;
+}
+
 int rsr_measure_fp32_peak(rsr_ctx *ctx, double *lane_ops_per_s) {
     if (!ctx || !lane_ops_per_s) return fail(RSR_EINVAL, "null argument");
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -820,6 +896,20 @@ int rsr_validate_program(const rsr_program *prog, uint32_t num_features) {
     int rc = encode_program(prog->code, prog->len, prog->const_kinds, prog->n_consts, prog->params, prog->n_params,
                             num_features, &E, &err);
     if (rc) return fail(rc, err);
+    return RSR_OK;
+}
+
+int rsr_program_encoding(const rsr_program *prog, uint32_t num_features, int form, uint32_t *out, uint32_t cap,
+                         uint32_t *len) {
+    if (!prog || !len || (cap && !out)) return fail(RSR_EINVAL, "null argument");
+    EncodedProgram E;
+    std::string err;
+    int rc = encode_program(prog->code, prog->len, prog->const_kinds, prog->n_consts, prog->params, prog->n_params,
+                            num_features, &E, &err);
+    if (rc) return fail(rc, err);
+    const std::vector<uint32_t> &v = form == 0 ? E.slot_code : form == 1 ? E.reg_code : E.tape_code;
+    *len = (uint32_t)v.size();
+    for (uint32_t i = 0; i < cap && i < v.size(); ++i) out[i] = v[i];
     return RSR_OK;
 }
 

@@ -59,6 +59,7 @@ struct Group {
     int G = 1;
     uint32_t item_begin = 0, n_items = 0;  // into the plan's item array
     uint32_t code_words = 0, const_floats = 0, slots = 0;  // per-warp staging maxima
+    uint32_t stack_depth[N_STACKS] = {0, 0, 0, 0, 0};       // register kernel: spill slots per type
     uint32_t grid = 0;
     size_t smem = 0;
     uint32_t warps_per_block = 0;
@@ -109,6 +110,7 @@ struct rsr_ctx {
     uint64_t next_handle = 1;
     uint64_t mem_in_use = 0;
     std::map<std::pair<int, int>, rsr::TuneChoice> tune;  // (profile, log2 points) -> choice
+    rsr::TuneChoice force;     // set while the autotuner measures a candidate
     rsr::DevicePlan scratch;   // for one-shot calls
     void *pinned = nullptr;
     size_t pinned_cap = 0;

@@ -13,15 +13,24 @@
 //       w1 = out_slot | in0_slot << 16
 //       w2 = in1_slot | in2_slot << 16
 //
-//  * Register form, for the register-stack kernel.  The expression tree that
-//    produces the result is re-emitted with its subtrees evaluated in the order
-//    that needs the fewest stack slots (values are pure, so every value is
-//    bit-identical to the reference's); leaf loads are fused into their
-//    consumer; cross-stack operands move through transfer registers T[0..8].
-//    One word per micro-op:
-//       bits 0-2 stack position, bits 3-10 micro-op kind, bits 11-31 argument.
+//  * Accumulator form, for the register (batched) kernel.  Each value type
+//    has one accumulator register set (A_F, A_V2, A_V3, A_M2, A_M3), P data
+//    points wide; every micro-op reads and writes accumulators, and a value
+//    that must wait while a sibling subtree is evaluated is pushed to a
+//    per-type stack in shared memory at a slot fixed by the encoder.  Leaf
+//    operands (features, constants) are fused into the consuming op.  Sibling
+//    subtrees are evaluated largest first; values are pure, so every result is
+//    bit-identical to the reference's.  One word per micro-op:
+//       bits 0-7 micro-op kind, bits 8-31 argument (feature offset, flat
+//       param offset or stack slot).
 #pragma once
 #include <stdint.h>
+
+#if defined(__CUDACC__)
+#define RSR_HD __host__ __device__
+#else
+#define RSR_HD
+#endif
 
 namespace rsr {
 
@@ -46,65 +55,62 @@ enum Stack : int { SF = 0, SV2 = 1, SV3 = 2, SM2 = 3, SM3 = 4, N_STACKS = 5 };
 static constexpr int kStackWidth[N_STACKS] = {1, 2, 3, 4, 9};
 static constexpr int kRefStackSlots = 32;
 
-// ----------------------------------------------------- register micro-ops
-// Argument source suffixes: S = stack position s+1, X = feature, C = constant.
-enum UopKind : uint8_t {
-    // F stack
-    U_F_LDX = 0, U_F_LDC, U_F_FROM_T0, U_F_TO_T0, U_F_TO_T1, U_F_TO_T2,
-    U_F_ADD, U_F_SUB, U_F_RSUB, U_F_MUL, U_F_DIV, U_F_RDIV,
-    U_F_ADDX, U_F_SUBX, U_F_RSUBX, U_F_MULX, U_F_DIVX, U_F_RDIVX,
-    U_F_ADDC, U_F_SUBC, U_F_RSUBC, U_F_MULC, U_F_DIVC, U_F_RDIVC,
-    U_F_SIN, U_F_COS, U_F_EXP, U_F_SQR, U_F_SQRT, U_F_LN,
-    // V2 stack
-    U_V2_LDX = 32, U_V2_LDC, U_V2_FROM_T, U_V2_TO_T0, U_V2_TO_T2,
-    U_V2_ADD, U_V2_SUB, U_V2_RSUB, U_V2_ADDX, U_V2_SUBX, U_V2_RSUBX, U_V2_ADDC, U_V2_SUBC, U_V2_RSUBC,
-    U_V2_SCALE_T, U_V2_SCALE_X, U_V2_SCALE_C,
-    U_V2_DOT_T, U_V2_DOTX_T, U_V2_DOTC_T, U_V2_NORM_T, U_V2_GETX_T, U_V2_GETY_T,
-    U_V2_MULM_T, U_V2_MULMX, U_V2_MULMC,
-    // V3 stack
-    U_V3_LDX = 64, U_V3_LDC, U_V3_FROM_T, U_V3_TO_T0, U_V3_TO_T3, U_V3_TO_T6,
-    U_V3_ADD, U_V3_SUB, U_V3_RSUB, U_V3_CROSS, U_V3_RCROSS,
-    U_V3_ADDX, U_V3_SUBX, U_V3_RSUBX, U_V3_CROSSX, U_V3_RCROSSX,
-    U_V3_ADDC, U_V3_SUBC, U_V3_RSUBC, U_V3_CROSSC, U_V3_RCROSSC,
-    U_V3_SCALE_T, U_V3_SCALE_X, U_V3_SCALE_C,
-    U_V3_DOT_T, U_V3_DOTX_T, U_V3_DOTC_T, U_V3_NORM_T, U_V3_GETX_T, U_V3_GETY_T, U_V3_GETZ_T,
-    U_V3_MULM_T, U_V3_MULMX, U_V3_MULMC,
-    // M2 stack
-    U_M2_LDX = 104, U_M2_LDC, U_M2_FROM_T, U_M2_TO_T,
-    U_M2_ADD, U_M2_SUB, U_M2_RSUB, U_M2_MUL, U_M2_RMUL,
-    U_M2_ADDX, U_M2_SUBX, U_M2_RSUBX, U_M2_MULX, U_M2_RMULX,
-    U_M2_ADDC, U_M2_SUBC, U_M2_RSUBC, U_M2_MULC, U_M2_RMULC,
-    U_M2_SCALE_T, U_M2_SCALE_X, U_M2_SCALE_C,
-    U_M2_DET_T, U_M2_TRACE_T, U_M2_TRANSPOSE, U_M2_INVERSE,
-    // M3 stack
-    U_M3_LDX = 136, U_M3_LDC, U_M3_FROM_T, U_M3_TO_T,
-    U_M3_ADD, U_M3_SUB, U_M3_RSUB, U_M3_MUL, U_M3_RMUL,
-    U_M3_ADDX, U_M3_SUBX, U_M3_RSUBX, U_M3_MULX, U_M3_RMULX,
-    U_M3_ADDC, U_M3_SUBC, U_M3_RSUBC, U_M3_MULC, U_M3_RMULC,
-    U_M3_SCALE_T, U_M3_SCALE_X, U_M3_SCALE_C,
-    U_M3_DET_T, U_M3_TRACE_T, U_M3_TRANSPOSE, U_M3_INVERSE,
-    U_END = 168
-};
+// --------------------------------------------------- accumulator micro-ops
+// Sources of the second operand: X feature, C constant, S shared-memory stack
+// slot, A the accumulator of the operand's own type.
+enum AccSrc : int { SRC_X = 0, SRC_C = 1, SRC_S = 2 };
+// Binary operations on one type: a = a op b, R-forms b op a.
+enum AccBin : int { BIN_ADD = 0, BIN_SUB, BIN_RSUB, BIN_MUL, BIN_DIV, BIN_RDIV, BIN_CROSS, BIN_RCROSS,
+                    BIN_MMUL, BIN_RMMUL };
 
-static inline constexpr uint32_t uop_word(uint32_t kind, uint32_t slot, uint32_t arg) {
-    return (slot & 0x7u) | ((kind & 0xFFu) << 3) | (arg << 11);
+// Kind numbering: one block per accumulator type.
+//   F  (base 0):   LDX LDC PUSH, {ADD SUB RSUB MUL DIV RDIV} x {X C S}, SIN COS EXP SQR SQRT LN
+//   V2 (base 32):  LDX LDC PUSH, {ADD SUB RSUB} x {X C S}, SCALE{A X C S}, DOT{X C S}, NORM GETX GETY,
+//                  MULM{A X C S}, MAKE
+//   V3 (base 64):  LDX LDC PUSH, {ADD SUB RSUB CROSS RCROSS} x {X C S}, SCALE{A X C S}, DOT{X C S},
+//                  NORM GETX GETY GETZ, MULM{A X C S}, MAKE
+//   M2 (base 104), M3 (base 136): LDX LDC PUSH, {ADD SUB RSUB MUL RMUL} x {X C S}, SCALE{A X C S},
+//                  DET TRACE TRANSPOSE INVERSE, MAKE
+enum AccKind : int {
+    K_F = 0, K_F_LDX = 0, K_F_LDC = 1, K_F_PUSH = 2, K_F_BIN = 3, K_F_UN = 21, K_F_END = 27,
+    K_V2 = 32, K_V3 = 64, K_M2 = 104, K_M3 = 136, K_END = 163,
+    // offsets within the V2 / V3 blocks
+    KV_LDX = 0, KV_LDC = 1, KV_PUSH = 2, KV_BIN = 3,
+    // offsets within the M blocks
+    KM_LDX = 0, KM_LDC = 1, KM_PUSH = 2, KM_BIN = 3, KM_SCALE = 18, KM_DET = 22, KM_TRACE = 23,
+    KM_TRANSPOSE = 24, KM_INVERSE = 25, KM_MAKE = 26,
+};
+// number of binary ops in each block
+static constexpr int kBinOps[5] = {6, 3, 5, 5, 5};
+static constexpr int kBlockBase[5] = {K_F, K_V2, K_V3, K_M2, K_M3};
+// V-block offsets after the binary ops
+RSR_HD static constexpr int kv_scale(int nbin) { return KV_BIN + 3 * nbin; }       // 4 kinds: A X C S
+RSR_HD static constexpr int kv_dot(int nbin) { return kv_scale(nbin) + 4; }        // 3 kinds: X C S
+RSR_HD static constexpr int kv_norm(int nbin) { return kv_dot(nbin) + 3; }         // NORM, GETX, GETY[, GETZ]
+RSR_HD static constexpr int kv_mulm(int nbin, int w) { return kv_norm(nbin) + 1 + w; }  // 4 kinds: A X C S
+RSR_HD static constexpr int kv_make(int nbin, int w) { return kv_mulm(nbin, w) + 4; }
+
+RSR_HD static inline constexpr uint32_t uop_word(uint32_t kind, uint32_t arg) { return (kind & 0xFFu) | (arg << 8); }
+
+// Fused loads.  A unary op (F unary, NORM/GET, DET/TRACE/TRANSPOSE/INVERSE)
+// may first load its operand, and a PUSH may be followed by a load:
+//   unary arg:  bits 0-11 feature or param offset, bits 12-13 load first
+//               (0 none, 1 feature, 2 constant)
+//   PUSH arg:   bits 0-3 slot, bits 4-6 then load into accumulator type
+//               (0 none, 1 + type), bit 7 constant (else feature),
+//               bits 8-19 offset
+static constexpr uint32_t kLdOffsetBits = 12;
+RSR_HD static inline constexpr uint32_t unary_load_arg(uint32_t off, uint32_t src1) { return off | (src1 << 12); }
+RSR_HD static inline constexpr uint32_t push_load_arg(uint32_t slot, uint32_t type1, uint32_t is_const, uint32_t off) {
+    return slot | (type1 << 4) | (is_const << 7) | (off << 8);
 }
-static constexpr int kMaxRegSlots = 8;
 
-// Register-stack kernel profiles: which stacks are held in registers and how
-// many positions each has.  A program runs on the first profile it fits.
-struct ProfileCaps {
-    int cap[N_STACKS];
-    int n_transfer;   // transfer registers T[0..n)
-};
+// Register-kernel profiles: the accumulator types a kernel instance holds.
 enum Profile : int { P_F = 0, P_FV3 = 1, P_FV2M2 = 2, P_FV3M3 = 3, P_ALL = 4, N_PROFILES = 5 };
-static constexpr ProfileCaps kProfiles[N_PROFILES] = {
-    {{8, 0, 0, 0, 0}, 1},
-    {{8, 0, 4, 0, 0}, 3},
-    {{6, 3, 0, 3, 0}, 4},
-    {{6, 0, 3, 0, 2}, 9},
-    {{6, 2, 3, 2, 2}, 9},
-};
+static constexpr uint32_t kProfileTypes[N_PROFILES] = {
+    1u << SF, (1u << SF) | (1u << SV3), (1u << SF) | (1u << SV2) | (1u << SM2), (1u << SF) | (1u << SV3) | (1u << SM3),
+    0x1Fu};
+static constexpr int kMaxAccStack = 16;   // shared-memory stack slots per type
 
 // Program descriptor for the kernels (one per program in a launch).
 struct ProgDesc {

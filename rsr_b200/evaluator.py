@@ -65,7 +65,8 @@ class Engine:
     """One context on one GPU (rsr_ctx)."""
 
     def __init__(self, device: int = 0, kernel: int = N.KERNEL_AUTO, points_per_thread: int = 0,
-                 programs_per_warp: int = 0, use_graphs: bool = True, mem_budget_bytes: int = 0):
+                 programs_per_warp: int = 0, use_graphs: bool = True, mem_budget_bytes: int = 0,
+                 flags: int = 0):
         L = N.lib()
         opts = N.Options()
         L.rsr_options_default(C.byref(opts))
@@ -74,10 +75,11 @@ class Engine:
         opts.programs_per_warp = programs_per_warp
         opts.use_graphs = 1 if use_graphs else 0
         opts.mem_budget_bytes = mem_budget_bytes
+        opts.flags = flags
         ctx = C.c_void_p()
         N.check(L.rsr_ctx_create(device, C.byref(opts), C.byref(ctx)))
         self.ctx = ctx
-        self._cache: Dict[int, DeviceDataset] = {}
+        self._cache: Dict[int, tuple] = {}
 
     def close(self) -> None:
         if self.ctx:
@@ -92,16 +94,19 @@ class Engine:
 
     # ------------------------------------------------------------ datasets
     def upload(self, ds: Dataset) -> DeviceDataset:
+        # cache by object identity; the entry keeps the Dataset alive so its
+        # id() cannot be reused by another object
         key = id(ds)
-        if key in self._cache and self._cache[key].handle:
-            return self._cache[key]
+        hit = self._cache.get(key)
+        if hit is not None and hit[0] is ds and hit[1].handle:
+            return hit[1]
         ff = np.ascontiguousarray(ds.feature_flat, np.float32)
         tb = np.ascontiguousarray(ds.target_batches, np.float32)
         h = C.c_uint64()
         N.check(N.lib().rsr_dataset_upload(self.ctx, ff.ctypes.data, tb.ctypes.data, ds.num_features,
                                            ds.num_batches, ds.num_samples, C.byref(h)))
         d = DeviceDataset(self, h.value, ds.num_features, ds.num_batches, ds.num_samples)
-        self._cache[key] = d
+        self._cache[key] = (ds, d)
         return d
 
     def _ds(self, ds) -> DeviceDataset:
@@ -185,6 +190,17 @@ class Engine:
         N.check(N.lib().rsr_ctx_last_transfer(self.ctx, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    def autotune(self, programs: PopulationLike, dataset=None, datasets=None, reps: int = 3) -> dict:
+        """Times the register kernel's launch shapes on this population and
+        keeps the fastest for later calls on this engine."""
+        pk = _packed(programs)
+        s, keep = _as_population(pk)
+        h, dsp = self._handles(pk.n, dataset, datasets)
+        buf = C.create_string_buffer(1 << 16)
+        N.check(N.lib().rsr_autotune(self.ctx, C.byref(s), h, dsp.ctypes.data if dsp is not None else None, reps,
+                                     buf, len(buf)))
+        return json.loads(buf.value.decode())
+
     def launch_count(self) -> int:
         return int(N.lib().rsr_ctx_launch_count(self.ctx))
 
@@ -264,3 +280,14 @@ def analyze(program: Program, num_features: int = 0) -> dict:
     return {"depth_ref": list(info.depth_ref), "depth_fast": list(info.depth_fast),
             "n_uops_fast": info.n_uops_fast, "n_uops_plain": info.n_uops_plain,
             "fast_profile": info.fast_profile, "flops_per_point": info.flops_per_point}
+
+
+def encoding(program: Program, num_features: int = 0, form: int = 1) -> np.ndarray:
+    """Device encoding of a program (0 slot form, 1 accumulator form, 2 tape form)."""
+    s, keep = _as_program(program)
+    n = C.c_uint32()
+    N.check(N.lib().rsr_program_encoding(C.byref(s), num_features, form, None, 0, C.byref(n)))
+    out = np.zeros(max(1, n.value), np.uint32)
+    N.check(N.lib().rsr_program_encoding(C.byref(s), num_features, form, out.ctypes.data, n.value, C.byref(n)))
+    return out[:n.value]
+

@@ -61,8 +61,10 @@ def test_points_bit_identical_all_tile_shapes(ppt, ppw):
                 assert same_bits(got[i], want[i]), (wl, ppt, ppw, i)
 
 
-def check_mse(got, m64):
-    bad = ~np.isfinite(m64) | (m64 > FMAX)
+def check_mse(got, m64, num_samples):
+    # the reference accumulates in f32: a sum of squared errors above f32::MAX
+    # overflows there and the fitness becomes f32::MAX (evaluator.rs:172-173)
+    bad = ~np.isfinite(m64) | (m64 * float(num_samples) > FMAX)
     assert np.array_equal(got[bad], np.full(bad.sum(), FMAX, f32))
     ok = ~bad
     rel = np.abs(got[ok].astype(np.float64) - m64[ok]) / np.maximum(np.abs(m64[ok]), 1e-30)
@@ -75,7 +77,7 @@ def test_mse_within_1e6_of_fp64_oracle(engine, wl, kernel):
     ds, pop = WORKLOADS[wl][0](), WORKLOADS[wl][1]()
     got = engine.compute_mse_batch(pop, ds, kernel=kernel)
     m64, _ = O.mse_batch(I.pack(pop), ds)
-    check_mse(got, m64)
+    check_mse(got, m64, ds.num_samples)
 
 
 @pytest.mark.parametrize("name", sorted(PR.kat_cases().keys()))
@@ -119,7 +121,7 @@ def test_edge_programs(engine):
         for i in range(len(progs)):
             assert same_bits(got[i], want[i]), (k, i)
         m64, _ = O.mse_batch(I.pack(progs), ds)
-        check_mse(engine.compute_mse_batch(progs, ds, kernel=k), m64)
+        check_mse(engine.compute_mse_batch(progs, ds, kernel=k), m64, ds.num_samples)
 
 
 def test_tiny_and_ragged_datasets(engine):
@@ -128,7 +130,7 @@ def test_tiny_and_ragged_datasets(engine):
         ds = W.scalar_dataset(n, seed=n)
         m64, _ = O.mse_batch(I.pack(pop), ds)
         for k in (N.KERNEL_PLAIN, N.KERNEL_AUTO):
-            check_mse(engine.compute_mse_batch(pop, ds, kernel=k), m64)
+            check_mse(engine.compute_mse_batch(pop, ds, kernel=k), m64, ds.num_samples)
 
 
 def test_empty_population(engine):
@@ -141,34 +143,45 @@ def test_reference_drop_ins(engine):
     for p in W.lorentz_population(10, seed=42):
         m = engine.compute_mse(p, ds)
         m64 = O.mse_f64(p, ds)
-        check_mse(np.array([m], f32), np.array([m64]))
+        check_mse(np.array([m], f32), np.array([m64]), ds.num_samples)
         assert same_bits(engine.eval_points(p, ds), O.eval_points(p, ds))
 
 
-def grad_ok(g, ref, tol=1e-3):
-    scale = max(float(np.abs(ref).max()), 1e-4)
-    return float(np.abs(g - ref).max()) <= tol * scale
+def grad_ok(g, ref, mse, tol=1e-3, noise=0.0):
+    """|g - ref| <= tol * scale + noise.  scale = max(|ref|_inf, 1e-4 sqrt(MSE)):
+    a gradient far below the loss's own scale is rounding noise (e.g. the
+    derivative of a cross product of parallel vectors), where relative error
+    means nothing."""
+    scale = max(float(np.abs(ref).max()), 1e-4 * float(np.sqrt(max(mse, 0.0))), 1e-12)
+    return float(np.abs(g - ref).max()) <= tol * scale + noise
+
+
+def fd_noise(p, ds, h=1e-3):
+    """Noise and truncation estimate of the central difference: how far the
+    estimates at steps h and 2h disagree (large where cancellation inside
+    the program makes the f32 loss noisy in a parameter)."""
+    return 2.0 * float(np.abs(O.grad_fd(p, ds, h) - O.grad_fd(p, ds, 2 * h)).max())
 
 
 def test_gradient_vs_finite_differences_and_dual():
     ds = W.transform_dataset(3000, seed=51)
-    pop = W.transform_population(40, seed=52)
+    pop = W.transform_population(60, seed=52)
     with Engine() as e:
         mse, grad = e.compute_mse_grad_batch(pop, ds)
     checked = 0
     for i, p in enumerate(pop):
         n = min(32, p.param_count())
         m64 = O.mse_f64(p, ds)
-        check_mse(mse[i:i + 1], np.array([m64]))
+        check_mse(mse[i:i + 1], np.array([m64]), ds.num_samples)
         md, gd = O.mse_grad_dual(p, ds)
         if not (np.isfinite(gd).all() and md < 1e4):
             continue
         fd = O.grad_fd(p, ds, 1e-3)
-        assert grad_ok(grad[i, :n], gd[:n]), (i, grad[i, :n], gd[:n])
-        assert grad_ok(grad[i, :n], fd[:n], 2e-2), (i, grad[i, :n], fd[:n])  # FD truncation error at h=1e-3
+        assert grad_ok(grad[i, :n], gd[:n], m64), (i, grad[i, :n], gd[:n])
+        assert grad_ok(grad[i, :n], fd[:n], m64, noise=fd_noise(p, ds)), (i, grad[i, :n], fd[:n])
         assert np.all(grad[i, n:] == 0)
         checked += 1
-    assert checked >= 20
+    assert checked >= 25
 
 
 def test_gradient_all_op_kinds():
@@ -181,14 +194,15 @@ def test_gradient_all_op_kinds():
             m, g = e.compute_mse_with_gradient(p, ds)
             md, gd = O.mse_grad_dual(p, ds)
             n = min(32, p.param_count())
+            m64 = O.mse_f64(p, ds)
             if name in ("InverseM2", "InverseM3"):
                 fd = O.grad_fd(p, ds, 1e-3)   # the reference's dual skips inverses
-                assert grad_ok(g[:n], fd[:n], 5e-2), (name, g[:n], fd[:n])
+                assert grad_ok(g[:n], fd[:n], m64, noise=fd_noise(p, ds)), (name, g[:n], fd[:n])
                 continue
             if not np.isfinite(gd[:n]).all():
                 assert not np.isfinite(g[:n]).all(), name
                 continue
-            assert grad_ok(g[:n], gd[:n]), (name, g[:n], gd[:n])
+            assert grad_ok(g[:n], gd[:n], m64), (name, g[:n], gd[:n])
 
 
 def test_alone_and_in_the_mix_identical(engine):
@@ -207,7 +221,7 @@ def test_multi_dataset_batch(engine):
     which = [dss[i % len(dss)] for i in range(len(pop))]
     got = engine.compute_mse_batch(pop, datasets=which)
     for i, p in enumerate(pop):
-        check_mse(got[i:i + 1], np.array([O.mse_f64(p, which[i])]))
+        check_mse(got[i:i + 1], np.array([O.mse_f64(p, which[i])]), which[i].num_samples)
 
 
 def test_prepared_batch_graph_replay(engine):
@@ -255,4 +269,4 @@ def test_full_size_vector_workload_properties():
     assert rel.max() <= 2e-6
     idx = np.arange(0, 4096, 64)
     m64, _ = O.mse_batch(I.pack([pop[i] for i in idx]), ds)
-    check_mse(fast[idx], m64)
+    check_mse(fast[idx], m64, ds.num_samples)
