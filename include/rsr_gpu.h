@@ -143,6 +143,21 @@ RSR_API int rsr_eval_mse_grad_batch(rsr_ctx *ctx, const rsr_population *pop, rsr
 /* eval_simd over every batch for each program: out[i*num_batches*8 + j]. */
 RSR_API int rsr_eval_points_batch(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, int kernel, float *out);
 
+/* ----------------------------------------------------- constant fitting */
+typedef struct rsr_fit_stats {
+    uint32_t iterations;            /* L-BFGS iterations taken by the slowest program */
+    uint32_t gradient_evaluations;  /* batched gradient launches */
+    uint32_t mse_evaluations;       /* batched line-search launches */
+} rsr_fit_stats;
+/* run_lbfgs (src/engine/optimize/lbfgs.rs:9-165) for a whole population:
+ * up to max_iterations L-BFGS steps per program (memory 6, at most 32
+ * parameters, Armijo backtracking c1 = 1e-4 with up to 11 halvings, stop at
+ * |grad| < 1e-5), gradients from the adjoint kernel, line-search MSEs from
+ * the register kernel.  params_out (same layout as pop->params) receives the
+ * fitted constants, mse_out[i] the final fitness of program i. */
+RSR_API int rsr_fit_lbfgs(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const rsr_dataset *ds_per_program,
+                          uint32_t max_iterations, float *params_out, float *mse_out, rsr_fit_stats *stats);
+
 /* -------------------------------------------------- prepared batches */
 /* A population encoded and uploaded once, then run many times with inputs
  * resident on the device (the timed unit of the benchmark).  run() enqueues

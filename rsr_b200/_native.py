@@ -43,6 +43,10 @@ class Options(C.Structure):
                 ("tune_cache_path", C.c_char_p), ("flags", C.c_uint32)]
 
 
+class FitStats(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("gradient_evaluations", C.c_uint32), ("mse_evaluations", C.c_uint32)]
+
+
 class ProgramInfo(C.Structure):
     _fields_ = [("depth_ref", C.c_uint32 * 5), ("depth_fast", C.c_uint32 * 5), ("n_uops_fast", C.c_uint32),
                 ("n_uops_plain", C.c_uint32), ("fast_profile", C.c_int32), ("flops_per_point", C.c_uint32)]
@@ -72,6 +76,8 @@ _SIGS = {
     "rsr_eval_mse_grad_batch": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_void_p,
                                           C.c_void_p]),
     "rsr_eval_points_batch": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_int, C.c_void_p]),
+    "rsr_fit_lbfgs": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p,
+                                C.c_void_p, C.POINTER(FitStats)]),
     "rsr_batch_prepare": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_int, C.c_int,
                                     C.POINTER(C.c_void_p)]),
     "rsr_batch_run": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -22,6 +22,7 @@ struct LaunchArgs {
     uint64_t points_stride;   // MODE_POINTS: floats between consecutive programs
     uint32_t *item_counter;   // persistent kernels: next work item
     uint32_t *status;         // sticky error flags (bit 0: bad micro-op)
+    const uint8_t *active;    // optional per-program mask (launch order): 0 = skip
     uint32_t n_items;
     uint32_t mode;
     uint32_t smem_code_words; // per warp
@@ -29,7 +30,8 @@ struct LaunchArgs {
     uint32_t smem_slots;      // per warp (slot-file kernels)
     uint32_t progs_per_warp;
     // register kernel: per-warp shared-memory layout (floats)
-    uint32_t region_floats;
+    uint32_t region_floats;   // per warp
+    uint32_t block_hdr_floats;
     uint32_t acc_off;
     uint32_t stack_off[N_STACKS];
 };

@@ -324,6 +324,7 @@ __global__ void __launch_bounds__(kGradThreads) grad_kernel(const LaunchArgs a) 
     Vf<P> *adj = val + (size_t)a.smem_slots * 32u;
 
     const WorkItem it = a.items[item_id];
+    if (a.active && !a.active[it.prog_begin]) return;
     const ProgDesc pd = a.progs[it.prog_begin];
     const DatasetDesc ds = a.datasets[pd.dataset];
     for (uint32_t i = lane; i < pd.uop_len; i += 32) scode[i] = __ldg(a.code + pd.uop_off + i);

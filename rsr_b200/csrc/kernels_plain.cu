@@ -130,6 +130,7 @@ __global__ void __launch_bounds__(kPlainThreads) plain_eval_kernel(const LaunchA
     const WorkItem it = a.items[item_id];
     for (uint32_t g = 0; g < it.n_progs; ++g) {
         const uint32_t pid = it.prog_begin + g;
+        if (a.active && !a.active[pid]) continue;
         const ProgDesc pd = a.progs[pid];
         const DatasetDesc ds = a.datasets[pd.dataset];
         stage_program(scode, sconst, a, pd, lane);

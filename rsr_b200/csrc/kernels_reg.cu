@@ -292,51 +292,70 @@ __host__ __device__ __forceinline__ uint32_t align4r(uint32_t v) { return (v + 3
 
 constexpr uint32_t kMaxProgsPerWarp = 8;
 
+// Block-cooperative item loop.  All warps of a block run the same programs
+// (one work item) on different tiles of the item's chunk, so the SM's
+// instruction cache holds one program's case bodies instead of one per warp.
+// Per-warp Kahan sums are reduced across warps in a fixed order.
+//
+// Shared memory: block header (code | constants | meta | cross-warp sums)
+// then one region per warp (spill stacks | Kahan state).
 template <int PROF, int P>
 __global__ void __launch_bounds__(kRegThreads) reg_eval_kernel(const LaunchArgs a) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float *base = smem + (size_t)warp * a.region_floats;
-    uint32_t *scode = reinterpret_cast<uint32_t *>(base);
-    float *sconst = base + align4r(a.smem_code_words);
-    float *sacc = base + a.acc_off;  // [g][2][32] Kahan state
-    __shared__ uint32_t meta[kRegThreads / 32][kMaxProgsPerWarp][3];  // code off, len, const off
+    const int nw = blockDim.x >> 5;
+    uint32_t *scode = reinterpret_cast<uint32_t *>(smem);
+    float *sconst = smem + align4r(a.smem_code_words);
+    uint32_t *meta = reinterpret_cast<uint32_t *>(sconst + align4r(a.smem_const_floats));  // [g][3], [24] item
+    double *red = reinterpret_cast<double *>(meta + 32);                                  // [warp][g]
+    float *wbase = smem + a.block_hdr_floats + (size_t)warp * a.region_floats;
+    float *sacc = wbase + a.acc_off;  // [g][2][32] Kahan state of this warp
 
     AccIO<P> io;
 #pragma unroll
-    for (int t = 0; t < N_STACKS; ++t) io.stk[t] = reinterpret_cast<Vf<P> *>(base + a.stack_off[t]);
+    for (int t = 0; t < N_STACKS; ++t) io.stk[t] = reinterpret_cast<Vf<P> *>(wbase + a.stack_off[t]);
     io.lane = lane;
 
     for (;;) {
-        uint32_t item_id = 0;
-        if (lane == 0) item_id = atomicAdd(a.item_counter, 1u);
-        item_id = __shfl_sync(0xffffffffu, item_id, 0);
+        if (threadIdx.x == 0) meta[24] = atomicAdd(a.item_counter, 1u);
+        __syncthreads();
+        const uint32_t item_id = meta[24];
         if (item_id >= a.n_items) break;
         const WorkItem it = a.items[item_id];
         const uint32_t G = it.n_progs;
-        uint32_t coff = 0, koff = 0;
+        if (threadIdx.x == 0) {
+            uint32_t coff = 0, koff = 0;
+            for (uint32_t g = 0; g < G; ++g) {
+                const ProgDesc pd = a.progs[it.prog_begin + g];
+                meta[3 * g] = coff;
+                meta[3 * g + 1] = pd.uop_len;
+                meta[3 * g + 2] = koff;
+                scode[coff + pd.uop_len] = 0u;  // prefetch pad
+                coff += pd.uop_len + 1;
+                koff += pd.n_consts;
+            }
+        }
+        __syncthreads();
         for (uint32_t g = 0; g < G; ++g) {
             const ProgDesc pd = a.progs[it.prog_begin + g];
-            for (uint32_t i = lane; i < pd.uop_len; i += 32) scode[coff + i] = __ldg(a.code + pd.uop_off + i);
-            if (lane == 0) scode[coff + pd.uop_len] = 0u;  // prefetch pad
-            for (uint32_t i = lane; i < pd.n_consts; i += 32) sconst[koff + i] = __ldg(a.consts + pd.const_off + i);
-            if (lane == 0) { meta[warp][g][0] = coff; meta[warp][g][1] = pd.uop_len; meta[warp][g][2] = koff; }
+            for (uint32_t i = threadIdx.x; i < pd.uop_len; i += blockDim.x) scode[meta[3 * g] + i] = __ldg(a.code + pd.uop_off + i);
+            for (uint32_t i = threadIdx.x; i < pd.n_consts; i += blockDim.x)
+                sconst[meta[3 * g + 2] + i] = __ldg(a.consts + pd.const_off + i);
             sacc[(g * 2) * 32 + lane] = 0.0f;
             sacc[(g * 2 + 1) * 32 + lane] = 0.0f;
-            coff += pd.uop_len + 1;
-            koff += pd.n_consts;
         }
-        __syncwarp();
+        __syncthreads();
         const DatasetDesc ds = a.datasets[a.progs[it.prog_begin].dataset];
         io.x = ds.x;
         io.stride = ds.stride;
         Acc<PROF, P> acc;
-        for (uint32_t tile = it.tile_begin; tile < it.tile_end; ++tile) {
+        for (uint32_t tile = it.tile_begin + warp; tile < it.tile_end; tile += nw) {
             io.p0 = (uint64_t)tile * (32u * P) + (uint64_t)lane * P;
             const Vf<P> y = load_pts<P>(ds.y + io.p0);
             for (uint32_t g = 0; g < G; ++g) {
-                io.consts = sconst + meta[warp][g][2];
-                run_program<PROF, P>(acc, io, scode + meta[warp][g][0], meta[warp][g][1]);
+                if (a.active && !a.active[it.prog_begin + g]) continue;
+                io.consts = sconst + meta[3 * g + 2];
+                run_program<PROF, P>(acc, io, scode + meta[3 * g], meta[3 * g + 1]);
                 const Vf<P> pred = acc.F[0];
                 if (a.mode == MODE_POINTS) {
                     store_pts<P>(a.points_out + (uint64_t)(it.prog_begin + g) * a.points_stride + io.p0, pred, io.p0,
@@ -363,19 +382,27 @@ __global__ void __launch_bounds__(kRegThreads) reg_eval_kernel(const LaunchArgs 
                 k.s = sacc[(g * 2) * 32 + lane];
                 k.c = sacc[(g * 2 + 1) * 32 + lane];
                 const double s = warp_sum(k.value());
-                if (lane == 0) a.partials[a.progs[it.prog_begin + g].part_off + it.chunk] = s;
+                if (lane == 0) red[warp * kMaxProgsPerWarp + g] = s;
+            }
+            __syncthreads();
+            if (threadIdx.x < G) {
+                double s = 0.0;
+                for (int w = 0; w < nw; ++w) s += red[w * kMaxProgsPerWarp + threadIdx.x];
+                a.partials[a.progs[it.prog_begin + threadIdx.x].part_off + it.chunk] = s;
             }
         }
-        __syncwarp();
+        __syncthreads();
     }
 }
 
 // ------------------------------------------------------------- launchers
-// Shared-memory layout of one warp: code | constants | stacks (per type) |
-// Kahan state.  Offsets in floats.
+// Shared-memory layout (floats).  Block header: code | constants | meta (32
+// words) | cross-warp sums (kRegThreads/32 x 8 doubles).  Per warp: stacks
+// (per type) | Kahan state.
 void reg_layout(uint32_t code_words, uint32_t const_floats, const uint32_t *stack_depth, int P,
-                uint32_t *stack_off, uint32_t *acc_off, uint32_t *region_floats) {
-    uint32_t off = align4r(code_words) + align4r(const_floats);
+                uint32_t *stack_off, uint32_t *acc_off, uint32_t *region_floats, uint32_t *block_hdr_floats) {
+    *block_hdr_floats = align4r(code_words) + align4r(const_floats) + 32u + 2u * (kRegThreads / 32) * kMaxProgsPerWarp;
+    uint32_t off = 0;
     for (int t = 0; t < N_STACKS; ++t) {
         stack_off[t] = off;
         off += stack_depth[t] * (uint32_t)kStackWidth[t] * 32u * (uint32_t)P;
@@ -385,10 +412,16 @@ void reg_layout(uint32_t code_words, uint32_t const_floats, const uint32_t *stac
     *region_floats = align4r(off);
 }
 
+size_t reg_smem_bytes(uint32_t code_words, uint32_t const_floats, const uint32_t *stack_depth, int P) {
+    uint32_t so[N_STACKS], ao, rf, hf;
+    reg_layout(code_words, const_floats, stack_depth, P, so, &ao, &rf, &hf);
+    return ((size_t)hf + (size_t)rf * (kRegThreads / 32)) * 4u;
+}
+
 template <int PROF, int P>
 static cudaError_t launch_reg_pp(const LaunchArgs &a, uint32_t grid, cudaStream_t st) {
     auto k = reg_eval_kernel<PROF, P>;
-    const size_t smem = (size_t)a.region_floats * 4u * (kRegThreads / 32);
+    const size_t smem = ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (kRegThreads / 32)) * 4u;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, kRegThreads, smem, st>>>(a);
@@ -413,8 +446,12 @@ cudaError_t launch_reg(const LaunchArgs &a, int profile, int P, uint32_t grid, c
 
 template <int PROF, int P>
 static int occ(size_t smem) {
+    // the occupancy query counts a block above 48 KB of dynamic shared memory
+    // as unlaunchable until the kernel's limit has been raised
+    auto k = reg_eval_kernel<PROF, P>;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, reg_eval_kernel<PROF, P>, kRegThreads, smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kRegThreads, smem) != cudaSuccess) return 0;
     return n;
 }
 

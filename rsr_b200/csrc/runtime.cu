@@ -125,7 +125,14 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
     for (uint32_t i = 0; i < n; ++i) {
         if (gradient) path[i] = -2;
         else if (kernel == RSR_KERNEL_PLAIN || enc[i].profile < 0) path[i] = -1;
-        else path[i] = enc[i].profile;
+        else {
+            // the register kernel's spill stacks for 2 points per lane must fit
+            // one block next to the program's own code and constants
+            uint32_t depth[N_STACKS];
+            for (int t = 0; t < N_STACKS; ++t) depth[t] = (uint32_t)enc[i].depth_fast[t];
+            const uint32_t cw = (uint32_t)enc[i].reg_code.size() + 1, cf = (uint32_t)enc[i].consts.size();
+            path[i] = reg_smem_bytes(cw, cf, depth, 2) <= kRegSmemBudget / 2 ? enc[i].profile : -1;
+        }
     }
     // group programs by (path, dataset), each group sorted by descending code length
     std::vector<uint32_t> order(n);
@@ -211,6 +218,11 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             items.emplace_back(len_sum, WorkItem{j, k - j, 0, 0, 0, 0});
             j = k;
         }
+        // register kernel: the tuned points per thread, halved while a block
+        // would not fit
+        if (g.kind == 1)
+            while (g.P > 2 && reg_smem_bytes(g.code_words, g.const_floats, g.stack_depth, g.P) > kRegSmemBudget)
+                g.P >>= 1;
         // points per thread of slot-file kernels: largest that fits the smem budget
         if (g.kind != 1) {
             const size_t budget = 110 * 1024;
@@ -344,19 +356,28 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
         if (g.kind == 0) {
             const size_t per = plain_smem_per_warp(g.code_words, g.const_floats, g.slots, g.P);
             uint32_t wpb = (uint32_t)std::max<size_t>(1, std::min<size_t>(kPlainThreads / 32, (200 * 1024) / per));
+            g.grid = (g.n_items + wpb - 1) / wpb;
+            g.smem = per * wpb;
+            g.warps_per_block = wpb;
             e = launch_plain(a, g.P, wpb, per * wpb, st);
         } else if (g.kind == 1) {
-            reg_layout(g.code_words, g.const_floats, g.stack_depth, g.P, a.stack_off, &a.acc_off, &a.region_floats);
-            const size_t smem = (size_t)a.region_floats * 4u * (kRegThreads / 32);
+            reg_layout(g.code_words, g.const_floats, g.stack_depth, g.P, a.stack_off, &a.acc_off, &a.region_floats,
+                       &a.block_hdr_floats);
+            const size_t smem = ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (kRegThreads / 32)) * 4u;
             int bps = std::max(1, reg_max_blocks_per_sm(g.profile, g.P, smem));
-            uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)bps * ctx->num_sms,
-                                                         (g.n_items + (kRegThreads / 32) - 1) / (kRegThreads / 32));
-            e = launch_reg(a, g.profile, g.P, std::max(1u, grid), st);
+            uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)bps * ctx->num_sms, g.n_items);
+            g.grid = std::max(1u, grid);
+            g.smem = smem;
+            g.warps_per_block = kRegThreads / 32;
+            e = launch_reg(a, g.profile, g.P, g.grid, st);
         } else {
             size_t per = grad_smem_per_warp(g.code_words, g.const_floats, g.slots);
             per += (size_t)g.slots * 32u * 4u * (g.P - 1) * 2u;
             uint32_t wpb = (uint32_t)std::max<size_t>(1, std::min<size_t>(kGradThreads / 32, (200 * 1024) / per));
             a.progs_per_warp = (uint32_t)g.P;  // adjoint kernel reads P from here
+            g.grid = (g.n_items + wpb - 1) / wpb;
+            g.smem = per * wpb;
+            g.warps_per_block = wpb;
             e = launch_grad(a, wpb, per * wpb, st);
         }
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
@@ -755,7 +776,9 @@ int rsr_batch_describe(rsr_ctx *ctx, rsr_batch *b, char *buf, size_t len) {
         s += (i ? ", " : "") + std::string("{\"kernel\": \"") + kn + "\", \"profile\": " + std::to_string(g.profile) +
              ", \"points_per_thread\": " + std::to_string(g.P) + ", \"programs_per_warp\": " + std::to_string(g.G) +
              ", \"items\": " + std::to_string(g.n_items) + ", \"flops\": " + std::to_string(g.flops) +
-             ", \"program_points\": " + std::to_string(g.program_points) + ", \"last_ms\": " +
+             ", \"program_points\": " + std::to_string(g.program_points) + ", \"grid\": " + std::to_string(g.grid) +
+             ", \"warps_per_block\": " + std::to_string(g.warps_per_block) + ", \"smem_bytes\": " +
+             std::to_string(g.smem) + ", \"last_ms\": " +
              std::to_string(b->group_ms.size() > i ? b->group_ms[i] : 0.0f) + "}";
     }
     s += "], \"upload_bytes\": " + std::to_string(b->pool_bytes) + "}";

@@ -60,9 +60,10 @@ struct Group {
     uint32_t item_begin = 0, n_items = 0;  // into the plan's item array
     uint32_t code_words = 0, const_floats = 0, slots = 0;  // per-warp staging maxima
     uint32_t stack_depth[N_STACKS] = {0, 0, 0, 0, 0};       // register kernel: spill slots per type
-    uint32_t grid = 0;
-    size_t smem = 0;
-    uint32_t warps_per_block = 0;
+    // launch shape of the last enqueue (filled in by enqueue_plan)
+    mutable uint32_t grid = 0;
+    mutable size_t smem = 0;
+    mutable uint32_t warps_per_block = 0;
     uint64_t flops = 0;           // algorithmic FP32 lane-ops of one run
     uint64_t program_points = 0;
 };
