@@ -143,6 +143,22 @@ RSR_API int rsr_eval_mse_grad_batch(rsr_ctx *ctx, const rsr_population *pop, rsr
 /* eval_simd over every batch for each program: out[i*num_batches*8 + j]. */
 RSR_API int rsr_eval_points_batch(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, int kernel, float *out);
 
+/* rsr_compute_mse without allocation.  No reference counterpart: an extra
+ * entry point for callers that must not allocate device memory per call --
+ * a serving loop whose device memory is all handed out to a fixed pool (a
+ * cudaMalloc there fails or evicts), or a host thread that shares the GPU
+ * with running streams (cudaFree synchronises the whole device).
+ * The slot-file kernel runs with its descriptors, code, constants, work
+ * items and partial sums in one static device array of 256 KiB per device,
+ * so the program is limited to 512 instructions and 1024 constants /
+ * parameter floats, and the dataset to 16,777,216 points; larger inputs
+ * return RSR_EINVAL.  The first call on a device takes the array's address
+ * (cudaGetSymbolAddress, with the device current) and should come before any
+ * stream capture on that device.  Calls that overlap in time on one device
+ * through different contexts race on the array.  The dataset must already
+ * be resident (rsr_dataset_upload). */
+RSR_API int rsr_compute_mse_noalloc(rsr_ctx *ctx, const rsr_program *prog, rsr_dataset ds, float *mse);
+
 /* ----------------------------------------------------- constant fitting */
 typedef struct rsr_fit_stats {
     uint32_t iterations;            /* L-BFGS iterations taken by the slowest program */

@@ -76,6 +76,7 @@ _SIGS = {
     "rsr_eval_mse_grad_batch": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_void_p,
                                           C.c_void_p]),
     "rsr_eval_points_batch": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_int, C.c_void_p]),
+    "rsr_compute_mse_noalloc": (C.c_int, [C.c_void_p, C.POINTER(Program), C.c_uint64, C.POINTER(C.c_float)]),
     "rsr_fit_lbfgs": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p,
                                 C.c_void_p, C.POINTER(FitStats)]),
     "rsr_batch_prepare": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_int, C.c_int,
