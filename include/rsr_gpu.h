@@ -174,6 +174,76 @@ typedef struct rsr_fit_stats {
 RSR_API int rsr_fit_lbfgs(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const rsr_dataset *ds_per_program,
                           uint32_t max_iterations, float *params_out, float *mse_out, rsr_fit_stats *stats);
 
+/* ------------------------------------------------------------ serving
+ * A device-resident request loop for the island threads (the callers of
+ * Individual::calculate_mse, src/engine/search/island.rs:150-238, and of
+ * optimize_individual_constants, src/engine/optimize/mod.rs:10-59): jobs are
+ * submitted from any thread, datasets stay resident, and `slots` worker
+ * streams keep several jobs on the device at once.  Continuous batching:
+ * a free slot takes the oldest waiting job and merges the evaluation jobs of
+ * the same kind queued behind it (up to max_batch_programs programs) into
+ * one launch.  Memory admission: a job whose estimated device footprint is
+ * above the budget is refused at submit (RSR_ENOMEM); otherwise it waits
+ * until the running jobs' footprints leave room for it. */
+typedef struct rsr_server rsr_server;
+
+typedef struct rsr_server_options {
+    uint32_t struct_size;
+    uint32_t slots;               /* jobs on the device at once; default 4 */
+    uint32_t max_batch_programs;  /* programs merged into one launch; default 16384 */
+    uint32_t max_queue;           /* waiting jobs before submit returns RSR_EBUSY; default 65536 */
+    uint64_t mem_budget_bytes;    /* device bytes of in-flight jobs; 0 = half the context's free budget */
+} rsr_server_options;
+
+typedef enum rsr_job_kind {
+    RSR_JOB_MSE = 0,       /* mse_out[n] */
+    RSR_JOB_MSE_GRAD = 1,  /* mse_out[n], grad_out[n*32] */
+    RSR_JOB_FIT = 2        /* rsr_fit_lbfgs: params_out (pop->params layout), mse_out[n] */
+} rsr_job_kind;
+
+typedef struct rsr_job {
+    uint32_t kind;                       /* rsr_job_kind */
+    uint32_t fit_iterations;             /* RSR_JOB_FIT */
+    const rsr_population *pop;           /* copied by rsr_submit */
+    rsr_dataset ds;                      /* dataset of every program, unless ... */
+    const rsr_dataset *ds_per_program;   /* ... one per program (copied) */
+    float *mse_out;                      /* written when the job completes; */
+    float *grad_out;                     /* the caller keeps these valid until */
+    float *params_out;                   /* rsr_wait returns or the job is cancelled */
+} rsr_job;
+
+typedef enum rsr_job_state { RSR_JOB_QUEUED = 0, RSR_JOB_RUNNING = 1, RSR_JOB_DONE = 2 } rsr_job_state;
+
+typedef struct rsr_job_info {
+    int32_t status;          /* rsr_status of the job */
+    uint32_t batch_jobs;     /* jobs that shared its launch */
+    double queue_ms;         /* submit -> taken by a slot */
+    double latency_ms;       /* submit -> results written */
+} rsr_job_info;
+
+typedef struct rsr_serving_stats {
+    uint64_t submitted, completed, failed, cancelled, refused;
+    uint64_t launches;               /* batches run (merged launches count once) */
+    uint64_t peak_mem_bytes;         /* largest admitted in-flight footprint */
+    double p50_ms, p95_ms, p99_ms, mean_ms, max_ms;   /* latency of completed jobs */
+    double program_points_per_sec;   /* completed program*points / busy wall time */
+    double wall_s;                   /* first submit -> last completion */
+} rsr_serving_stats;
+
+RSR_API void rsr_server_options_default(rsr_server_options *opts);
+RSR_API int rsr_server_create(rsr_ctx *ctx, const rsr_server_options *opts, rsr_server **out);
+/* Cancels waiting jobs, finishes running ones, joins the workers. */
+RSR_API int rsr_server_destroy(rsr_server *srv);
+RSR_API int rsr_submit(rsr_server *srv, const rsr_job *job, uint64_t *ticket);
+RSR_API int rsr_poll(rsr_server *srv, uint64_t ticket, uint32_t *state);
+/* Waits up to timeout_us (0 = forever) and returns the job's status (the
+ * ticket is then retired), or RSR_ETIMEDOUT leaving the job in place. */
+RSR_API int rsr_wait(rsr_server *srv, uint64_t ticket, uint64_t timeout_us, rsr_job_info *info);
+/* A waiting job is dropped; a running fit stops after its current step;
+ * a running evaluation completes.  Wait on the ticket afterwards. */
+RSR_API int rsr_cancel(rsr_server *srv, uint64_t ticket);
+RSR_API int rsr_server_stats(rsr_server *srv, rsr_serving_stats *stats, int reset);
+
 /* -------------------------------------------------- prepared batches */
 /* A population encoded and uploaded once, then run many times with inputs
  * resident on the device (the timed unit of the benchmark).  run() enqueues

@@ -5,12 +5,15 @@ from . import isa
 from .dataset import Dataset
 from .isa import Program, Scalar, pack
 
-__all__ = ["isa", "Dataset", "Program", "Scalar", "pack", "Engine", "compute_mse", "compute_mse_with_gradient"]
+__all__ = ["isa", "Dataset", "Program", "Scalar", "pack", "Engine", "Server", "compute_mse",
+           "compute_mse_with_gradient"]
 
 
 def __getattr__(name):
     # the evaluator needs the CUDA library; import it on first use
+    import importlib
     if name in ("Engine", "compute_mse", "compute_mse_with_gradient"):
-        import importlib
         return getattr(importlib.import_module(".evaluator", __name__), name)
+    if name == "Server":
+        return importlib.import_module(".serving", __name__).Server
     raise AttributeError(name)

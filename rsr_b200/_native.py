@@ -47,6 +47,34 @@ class FitStats(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("gradient_evaluations", C.c_uint32), ("mse_evaluations", C.c_uint32)]
 
 
+JOB_MSE, JOB_MSE_GRAD, JOB_FIT = 0, 1, 2
+JOB_QUEUED, JOB_RUNNING, JOB_DONE = 0, 1, 2
+
+
+class ServerOptions(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("slots", C.c_uint32), ("max_batch_programs", C.c_uint32),
+                ("max_queue", C.c_uint32), ("mem_budget_bytes", C.c_uint64)]
+
+
+class Job(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("fit_iterations", C.c_uint32), ("pop", C.POINTER(Population)),
+                ("ds", C.c_uint64), ("ds_per_program", C.POINTER(C.c_uint64)), ("mse_out", C.POINTER(C.c_float)),
+                ("grad_out", C.POINTER(C.c_float)), ("params_out", C.POINTER(C.c_float))]
+
+
+class JobInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("batch_jobs", C.c_uint32), ("queue_ms", C.c_double),
+                ("latency_ms", C.c_double)]
+
+
+class ServingStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("cancelled", C.c_uint64), ("refused", C.c_uint64), ("launches", C.c_uint64),
+                ("peak_mem_bytes", C.c_uint64), ("p50_ms", C.c_double), ("p95_ms", C.c_double),
+                ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double),
+                ("program_points_per_sec", C.c_double), ("wall_s", C.c_double)]
+
+
 class ProgramInfo(C.Structure):
     _fields_ = [("depth_ref", C.c_uint32 * 5), ("depth_fast", C.c_uint32 * 5), ("n_uops_fast", C.c_uint32),
                 ("n_uops_plain", C.c_uint32), ("fast_profile", C.c_int32), ("flops_per_point", C.c_uint32)]
@@ -76,6 +104,14 @@ _SIGS = {
     "rsr_eval_mse_grad_batch": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_void_p,
                                           C.c_void_p]),
     "rsr_eval_points_batch": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_int, C.c_void_p]),
+    "rsr_server_options_default": (None, [C.POINTER(ServerOptions)]),
+    "rsr_server_create": (C.c_int, [C.c_void_p, C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]),
+    "rsr_server_destroy": (C.c_int, [C.c_void_p]),
+    "rsr_submit": (C.c_int, [C.c_void_p, C.POINTER(Job), C.POINTER(C.c_uint64)]),
+    "rsr_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint32)]),
+    "rsr_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.POINTER(JobInfo)]),
+    "rsr_cancel": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "rsr_server_stats": (C.c_int, [C.c_void_p, C.POINTER(ServingStats), C.c_int]),
     "rsr_compute_mse_noalloc": (C.c_int, [C.c_void_p, C.POINTER(Program), C.c_uint64, C.POINTER(C.c_float)]),
     "rsr_fit_lbfgs": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p,
                                 C.c_void_p, C.POINTER(FitStats)]),

@@ -40,20 +40,27 @@ struct State {
 // between launches.
 struct Evaluator {
     Plan plan;
-    DevicePlan dev;
-    DevBuf active;
+    DevicePlan *dev = nullptr;  // device buffers, owned by a FitWorkspace
+    DevBuf *active = nullptr;
     std::vector<uint8_t> mask;  // launch order
     std::vector<float> host_out;
 };
 
-int prepare(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *dsp, uint64_t ds, bool gradient, Evaluator *ev) {
-    int rc = build_plan(ctx, pop, dsp, ds, RSR_KERNEL_AUTO, gradient, MODE_MSE, &ev->plan);
+int prepare(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *dsp, uint64_t ds, bool gradient,
+            cudaStream_t st, std::mutex *plan_mu, Evaluator *ev) {
+    int rc;
+    if (plan_mu) {
+        std::lock_guard<std::mutex> lk(*plan_mu);
+        rc = build_plan(ctx, pop, dsp, ds, RSR_KERNEL_AUTO, gradient, MODE_MSE, &ev->plan);
+    } else {
+        rc = build_plan(ctx, pop, dsp, ds, RSR_KERNEL_AUTO, gradient, MODE_MSE, &ev->plan);
+    }
     if (rc) return rc;
-    if ((rc = upload_plan(ctx, ev->plan, &ev->dev, ctx->stream))) return rc;
+    if ((rc = upload_plan(ctx, ev->plan, ev->dev, st))) return rc;
     const size_t n = ev->plan.progs.size();
-    cudaError_t e = ev->active.reserve(std::max<size_t>(n, 1));
+    cudaError_t e = ev->active->reserve(std::max<size_t>(n, 1));
     if (e != cudaSuccess) return cuda_fail(e, "active mask");
-    ev->dev.base.active = (const uint8_t *)ev->active.p;
+    ev->dev->base.active = (const uint8_t *)ev->active->p;
     ev->mask.assign(n, 1);
     return RSR_OK;
 }
@@ -61,8 +68,8 @@ int prepare(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *dsp, uint64
 // Writes every program's parameters (caller order, flat) into the constant
 // pool and the activity of each program into the mask, runs, and returns
 // mse (and grad, n x 32) in caller order.
-int evaluate(rsr_ctx *ctx, Evaluator *ev, const std::vector<State> &st, const std::vector<char> &want,
-             bool use_next_x, std::vector<float> *mse, std::vector<float> *grad) {
+int evaluate(rsr_ctx *ctx, cudaStream_t stream, Evaluator *ev, const std::vector<State> &st,
+             const std::vector<char> &want, bool use_next_x, std::vector<float> *mse, std::vector<float> *grad) {
     Plan &P = ev->plan;
     const size_t n = P.progs.size();
     for (size_t li = 0; li < n; ++li) {
@@ -74,19 +81,19 @@ int evaluate(rsr_ctx *ctx, Evaluator *ev, const std::vector<State> &st, const st
         ev->mask[li] = want[i] ? 1 : 0;
     }
     cudaError_t e;
-    if ((e = cudaMemcpyAsync((void *)ev->dev.base.consts, P.consts.data(), P.consts.size() * sizeof(float),
-                             cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+    if ((e = cudaMemcpyAsync((void *)ev->dev->base.consts, P.consts.data(), P.consts.size() * sizeof(float),
+                             cudaMemcpyHostToDevice, stream)) != cudaSuccess)
         return cuda_fail(e, "constant upload");
-    if ((e = cudaMemcpyAsync(ev->active.p, ev->mask.data(), n, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+    if ((e = cudaMemcpyAsync(ev->active->p, ev->mask.data(), n, cudaMemcpyHostToDevice, stream)) != cudaSuccess)
         return cuda_fail(e, "mask upload");
-    int rc = enqueue_plan(ctx, P, &ev->dev, ctx->stream, nullptr);
+    int rc = enqueue_plan(ctx, P, ev->dev, stream, nullptr);
     if (rc) return rc;
     const size_t nf = n * (P.gradient ? 33 : 1);
     ev->host_out.resize(nf);
-    if ((e = cudaMemcpyAsync(ev->host_out.data(), ev->dev.out.p, nf * sizeof(float), cudaMemcpyDeviceToHost,
-                             ctx->stream)) != cudaSuccess)
+    if ((e = cudaMemcpyAsync(ev->host_out.data(), ev->dev->out.p, nf * sizeof(float), cudaMemcpyDeviceToHost,
+                             stream)) != cudaSuccess)
         return cuda_fail(e, "result download");
-    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(e, "evaluation");
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(e, "evaluation");
     for (size_t li = 0; li < n; ++li) {
         const uint32_t i = P.orig[li];
         if (!want[i]) continue;
@@ -97,26 +104,26 @@ int evaluate(rsr_ctx *ctx, Evaluator *ev, const std::vector<State> &st, const st
 }
 
 }  // namespace
-}  // namespace rsr
 
-using namespace rsr;
-
-extern "C" {
-
-int rsr_fit_lbfgs(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const rsr_dataset *dsp,
-                  uint32_t max_iterations, float *params_out, float *mse_out, rsr_fit_stats *stats) {
-    if (!ctx || !pop || !params_out || !mse_out) return fail(RSR_EINVAL, "null argument");
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    cudaSetDevice(ctx->device);
+int fit_population(rsr_ctx *ctx, const rsr_population *pop, const uint64_t *dsp, uint64_t ds,
+                   uint32_t max_iterations, cudaStream_t stream, std::mutex *plan_mu,
+                   const std::atomic<bool> *cancel, FitWorkspace *ws, float *params_out, float *mse_out,
+                   rsr_fit_stats *stats) {
     const uint32_t N = pop->n_programs;
     rsr_fit_stats local{};
     if (N == 0) {
         if (stats) *stats = local;
         return RSR_OK;
     }
+    FitWorkspace own;
+    if (!ws) ws = &own;
     Evaluator gev, mev;
-    int rc = prepare(ctx, *pop, dsp, ds, true, &gev);
-    if (!rc) rc = prepare(ctx, *pop, dsp, ds, false, &mev);
+    gev.dev = &ws->grad;
+    gev.active = &ws->grad_active;
+    mev.dev = &ws->mse;
+    mev.active = &ws->mse_active;
+    int rc = prepare(ctx, *pop, dsp, ds, true, stream, plan_mu, &gev);
+    if (!rc) rc = prepare(ctx, *pop, dsp, ds, false, stream, plan_mu, &mev);
     if (rc) return rc;
 
     std::vector<State> st(N);
@@ -131,7 +138,7 @@ int rsr_fit_lbfgs(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const
     std::vector<char> want(N, 1);
     // initial gradient (lbfgs.rs:32-33); programs without parameters only get
     // their MSE (their constants are not touched, lbfgs.rs:18-21)
-    if ((rc = evaluate(ctx, &gev, st, want, false, &mse, &grad))) return rc;
+    if ((rc = evaluate(ctx, stream, &gev, st, want, false, &mse, &grad))) return rc;
     local.gradient_evaluations++;
     for (uint32_t i = 0; i < N; ++i) {
         st[i].mse = mse[i];
@@ -139,6 +146,7 @@ int rsr_fit_lbfgs(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const
     }
 
     for (uint32_t iter = 0; iter < max_iterations; ++iter) {
+        if (cancel && cancel->load()) return fail(RSR_ECANCELED, "fit cancelled");
         bool any = false;
         // direction (lbfgs.rs:39-106)
         for (uint32_t i = 0; i < N; ++i) {
@@ -200,7 +208,7 @@ int rsr_fit_lbfgs(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const
                     left = true;
                 }
             if (!left) break;
-            if ((rc = evaluate(ctx, &mev, st, searching, true, &mse, nullptr))) return rc;
+            if ((rc = evaluate(ctx, stream, &mev, st, searching, true, &mse, nullptr))) return rc;
             local.mse_evaluations++;
             for (uint32_t i = 0; i < N; ++i) {
                 if (!searching[i]) continue;
@@ -218,7 +226,7 @@ int rsr_fit_lbfgs(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const
         }
         // gradient at the new point (lbfgs.rs:127)
         for (uint32_t i = 0; i < N; ++i) want[i] = !st[i].done;
-        if ((rc = evaluate(ctx, &gev, st, want, true, &mse, &grad))) return rc;
+        if ((rc = evaluate(ctx, stream, &gev, st, want, true, &mse, &grad))) return rc;
         local.gradient_evaluations++;
         // history update (lbfgs.rs:129-151)
         for (uint32_t i = 0; i < N; ++i) {
@@ -254,4 +262,15 @@ int rsr_fit_lbfgs(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const
     return RSR_OK;
 }
 
-}  // extern "C"
+}  // namespace rsr
+
+using namespace rsr;
+
+extern "C" int rsr_fit_lbfgs(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const rsr_dataset *dsp,
+                             uint32_t max_iterations, float *params_out, float *mse_out, rsr_fit_stats *stats) {
+    if (!ctx || !pop || !params_out || !mse_out) return fail(RSR_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return fit_population(ctx, pop, dsp, ds, max_iterations, ctx->stream, nullptr, nullptr, nullptr, params_out,
+                          mse_out, stats);
+}

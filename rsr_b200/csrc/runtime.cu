@@ -44,6 +44,25 @@ void DevBuf::release() {
     cap = 0;
 }
 
+cudaError_t HostBuf::reserve(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    release();
+    size_t want = std::max<size_t>(bytes, 1 << 20);
+    cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        cap = 0;
+        return e;
+    }
+    cap = want;
+    return cudaSuccess;
+}
+void HostBuf::release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+}
+
 static constexpr uint64_t kChunkPoints = 4096;   // points per work-item chunk (all P)
 static constexpr uint64_t kStrideAlign = 1024;   // dataset column padding
 static constexpr int kGradSlotDoubles = 33;      // sse + 32 gradient sums
@@ -269,19 +288,6 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
     return RSR_OK;
 }
 
-// Pinned staging buffer of the context.
-static int ensure_pinned(rsr_ctx *ctx, size_t bytes) {
-    if (bytes <= ctx->pinned_cap) return RSR_OK;
-    if (ctx->pinned) cudaFreeHost(ctx->pinned);
-    ctx->pinned = nullptr;
-    ctx->pinned_cap = 0;
-    size_t want = std::max<size_t>(bytes, 1 << 20);
-    cudaError_t e = cudaHostAlloc(&ctx->pinned, want, cudaHostAllocDefault);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaHostAlloc");
-    ctx->pinned_cap = want;
-    return RSR_OK;
-}
-
 int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st) {
     const size_t n = plan.progs.size();
     auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
@@ -300,11 +306,10 @@ int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st
         return cuda_fail(e, "outputs");
     if ((e = dev->counters.reserve(std::max<size_t>(plan.groups.size(), 1) * sizeof(uint32_t) + 64)) != cudaSuccess)
         return cuda_fail(e, "counters");
-    int rc = ensure_pinned(ctx, total);
-    if (rc) return rc;
-    // the pinned buffer is shared: wait for earlier copies out of it
+    // the staging buffer may still feed an earlier copy on this stream
     cudaStreamSynchronize(st);
-    char *h = (char *)ctx->pinned;
+    if ((e = dev->staging.reserve(total)) != cudaSuccess) return cuda_fail(e, "cudaHostAlloc");
+    char *h = (char *)dev->staging.p;
     memcpy(h + o_progs, plan.progs.data(), n * sizeof(ProgDesc));
     memcpy(h + o_ds, plan.datasets.data(), plan.datasets.size() * sizeof(DatasetDesc));
     memcpy(h + o_items, plan.items.data(), plan.items.size() * sizeof(WorkItem));
@@ -512,7 +517,7 @@ int rsr_ctx_destroy(rsr_ctx *ctx) {
     ctx->scratch.partials.release();
     ctx->scratch.out.release();
     ctx->scratch.counters.release();
-    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->scratch.staging.release();
     if (ctx->l2buf) cudaFree(ctx->l2buf);
     for (auto &ev : ctx->ev) if (ev) cudaEventDestroy(ev);
     cudaStreamDestroy(ctx->stream);

@@ -30,6 +30,15 @@ struct DevBuf {
     ~DevBuf() { release(); }
 };
 
+// Pinned host staging buffer.
+struct HostBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t reserve(size_t bytes);
+    void release();
+    ~HostBuf() { release(); }
+};
+
 struct DatasetRec {
     float *x = nullptr;   // features, SoA, stride points per feature
     float *y = nullptr;
@@ -95,6 +104,7 @@ struct DevicePlan {
     DevBuf out;         // mse (n floats) [+ grad (n*32 floats)]
     DevBuf counters;    // one item counter per group
     DevBuf status;
+    HostBuf staging;    // pinned image of the pool, uploaded with one copy
     LaunchArgs base{};
     float *mse = nullptr, *grad = nullptr;
 };
@@ -113,13 +123,11 @@ struct rsr_ctx {
     std::map<std::pair<int, int>, rsr::TuneChoice> tune;  // (profile, log2 points) -> choice
     rsr::TuneChoice force;     // set while the autotuner measures a candidate
     rsr::DevicePlan scratch;   // for one-shot calls
-    void *pinned = nullptr;
-    size_t pinned_cap = 0;
     void *l2buf = nullptr;
     size_t l2bytes = 0;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     std::atomic<uint64_t> launches{0};
-    uint64_t last_h2d = 0, last_d2h = 0;   // bytes copied by the last evaluation call
+    std::atomic<uint64_t> last_h2d{0}, last_d2h{0};   // bytes copied by the last evaluation call
 };
 
 struct rsr_batch {
@@ -139,6 +147,18 @@ namespace rsr {
 int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_prog, uint64_t ds_all, int kernel,
                bool gradient, int mode, Plan *plan);
 int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st);
+// Batched L-BFGS (lbfgs.cu) on stream st.  plan_mu, when given, is held while
+// plans are built (they read the context's dataset and tuning tables);
+// cancel, when set, stops the fit between iterations with RSR_ECANCELED.
+// ws, when given, supplies (and keeps) the device buffers of the fit.
+struct FitWorkspace {
+    DevicePlan grad, mse;
+    DevBuf grad_active, mse_active;
+};
+int fit_population(rsr_ctx *ctx, const rsr_population *pop, const uint64_t *dsp, uint64_t ds,
+                   uint32_t max_iterations, cudaStream_t stream, std::mutex *plan_mu,
+                   const std::atomic<bool> *cancel, FitWorkspace *ws, float *params_out, float *mse_out,
+                   rsr_fit_stats *stats);
 // group_events: optional, 2 per group (before/after its kernel); not used
 // while capturing a graph.
 int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st, cudaEvent_t ev_mid,
