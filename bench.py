@@ -168,6 +168,81 @@ def run_reference(args):
     return 0
 
 
+def serving_bench(eng, jobs: int, rate: float, threads: int = 16, seed: int = 7):
+    """The serving mix: `threads` island threads submit `jobs` jobs with
+    Poisson arrivals at `rate` jobs/s in total; each job holds 64-1024
+    programs (uniform) against one of the four workloads' resident datasets
+    (scalar 400 points; vector 100k; matrix 1M; uneven: 16 datasets of 400 to
+    262,144 points, one per program); 30% of the jobs ask for a 10-step
+    constant fit, the rest for MSE fitness.  Latency is submit -> results
+    written, measured by the server."""
+    from rsr_b200 import isa as I
+    from rsr_b200 import workloads as W
+    from rsr_b200.serving import Server
+    rng = np.random.default_rng(seed)
+    pools = {"scalar": (W.scalar_population(1024, seed=31), eng.upload(W.scalar_dataset(400, seed=1))),
+             "vector": (W.lorentz_population(1024, seed=32), eng.upload(W.lorentz_dataset(100_000, seed=2))),
+             "matrix": (W.transform_population(1024, seed=33), eng.upload(W.transform_dataset(1_000_000, seed=3)))}
+    uneven = [eng.upload(W.inverse_dataset(n, seed=40 + i)) for i, n in enumerate(W.uneven_sizes(16))]
+    pools["uneven"] = (W.inverse_population(1024, seed=34), None)
+    names = list(pools)
+    plan = []
+    for _ in range(jobs):
+        name = names[int(rng.integers(0, 4))]
+        n = int(rng.integers(64, 1025))
+        lo = int(rng.integers(0, 1024 - n + 1))
+        progs, dsd = pools[name]
+        pk = I.pack(progs[lo:lo + n])
+        handles = None
+        if dsd is None:
+            handles = np.array([uneven[int(k)].handle for k in rng.integers(0, 16, n)], np.uint64)
+        kind = "fit" if rng.random() < 0.3 else "mse"
+        plan.append((pk, dsd, handles, kind))
+    gaps = rng.exponential(threads / rate, jobs)
+    per_thread = [list(range(t, jobs, threads)) for t in range(threads)]
+    srv = Server(eng, slots=4)
+    tickets = [None] * jobs
+    errors = []
+
+    def island(idx):
+        t_next = time.perf_counter()
+        for i in idx:
+            t_next += gaps[i]
+            d = t_next - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            pk, dsd, handles, kind = plan[i]
+            try:
+                tickets[i] = srv.submit(pk, dsd, datasets=handles, kind=kind, fit_iterations=10)
+            except Exception as e:  # refused: counted by the server
+                errors.append(str(e))
+
+    th = [threading.Thread(target=island, args=(idx,)) for idx in per_thread]
+    t0 = time.perf_counter()
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    t_submit = time.perf_counter() - t0
+    batch_sizes = []
+    for t in tickets:
+        if t is not None:
+            batch_sizes.append(srv.wait(t)["info"]["batch_jobs"])
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    pts = {k: (v[1].num_batches * 8 if v[1] is not None else None) for k, v in pools.items()}
+    return {"jobs": jobs, "arrival_rate_jobs_per_s": rate, "submit_s": t_submit, "drain_s": wall,
+            "completed": st["completed"], "failed": st["failed"], "refused": st["refused"],
+            "latency_ms": {"p50": st["p50_ms"], "p95": st["p95_ms"], "p99": st["p99_ms"], "max": st["max_ms"]},
+            "program_points_per_sec": st["program_points_per_sec"],
+            "launches": st["launches"], "mean_jobs_per_launch": float(np.mean(batch_sizes)) if batch_sizes else 0.0,
+            "peak_inflight_bytes": st["peak_mem_bytes"], "slots": 4, "submitter_threads": threads,
+            "what": "rsr_server: 64-1024 programs per job, 30% with a 10-step L-BFGS fit, over the scalar/vector/"
+                    "matrix/uneven datasets resident on the device; latency = submit -> results written "
+                    "(program_points counts one evaluation per program)"}
+
+
 def run_engine(args):
     rank, world, local = rank_info()
     dist = None
@@ -271,6 +346,10 @@ def run_engine(args):
     e2e_value = pp_rank * world * len(e2e_ms) / (max_over_ranks(sum(e2e_ms)) * 1e-3)
     assert np.array_equal(out, mse_ref)
 
+    serving = None
+    if not args.no_serving:
+        serving = serving_bench(eng, args.serving_jobs, args.serving_rate)
+
     line = None
     if rank == 0:
         cpu = None
@@ -307,6 +386,7 @@ def run_engine(args):
             "autotune": tune["chosen"],
             "programs_on_register_kernel": desc["register_kernel_programs"],
             "programs_on_slot_kernel": desc["slot_kernel_programs"],
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     eng2.close()
@@ -324,6 +404,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-mix leg")
+    ap.add_argument("--serving-jobs", type=int, default=400)
+    ap.add_argument("--serving-rate", type=float, default=2000.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

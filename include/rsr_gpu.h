@@ -159,6 +159,18 @@ RSR_API int rsr_eval_points_batch(rsr_ctx *ctx, const rsr_population *pop, rsr_d
  * be resident (rsr_dataset_upload). */
 RSR_API int rsr_compute_mse_noalloc(rsr_ctx *ctx, const rsr_program *prog, rsr_dataset ds, float *mse);
 
+/* Point sharding (a dataset split across GPUs by 8-point batches, the last
+ * shard holding the padding): per-program unscaled f64 sums of one shard --
+ * SSE, or SSE followed by the 32 gradient sums when gradient != 0
+ * (n x 33 doubles) -- in caller order.  The shards' sums are added (one
+ * all-reduce) and rsr_finalize_sums applies the epilogue of compute_mse /
+ * compute_mse_with_gradient (evaluator.rs:172-173, 211-223) with the whole
+ * dataset's num_samples. */
+RSR_API int rsr_eval_sums_batch(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds,
+                                const rsr_dataset *ds_per_program, int gradient, double *sums_out);
+RSR_API int rsr_finalize_sums(uint32_t n, int gradient, const double *sums, uint64_t num_samples, float *mse_out,
+                              float *grad_out);
+
 /* ----------------------------------------------------- constant fitting */
 typedef struct rsr_fit_stats {
     uint32_t iterations;            /* L-BFGS iterations taken by the slowest program */

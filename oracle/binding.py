@@ -108,6 +108,13 @@ def mse_f64(p, ds) -> float:
     return float(lib().orc_mse_f64(*a, *d, ds.num_samples))
 
 
+def sse_f64(p, ds) -> float:
+    """Unscaled FP64 sum of squared errors over every padded point."""
+    a, k = _prog(p)
+    d, k2 = _ds(ds)
+    return float(lib().orc_mse_f64(*a, *d, 1))
+
+
 def mse_grad_dual(p, ds):
     a, k = _prog(p)
     d, k2 = _ds(ds)

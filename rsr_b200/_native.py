@@ -112,6 +112,9 @@ _SIGS = {
     "rsr_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.POINTER(JobInfo)]),
     "rsr_cancel": (C.c_int, [C.c_void_p, C.c_uint64]),
     "rsr_server_stats": (C.c_int, [C.c_void_p, C.POINTER(ServingStats), C.c_int]),
+    "rsr_eval_sums_batch": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_int,
+                                      C.c_void_p]),
+    "rsr_finalize_sums": (C.c_int, [C.c_uint32, C.c_int, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     "rsr_compute_mse_noalloc": (C.c_int, [C.c_void_p, C.POINTER(Program), C.c_uint64, C.POINTER(C.c_float)]),
     "rsr_fit_lbfgs": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p,
                                 C.c_void_p, C.POINTER(FitStats)]),

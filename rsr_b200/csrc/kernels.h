@@ -17,6 +17,8 @@ size_t plain_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t 
 cudaError_t launch_aosoa_to_soa(const float *ff, const float *tb, float *x, float *y, uint32_t nf, uint64_t nbatch,
                                 uint64_t stride, int num_sms, cudaStream_t st);
 cudaError_t measure_fp32_peak(int num_sms, cudaStream_t st, double *lane_ops_per_s);
+cudaError_t launch_finalize_sums(const ProgDesc *progs, const double *partials, uint32_t n, uint32_t stride,
+                                 double *out, cudaStream_t st);
 cudaError_t launch_finalize_mse(const ProgDesc *progs, const DatasetDesc *ds, const double *partials, uint32_t n,
                                 float *out, cudaStream_t st);
 

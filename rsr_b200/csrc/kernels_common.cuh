@@ -36,6 +36,12 @@ struct LaunchArgs {
     uint32_t stack_off[N_STACKS];
 };
 
+// Opt-in dynamic shared-memory limit of one block on sm_100 (227 KB).  Every
+// launcher raises its kernel's limit to this value rather than to the launch's
+// own size: the limit is per-function state shared by all host threads, and a
+// launch from one thread must not see it lowered by another thread.
+constexpr int kMaxDynSmemOptin = 227 * 1024;
+
 // Kahan-compensated single-precision running sum (one per lane).
 struct Kahan {
     float s = 0.0f, c = 0.0f;

@@ -398,7 +398,7 @@ __global__ void finalize_grad_kernel(const ProgDesc *progs, const DatasetDesc *d
 template <int P>
 static cudaError_t launch_grad_p(const LaunchArgs &a, uint32_t wpb, size_t smem, cudaStream_t st) {
     auto k = grad_kernel<P>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin);
     if (e != cudaSuccess) return e;
     k<<<(a.n_items + wpb - 1) / wpb, wpb * 32, smem, st>>>(a);
     return cudaGetLastError();

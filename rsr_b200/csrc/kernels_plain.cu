@@ -195,7 +195,7 @@ __global__ void finalize_mse_kernel(const ProgDesc *progs, const DatasetDesc *da
 template <int P>
 static cudaError_t launch_plain_p(const LaunchArgs &a, uint32_t warps_per_block, size_t smem, cudaStream_t st) {
     auto k = plain_eval_kernel<P>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin);
     if (e != cudaSuccess) return e;
     const uint32_t blocks = (a.n_items + warps_per_block - 1) / warps_per_block;
     k<<<blocks, warps_per_block * 32, smem, st>>>(a);
@@ -221,6 +221,27 @@ cudaError_t launch_aosoa_to_soa(const float *ff, const float *tb, float *x, floa
     if (blocks > (uint64_t)num_sms * 16) blocks = (uint64_t)num_sms * 16;
     if (blocks == 0) blocks = 1;
     aosoa_to_soa_kernel<<<(unsigned)blocks, 256, 0, st>>>(ff, tb, x, y, nf, nbatch, stride);
+    return cudaGetLastError();
+}
+
+// Per-program sums of the partials in the same fixed order, left unscaled
+// (stride 1: SSE; stride 33: SSE then the 32 gradient sums), for callers that
+// add the sums of several point shards before the epilogue.
+__global__ void finalize_sums_kernel(const ProgDesc *progs, const double *partials, uint32_t n_progs,
+                                     uint32_t stride, double *out) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n_progs) return;
+    const ProgDesc pd = progs[p];
+    for (uint32_t j = 0; j < stride; ++j) {
+        double s = 0.0;
+        for (uint32_t c = 0; c < pd.n_parts; ++c) s += partials[(size_t)(pd.part_off + c) * stride + j];
+        out[(size_t)p * stride + j] = s;
+    }
+}
+
+cudaError_t launch_finalize_sums(const ProgDesc *progs, const double *partials, uint32_t n, uint32_t stride,
+                                 double *out, cudaStream_t st) {
+    finalize_sums_kernel<<<(n + 127) / 128, 128, 0, st>>>(progs, partials, n, stride, out);
     return cudaGetLastError();
 }
 

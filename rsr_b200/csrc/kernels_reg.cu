@@ -422,7 +422,7 @@ template <int PROF, int P>
 static cudaError_t launch_reg_pp(const LaunchArgs &a, uint32_t grid, cudaStream_t st) {
     auto k = reg_eval_kernel<PROF, P>;
     const size_t smem = ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (kRegThreads / 32)) * 4u;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin);
     if (e != cudaSuccess) return e;
     k<<<grid, kRegThreads, smem, st>>>(a);
     return cudaGetLastError();
@@ -449,7 +449,7 @@ static int occ(size_t smem) {
     // the occupancy query counts a block above 48 KB of dynamic shared memory
     // as unlaunchable until the kernel's limit has been raised
     auto k = reg_eval_kernel<PROF, P>;
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin) != cudaSuccess) return 0;
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kRegThreads, smem) != cudaSuccess) return 0;
     return n;

@@ -301,7 +301,8 @@ int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st
     if ((e = dev->pool.reserve(total)) != cudaSuccess) return cuda_fail(e, "plan pool");
     if ((e = dev->partials.reserve(std::max<size_t>(plan.n_partials, 1) * sizeof(double))) != cudaSuccess)
         return cuda_fail(e, "partials");
-    const size_t out_floats = plan.mode == MODE_POINTS ? n * plan.points_stride : n * (plan.gradient ? 33 : 1);
+    size_t out_floats = plan.mode == MODE_POINTS ? n * plan.points_stride : n * (plan.gradient ? 33 : 1);
+    if (plan.raw_sums) out_floats *= 2;  // doubles
     if ((e = dev->out.reserve(std::max<size_t>(out_floats, 1) * sizeof(float))) != cudaSuccess)
         return cuda_fail(e, "outputs");
     if ((e = dev->counters.reserve(std::max<size_t>(plan.groups.size(), 1) * sizeof(uint32_t) + 64)) != cudaSuccess)
@@ -390,7 +391,12 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
         ctx->launches++;
     }
     if (ev_mid) cudaEventRecord(ev_mid, st);
-    if (plan.mode == MODE_MSE) {
+    if (plan.mode == MODE_MSE && plan.raw_sums) {
+        e = launch_finalize_sums(dev->base.progs, dev->base.partials, n, plan.gradient ? 33u : 1u,
+                                 (double *)dev->out.p, st);
+        if (e != cudaSuccess) return cuda_fail(e, "finalize launch");
+        ctx->launches++;
+    } else if (plan.mode == MODE_MSE) {
         if (plan.gradient)
             e = launch_finalize_grad(dev->base.progs, dev->base.datasets, dev->base.partials, n, dev->mse, dev->grad, st);
         else
@@ -667,6 +673,48 @@ int rsr_eval_mse_grad_batch(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaSetDevice(ctx->device);
     return run_oneshot(ctx, *pop, dsp, ds, RSR_KERNEL_AUTO, true, MODE_MSE, mse_out, grad_out, nullptr);
+}
+
+int rsr_eval_sums_batch(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const rsr_dataset *dsp,
+                        int gradient, double *sums_out) {
+    if (!ctx || !pop || (!sums_out && pop->n_programs)) return fail(RSR_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    Plan plan;
+    int rc = build_plan(ctx, *pop, dsp, ds, RSR_KERNEL_AUTO, gradient != 0, MODE_MSE, &plan);
+    if (rc) return rc;
+    plan.raw_sums = true;
+    const size_t n = plan.progs.size();
+    if (n == 0) return RSR_OK;
+    if ((rc = upload_plan(ctx, plan, &ctx->scratch, ctx->stream))) return rc;
+    if ((rc = enqueue_plan(ctx, plan, &ctx->scratch, ctx->stream, nullptr))) return rc;
+    const size_t stride = gradient ? 33 : 1;
+    std::vector<double> tmp(n * stride);
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(tmp.data(), ctx->scratch.out.p, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                             ctx->stream)) != cudaSuccess)
+        return cuda_fail(e, "sums download");
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(e, "evaluation");
+    ctx->last_d2h = tmp.size() * sizeof(double);
+    for (size_t li = 0; li < n; ++li)
+        memcpy(sums_out + (size_t)plan.orig[li] * stride, tmp.data() + li * stride, stride * sizeof(double));
+    return RSR_OK;
+}
+
+int rsr_finalize_sums(uint32_t n, int gradient, const double *sums, uint64_t num_samples, float *mse_out,
+                      float *grad_out) {
+    if ((!sums || !mse_out || (gradient && !grad_out)) && n) return fail(RSR_EINVAL, "null argument");
+    const size_t stride = gradient ? 33 : 1;
+    const double ns = (double)num_samples;
+    for (uint32_t p = 0; p < n; ++p) {
+        const double s = sums[p * stride];
+        const float m = (float)(s / ns);
+        const bool bad = !(s <= (double)FLT_MAX) || !std::isfinite(m);
+        mse_out[p] = bad ? FLT_MAX : m;
+        if (gradient)
+            for (int k = 0; k < 32; ++k) grad_out[(size_t)p * 32 + k] = bad ? 0.0f : (float)(sums[p * stride + 1 + k] / ns);
+    }
+    return RSR_OK;
 }
 
 int rsr_eval_points_batch(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, int kernel, float *out) {

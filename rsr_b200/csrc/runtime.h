@@ -90,6 +90,7 @@ struct Plan {
     std::vector<Group> groups;
     uint32_t n_partials = 0;                // doubles (gradient: 33 per slot)
     bool gradient = false;
+    bool raw_sums = false;                  // MODE_MSE: unscaled f64 sums instead of the epilogue
     int mode = MODE_MSE;
     uint64_t points_stride = 0;
     uint64_t flops = 0;                     // algorithmic lane-ops of one run

@@ -54,7 +54,10 @@ class Server:
         j.pop = C.pointer(pop)
         dsp = None
         if datasets is not None:
-            dsp = np.asarray([self.engine._ds(d).handle for d in datasets], np.uint64)
+            if isinstance(datasets, np.ndarray) and datasets.dtype == np.uint64:
+                dsp = np.ascontiguousarray(datasets)  # device handles already
+            else:
+                dsp = np.asarray([self.engine._ds(d).handle for d in datasets], np.uint64)
             j.ds_per_program = dsp.ctypes.data_as(C.POINTER(C.c_uint64))
         else:
             j.ds = self.engine._ds(dataset).handle
