@@ -10,7 +10,7 @@ namespace rsr {
 
 constexpr int kPlainThreads = 128;  // 4 warps per block, one work item per warp
 constexpr int kRegThreads = 256;  // 8 warps share one work item
-constexpr int kGradThreads = 64;
+constexpr int kGradThreads = 32;  // one warp per block, one item per warp
 
 cudaError_t launch_plain(const LaunchArgs &a, int P, uint32_t warps_per_block, size_t smem, cudaStream_t st);
 size_t plain_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t slots, int P);

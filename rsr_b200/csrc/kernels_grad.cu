@@ -44,6 +44,20 @@ struct TapeCtx {
     __device__ __forceinline__ Vf<P> X(uint32_t f) const { return load_pts<P>(x + f * stride + p0); }
 };
 
+// Element-wise vector/matrix ops with the width known at compile time, so
+// that their operands stay in registers.
+template <int P, int W, bool SUB>
+__device__ __forceinline__ void fwd_addsub(const TapeCtx<P> &t, uint32_t o, uint32_t i0, uint32_t i1) {
+#pragma unroll
+    for (int i = 0; i < W; ++i) t.SV(o + i, SUB ? t.V(i0 + i) - t.V(i1 + i) : t.V(i0 + i) + t.V(i1 + i));
+}
+template <int P, int W>
+__device__ __forceinline__ void fwd_scale(const TapeCtx<P> &t, uint32_t o, uint32_t i0, uint32_t i1) {
+    const Vf<P> s = t.V(i0);
+#pragma unroll
+    for (int i = 0; i < W; ++i) t.SV(o + i, t.V(i1 + i) * s);
+}
+
 // Forward value of one tape instruction (same semantics as the slot kernel).
 template <int P>
 __device__ __forceinline__ void tape_forward(const TapeCtx<P> &t, uint32_t w0, uint32_t w1, uint32_t w2) {
@@ -83,19 +97,18 @@ __device__ __forceinline__ void tape_forward(const TapeCtx<P> &t, uint32_t w0, u
         case GET_X_V2: case GET_X_V3: t.SV(o, t.V(i0)); break;
         case GET_Y_V2: case GET_Y_V3: t.SV(o, t.V(i0 + 1)); break;
         case GET_Z_V3: t.SV(o, t.V(i0 + 2)); break;
-        case ADD_V2: case ADD_V3: case ADD_M2: case ADD_M3: {
-            const int w = op == ADD_V2 ? 2 : op == ADD_V3 ? 3 : op == ADD_M2 ? 4 : 9;
-            Ln(A, i0, w); Ln(B, i1, w); for (int i = 0; i < w; ++i) R[i] = A[i] + B[i]; Sn(o, R, w); break;
-        }
-        case SUB_V2: case SUB_V3: case SUB_M2: case SUB_M3: {
-            const int w = op == SUB_V2 ? 2 : op == SUB_V3 ? 3 : op == SUB_M2 ? 4 : 9;
-            Ln(A, i0, w); Ln(B, i1, w); for (int i = 0; i < w; ++i) R[i] = A[i] - B[i]; Sn(o, R, w); break;
-        }
-        case SCALE_V2: case SCALE_V3: case SCALE_M2: case SCALE_M3: {
-            const int w = op == SCALE_V2 ? 2 : op == SCALE_V3 ? 3 : op == SCALE_M2 ? 4 : 9;
-            const Vf<P> s = t.V(i0);
-            Ln(A, i1, w); for (int i = 0; i < w; ++i) R[i] = A[i] * s; Sn(o, R, w); break;
-        }
+        case ADD_V2: fwd_addsub<P, 2, false>(t, o, i0, i1); break;
+        case ADD_V3: fwd_addsub<P, 3, false>(t, o, i0, i1); break;
+        case ADD_M2: fwd_addsub<P, 4, false>(t, o, i0, i1); break;
+        case ADD_M3: fwd_addsub<P, 9, false>(t, o, i0, i1); break;
+        case SUB_V2: fwd_addsub<P, 2, true>(t, o, i0, i1); break;
+        case SUB_V3: fwd_addsub<P, 3, true>(t, o, i0, i1); break;
+        case SUB_M2: fwd_addsub<P, 4, true>(t, o, i0, i1); break;
+        case SUB_M3: fwd_addsub<P, 9, true>(t, o, i0, i1); break;
+        case SCALE_V2: fwd_scale<P, 2>(t, o, i0, i1); break;
+        case SCALE_V3: fwd_scale<P, 3>(t, o, i0, i1); break;
+        case SCALE_M2: fwd_scale<P, 4>(t, o, i0, i1); break;
+        case SCALE_M3: fwd_scale<P, 9>(t, o, i0, i1); break;
         case DOT_V2: Ln(A, i0, 2); Ln(B, i1, 2); t.SV(o, dot2(A, B)); break;
         case DOT_V3: Ln(A, i0, 3); Ln(B, i1, 3); t.SV(o, dot3(A, B)); break;
         case NORM_V2: Ln(A, i0, 2); t.SV(o, norm2(A)); break;
@@ -143,6 +156,44 @@ __device__ __forceinline__ void inverse_adjoint(const TapeCtx<P> &t, uint32_t o,
             for (int k = 0; k < P; ++k) d.v[k] = fabsf(det.v[k]) < 1e-9f ? 0.0f : -s.v[k];
             t.AddA(i0 + N * j + i, d);
         }
+}
+
+// O = A B (N x N, column-major): dA = G B^T, dB = A^T G.
+template <int P, int N>
+__device__ __forceinline__ void rev_mulm(const TapeCtx<P> &t, uint32_t o, uint32_t i0, uint32_t i1) {
+    Vf<P> Am[N * N], Bm[N * N], G[N * N];
+#pragma unroll
+    for (int i = 0; i < N * N; ++i) { Am[i] = t.V(i0 + i); Bm[i] = t.V(i1 + i); G[i] = t.A(o + i); }
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int c = 0; c < N; ++c) {
+            Vf<P> da = splat<P>(0.0f), db = splat<P>(0.0f);
+#pragma unroll
+            for (int j = 0; j < N; ++j) {
+                da = da + G[N * j + r] * Bm[N * j + c];   // G(r,j) B(c,j)
+                db = db + Am[N * r + j] * G[N * c + j];   // A(j,r) G(j,c)
+            }
+            t.AddA(i0 + N * c + r, da);
+            t.AddA(i1 + N * c + r, db);
+        }
+}
+// o = M v: dM(r,c) += g_r v_c, dv_c += sum_r M(r,c) g_r.
+template <int P, int N>
+__device__ __forceinline__ void rev_mulmv(const TapeCtx<P> &t, uint32_t o, uint32_t i0, uint32_t i1) {
+    Vf<P> g[N], v[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) { g[i] = t.A(o + i); v[i] = t.V(i1 + i); }
+#pragma unroll
+    for (int c = 0; c < N; ++c) {
+        Vf<P> dv = splat<P>(0.0f);
+#pragma unroll
+        for (int r = 0; r < N; ++r) {
+            t.AddA(i0 + N * c + r, g[r] * v[c]);
+            dv = dv + t.V(i0 + N * c + r) * g[r];
+        }
+        t.AddA(i1 + c, dv);
+    }
 }
 
 // Reverse sweep of one tape instruction.  gacc: this lane's f32 gradient
@@ -244,36 +295,10 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, uint32_t w0, u
         case MAKE_MAT3:
             for (int i = 0; i < 3; ++i) { t.AddA(i0 + i, t.A(o + i)); t.AddA(i1 + i, t.A(o + 3 + i)); t.AddA(i2 + i, t.A(o + 6 + i)); }
             break;
-        case MUL_M2: case MUL_M3: {  // O = A B: dA = G B^T, dB = A^T G
-            const int N = op == MUL_M2 ? 2 : 3;
-            Vf<P> Am[9], Bm[9], G[9];
-            for (int i = 0; i < N * N; ++i) { Am[i] = t.V(i0 + i); Bm[i] = t.V(i1 + i); G[i] = t.A(o + i); }
-            for (int r = 0; r < N; ++r)
-                for (int c = 0; c < N; ++c) {
-                    Vf<P> da = splat<P>(0.0f), db = splat<P>(0.0f);
-                    for (int j = 0; j < N; ++j) {
-                        da = da + G[N * j + r] * Bm[N * j + c];   // G(r,j) B(c,j)
-                        db = db + Am[N * r + j] * G[N * c + j];   // A(j,r) G(j,c)
-                    }
-                    t.AddA(i0 + N * c + r, da);
-                    t.AddA(i1 + N * c + r, db);
-                }
-            break;
-        }
-        case MUL_M2V2: case MUL_M3V3: {  // o = M v: dM(r,c) += g_r v_c, dv_c += sum_r M(r,c) g_r
-            const int N = op == MUL_M2V2 ? 2 : 3;
-            Vf<P> g[3], v[3];
-            for (int i = 0; i < N; ++i) { g[i] = t.A(o + i); v[i] = t.V(i1 + i); }
-            for (int c = 0; c < N; ++c) {
-                Vf<P> dv = splat<P>(0.0f);
-                for (int r = 0; r < N; ++r) {
-                    t.AddA(i0 + N * c + r, g[r] * v[c]);
-                    dv = dv + t.V(i0 + N * c + r) * g[r];
-                }
-                t.AddA(i1 + c, dv);
-            }
-            break;
-        }
+        case MUL_M2: rev_mulm<P, 2>(t, o, i0, i1); break;
+        case MUL_M3: rev_mulm<P, 3>(t, o, i0, i1); break;
+        case MUL_M2V2: rev_mulmv<P, 2>(t, o, i0, i1); break;
+        case MUL_M3V3: rev_mulmv<P, 3>(t, o, i0, i1); break;
         case DET_M2: {
             const Vf<P> g = t.A(o);
             t.AddA(i0, g * t.V(i0 + 3));
@@ -309,18 +334,19 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, uint32_t w0, u
 }
 
 template <int P>
-__global__ void __launch_bounds__(kGradThreads) grad_kernel(const LaunchArgs a) {
+__global__ void __launch_bounds__(kGradThreads, 16) grad_kernel(const LaunchArgs a) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t item_id = blockIdx.x * (blockDim.x >> 5) + warp;
     if (item_id >= a.n_items) return;
     const uint32_t cw = align4g(a.smem_code_words), cf = align4g(a.smem_const_floats);
-    const uint32_t region = cw + cf + kGradParams * 32u + 2u * a.smem_slots * 32u * P;
+    const uint32_t gp = min(kGradParams, a.smem_const_floats);
+    const uint32_t region = cw + cf + gp * 32u + 2u * a.smem_slots * 32u * P;
     float *base = smem + (size_t)warp * region;
     uint32_t *scode = reinterpret_cast<uint32_t *>(base);
     float *sconst = base + cw;
-    float *gacc = sconst + cf;  // [param][lane] f32, per tile
-    Vf<P> *val = reinterpret_cast<Vf<P> *>(gacc + kGradParams * 32u);
+    float *gacc = sconst + cf;  // [param][lane] f32 gradient sums of this item's tiles
+    Vf<P> *val = reinterpret_cast<Vf<P> *>(gacc + gp * 32u);
     Vf<P> *adj = val + (size_t)a.smem_slots * 32u;
 
     const WorkItem it = a.items[item_id];
@@ -329,20 +355,17 @@ __global__ void __launch_bounds__(kGradThreads) grad_kernel(const LaunchArgs a) 
     const DatasetDesc ds = a.datasets[pd.dataset];
     for (uint32_t i = lane; i < pd.uop_len; i += 32) scode[i] = __ldg(a.code + pd.uop_off + i);
     for (uint32_t i = lane; i < pd.n_consts; i += 32) sconst[i] = __ldg(a.consts + pd.const_off + i);
+    const uint32_t np = min(pd.n_consts, kGradParams);
+    for (uint32_t k = 0; k < np; ++k) gacc[k * 32 + lane] = 0.0f;
     __syncwarp();
     const uint32_t result = scode[0];
     const uint32_t *code = scode + 1;
     const uint32_t n_nodes = (pd.uop_len - 1) / 3;
     TapeCtx<P> t{val, adj, sconst, ds.x, ds.stride, 0, ds.n_eval, lane};
     Kahan sse;
-    double gsum[kGradParams];
-#pragma unroll
-    for (int k = 0; k < (int)kGradParams; ++k) gsum[k] = 0.0;
-    const uint32_t np = min(pd.n_consts, kGradParams);
     for (uint32_t tile = it.tile_begin; tile < it.tile_end; ++tile) {
         t.p0 = (uint64_t)tile * (32u * P) + (uint64_t)lane * P;
-        for (uint32_t k = 0; k < np; ++k) gacc[k * 32 + lane] = 0.0f;
-        // forward sweep, adjoints cleared on the way
+        // forward sweep, then the adjoints cleared
         for (uint32_t i = 0; i < n_nodes; ++i) tape_forward<P>(t, code[3 * i], code[3 * i + 1], code[3 * i + 2]);
         for (uint32_t s = 0; s < pd.n_tape; ++s) adj[s * 32 + lane] = splat<P>(0.0f);
         const Vf<P> pred = result == 0xFFFFFFFFu ? splat<P>(0.0f) : t.V(result);
@@ -357,19 +380,15 @@ __global__ void __launch_bounds__(kGradThreads) grad_kernel(const LaunchArgs a) 
         }
         if (result == 0xFFFFFFFFu) continue;
         t.AddA(result, seed);
-        // reverse sweep
+        // reverse sweep; constant loads add their adjoints to gacc
         for (uint32_t i = n_nodes; i-- > 0;)
             tape_reverse<P>(t, code[3 * i], code[3 * i + 1], code[3 * i + 2], gacc + lane);
-#pragma unroll
-        for (int k = 0; k < (int)kGradParams; ++k)
-            if ((uint32_t)k < np) gsum[k] += (double)gacc[k * 32 + lane];
     }
     double *out = a.partials + (size_t)(pd.part_off + it.chunk) * (1 + kGradParams);
     const double s = warp_sum(sse.value());
     if (lane == 0) out[0] = s;
-#pragma unroll
-    for (int k = 0; k < (int)kGradParams; ++k) {
-        const double g = warp_sum(gsum[k]);
+    for (uint32_t k = 0; k < kGradParams; ++k) {
+        const double g = k < np ? warp_sum((double)gacc[k * 32 + lane]) : 0.0;
         if (lane == 0) out[1 + k] = g;
     }
 }
@@ -409,7 +428,8 @@ cudaError_t launch_grad(const LaunchArgs &a, uint32_t wpb, size_t smem, cudaStre
 }
 
 size_t grad_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t tape_slots) {
-    return ((size_t)align4g(code_words) + align4g(const_floats) + kGradParams * 32u + 2u * (size_t)tape_slots * 32u) * 4u;
+    const uint32_t gp = const_floats < kGradParams ? const_floats : kGradParams;
+    return ((size_t)align4g(code_words) + align4g(const_floats) + gp * 32u + 2u * (size_t)tape_slots * 32u) * 4u;
 }
 
 cudaError_t launch_finalize_grad(const ProgDesc *progs, const DatasetDesc *ds, const double *partials, uint32_t n,

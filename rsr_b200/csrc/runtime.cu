@@ -142,7 +142,12 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
     // path per program: -2 adjoint, -1 plain, >= 0 register profile
     std::vector<int> path(n);
     for (uint32_t i = 0; i < n; ++i) {
-        if (gradient) path[i] = -2;
+        if (gradient) {
+            // adjoint launches by tape size, so that a block's shared memory
+            // follows its own programs' tapes: <= 32, 64, 128, 256, more slots
+            const uint32_t nt = enc[i].n_tape_slots;
+            path[i] = nt <= 32 ? -2 : nt <= 64 ? -3 : nt <= 128 ? -4 : nt <= 256 ? -5 : -6;
+        }
         else if (kernel == RSR_KERNEL_PLAIN || enc[i].profile < 0) path[i] = -1;
         else {
             // the register kernel's spill stacks for 2 points per lane must fit
@@ -167,7 +172,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
     for (uint32_t li = 0; li < n; ++li) {
         const uint32_t i = order[li];
         const EncodedProgram &E = enc[i];
-        const std::vector<uint32_t> &code = path[i] == -2 ? E.tape_code : path[i] == -1 ? E.slot_code : E.reg_code;
+        const std::vector<uint32_t> &code = path[i] <= -2 ? E.tape_code : path[i] == -1 ? E.slot_code : E.reg_code;
         ProgDesc d{};
         d.uop_off = (uint32_t)P.code.size();
         d.uop_len = (uint32_t)code.size();
@@ -196,7 +201,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         uint32_t end = li;
         while (end < n && path[order[end]] == pth) ++end;
         Group g;
-        g.kind = pth == -2 ? 2 : pth == -1 ? 0 : 1;
+        g.kind = pth <= -2 ? 2 : pth == -1 ? 0 : 1;
         g.profile = pth >= 0 ? pth : -1;
         g.item_begin = (uint32_t)P.items.size();
         if (g.kind == 1) {
@@ -244,7 +249,9 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                 g.P >>= 1;
         // points per thread of slot-file kernels: largest that fits the smem budget
         if (g.kind != 1) {
-            const size_t budget = 110 * 1024;
+            // adjoint: two points per lane while eight warps' tapes still fit
+            // an SM; the tape's shared memory bounds the adjoint's occupancy
+            const size_t budget = g.kind == 2 ? 27 * 1024 : 110 * 1024;
             int Pp = g.kind == 2 ? 2 : 4;
             while (Pp > 1) {
                 size_t per = g.kind == 2 ? grad_smem_per_warp(g.code_words, g.const_floats, g.slots)
@@ -379,7 +386,9 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
         } else {
             size_t per = grad_smem_per_warp(g.code_words, g.const_floats, g.slots);
             per += (size_t)g.slots * 32u * 4u * (g.P - 1) * 2u;
-            uint32_t wpb = (uint32_t)std::max<size_t>(1, std::min<size_t>(kGradThreads / 32, (200 * 1024) / per));
+            // one warp per block: blocks as small as a tape, so an SM packs as
+            // many tapes as its shared memory holds
+            const uint32_t wpb = 1;
             a.progs_per_warp = (uint32_t)g.P;  // adjoint kernel reads P from here
             g.grid = (g.n_items + wpb - 1) / wpb;
             g.smem = per * wpb;
