@@ -74,6 +74,118 @@ struct Node {
 
 bool leaf(const Node &n) { return is_load(n.opcode) && !n.stale; }
 
+// Values that an opcode's reverse rule reads (the adjoint kernel's
+// tape_reverse): bit k < 3 for input k, bit 3 for the output.
+int reverse_reads(int op) {
+    switch (op) {
+        case MUL_F: return 1 | 2;
+        case DIV_F: return 2 | 8;
+        case SIN_F: case COS_F: case SQR_F: case LN_F: return 1;
+        case EXP_F: case SQRT_F: return 8;
+        case SCALE_V2: case SCALE_V3: case SCALE_M2: case SCALE_M3: return 1 | 2;
+        case DOT_V2: case DOT_V3: case CROSS_V3: return 1 | 2;
+        case NORM_V2: case NORM_V3: return 1 | 8;
+        case MUL_M2: case MUL_M3: case MUL_M2V2: case MUL_M3V3: return 1 | 2;
+        case DET_M2: case DET_M3: return 1;
+        case INVERSE_M2: case INVERSE_M3: return 1 | 8;
+        default: return 0;
+    }
+}
+
+// First-fit allocation of runs of `width` slots over time intervals: a slot
+// is free for an interval starting at t0 when its last holder ended before t0.
+struct SlotPool {
+    std::vector<int> busy_until;  // per slot, -1 = never used
+    uint32_t take(int width, int t0, int t1) {
+        for (uint32_t s = 0;; ++s) {
+            bool ok = true;
+            for (int k = 0; k < width && ok; ++k)
+                ok = s + k >= busy_until.size() || busy_until[s + k] < t0;
+            if (!ok) continue;
+            if (busy_until.size() < s + width) busy_until.resize(s + width, -1);
+            for (int k = 0; k < width; ++k) busy_until[s + k] = t1;
+            return s;
+        }
+    }
+};
+
+// Tape form for the adjoint kernel.  Live nodes in program order; node t runs
+// forward at time t and in reverse at time 2N-1-t.  A value slot lives from
+// its definition to its last forward read, or to the reverse step of the
+// last node whose reverse rule reads it; an adjoint slot lives from the
+// reverse step of its latest consumer (its first contribution) to its own
+// reverse step, after which the kernel zeroes it.  Feature loads keep no
+// adjoint: their contributions go to a sink run of 9 slots at 0 that is
+// never read.  Words: header (result value slot, result adjoint slot), then
+// 5 per node: op | aux << 8 | out_width << 28, vo | ao << 16, and
+// vi | ai << 16 for inputs 0..2.
+void emit_tape(const std::vector<Node> &nodes, const std::vector<char> &live, int root, EncodedProgram *E) {
+    std::vector<int> idx;  // tape order -> node id
+    std::vector<int> pos(nodes.size(), -1);
+    for (size_t i = 0; i < nodes.size(); ++i)
+        if (live[i]) {
+            pos[i] = (int)idx.size();
+            idx.push_back((int)i);
+        }
+    const int N = (int)idx.size();
+    const int rev = 2 * N - 1;
+    std::vector<int> vend(N, -1), astart(N, 1 << 30);
+    for (int t = 0; t < N; ++t) {
+        const Node &n = nodes[idx[t]];
+        const int rr = n.stale ? 0 : reverse_reads(n.opcode);
+        if (rr & 8) vend[t] = std::max(vend[t], rev - t);
+        auto use = [&](int in_node, int k) {
+            const int u = pos[in_node];
+            vend[u] = std::max(vend[u], t);                                // forward read
+            if (k >= 0 && ((rr >> k) & 1)) vend[u] = std::max(vend[u], rev - t);
+            astart[u] = std::min(astart[u], rev - t);                      // adjoint contribution
+        };
+        if (n.stale) {
+            if (n.alias >= 0) use(n.alias, -1);
+        } else {
+            for (int k = 0; k < n.n_in; ++k) use(n.in[k], k);
+        }
+    }
+    const int rt = root >= 0 ? pos[root] : -1;
+    if (rt >= 0) {
+        vend[rt] = std::max(vend[rt], N);          // read for the prediction
+        astart[rt] = std::min(astart[rt], N - 1);  // seeded before the reverse sweep
+    }
+    SlotPool vals, adjs;
+    adjs.take(9, -1, 1 << 30);  // the sink
+    std::vector<uint32_t> vs(N, 0), as(N, 0);
+    for (int t = 0; t < N; ++t) vs[t] = vals.take(kStackWidth[nodes[idx[t]].out], t, std::max(vend[t], t));
+    for (int t = N - 1; t >= 0; --t) {  // adjoint intervals start in reverse node order
+        const Node &n = nodes[idx[t]];
+        const bool feature = !n.stale && is_load(n.opcode) && !is_const_load(n.opcode);
+        if (feature || astart[t] > rev - t) continue;  // sink
+        as[t] = adjs.take(kStackWidth[n.out], astart[t], rev - t);
+    }
+    E->n_tape_val = (uint32_t)vals.busy_until.size();
+    E->n_tape_adj = (uint32_t)adjs.busy_until.size();
+    E->tape_code.clear();
+    E->tape_code.push_back(rt >= 0 ? vs[rt] : 0xFFFFFFFFu);
+    E->tape_code.push_back(rt >= 0 ? as[rt] : 0u);
+    for (int t = 0; t < N; ++t) {
+        const Node &n = nodes[idx[t]];
+        uint32_t w0, in[3] = {0, 0, 0};
+        if (n.stale) {
+            // copy of the value left in that slot, or zero; aux = has_alias | width << 1
+            w0 = (uint32_t)SLOT_NOP | (((n.alias >= 0 ? 1u : 0u) | ((uint32_t)kStackWidth[n.out] << 1)) << 8);
+            if (n.alias >= 0) in[0] = vs[pos[n.alias]] | (as[pos[n.alias]] << 16);
+        } else {
+            w0 = (uint32_t)n.opcode | (n.arg << 8);
+            for (int k = 0; k < n.n_in; ++k) in[k] = vs[pos[n.in[k]]] | (as[pos[n.in[k]]] << 16);
+        }
+        w0 |= (uint32_t)kStackWidth[n.out] << 28;
+        E->tape_code.push_back(w0);
+        E->tape_code.push_back(vs[t] | (as[t] << 16));
+        E->tape_code.push_back(in[0]);
+        E->tape_code.push_back(in[1]);
+        E->tape_code.push_back(in[2]);
+    }
+}
+
 }  // namespace
 
 const OpSig &op_sig(int opcode) { return sigs().s[opcode]; }
@@ -507,34 +619,8 @@ int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uin
         if (n.stale) E.needs_zero_init = true;
     }
 
-    // ---- tape form: every live value gets its own slots (SSA)
-    {
-        std::vector<uint32_t> tslot(nodes.size(), 0);
-        uint32_t tacc = 0;
-        for (size_t i = 0; i < nodes.size(); ++i) {
-            if (!live[i]) continue;
-            tslot[i] = tacc;
-            tacc += kStackWidth[nodes[i].out];
-        }
-        E.n_tape_slots = tacc;
-        E.tape_code.push_back(root >= 0 ? tslot[root] : 0xFFFFFFFFu);  // header: result slot
-        for (size_t i = 0; i < nodes.size(); ++i) {
-            if (!live[i]) continue;
-            const Node &n = nodes[i];
-            uint32_t w0, in[3] = {0, 0, 0};
-            if (n.stale) {
-                // copy of the value left in that slot, or zero; aux = has_alias | width << 1
-                w0 = (uint32_t)SLOT_NOP | (((n.alias >= 0 ? 1u : 0u) | ((uint32_t)kStackWidth[n.out] << 1)) << 8);
-                if (n.alias >= 0) in[0] = tslot[n.alias];
-            } else {
-                w0 = (uint32_t)n.opcode | (n.arg << 8);
-                for (int k = 0; k < n.n_in; ++k) in[k] = tslot[n.in[k]];
-            }
-            E.tape_code.push_back(w0);
-            E.tape_code.push_back(tslot[i] | (in[0] << 16));
-            E.tape_code.push_back(in[1] | (in[2] << 16));
-        }
-    }
+    // ---- tape form: value and adjoint slots allocated by lifetime
+    emit_tape(nodes, live, root, &E);
 
     // ---- accumulator form
     if (root >= 0 && !has_stale_live && n_params < (1u << kLdOffsetBits)) {

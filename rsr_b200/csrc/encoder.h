@@ -43,8 +43,8 @@ struct EncodedProgram {
     int depth_fast[N_STACKS] = {0, 0, 0, 0, 0};
     std::vector<uint32_t> reg_code;
     // adjoint (slot form with one slot range per value, never reused)
-    std::vector<uint32_t> tape_code;      // 3 words per instruction, SSA slots
-    uint32_t n_tape_slots = 0;
+    std::vector<uint32_t> tape_code;      // 2 header words + 5 words per live node
+    uint32_t n_tape_val = 0, n_tape_adj = 0;  // scalar value / adjoint slots
 };
 
 // Validates and encodes.  num_features == 0 skips feature-range checks.

@@ -27,7 +27,8 @@ struct LaunchArgs {
     uint32_t mode;
     uint32_t smem_code_words; // per warp
     uint32_t smem_const_floats;
-    uint32_t smem_slots;      // per warp (slot-file kernels)
+    uint32_t smem_slots;      // per warp (slot-file kernels; adjoint: value slots)
+    uint32_t smem_adj_slots;  // per warp (adjoint: adjoint slots)
     uint32_t progs_per_warp;
     // register kernel: per-warp shared-memory layout (floats)
     uint32_t region_floats;   // per warp

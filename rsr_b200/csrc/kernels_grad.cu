@@ -60,9 +60,9 @@ __device__ __forceinline__ void fwd_scale(const TapeCtx<P> &t, uint32_t o, uint3
 
 // Forward value of one tape instruction (same semantics as the slot kernel).
 template <int P>
-__device__ __forceinline__ void tape_forward(const TapeCtx<P> &t, uint32_t w0, uint32_t w1, uint32_t w2) {
-    const uint32_t op = w0 & 0xFFu, aux = w0 >> 8;
-    const uint32_t o = w1 & 0xFFFFu, i0 = w1 >> 16, i1 = w2 & 0xFFFFu, i2 = w2 >> 16;
+__device__ __forceinline__ void tape_forward(const TapeCtx<P> &t, const uint32_t *w) {
+    const uint32_t op = w[0] & 0xFFu, aux = (w[0] >> 8) & 0xFFFFFu;
+    const uint32_t o = w[1] & 0xFFFFu, i0 = w[2] & 0xFFFFu, i1 = w[3] & 0xFFFFu, i2 = w[4] & 0xFFFFu;
     Vf<P> A[9], B[9], R[9];
     auto Ln = [&](Vf<P> *d, uint32_t s, int n) { for (int i = 0; i < n; ++i) d[i] = t.V(s + i); };
     auto Sn = [&](uint32_t s, const Vf<P> *v, int n) { for (int i = 0; i < n; ++i) t.SV(s + i, v[i]); };
@@ -134,9 +134,9 @@ __device__ __forceinline__ void tape_forward(const TapeCtx<P> &t, uint32_t w0, u
 
 // dA = -O^T G O^T for O = A^-1 (N x N, column-major), zero where singular.
 template <int P, int N>
-__device__ __forceinline__ void inverse_adjoint(const TapeCtx<P> &t, uint32_t o, uint32_t i0) {
+__device__ __forceinline__ void inverse_adjoint(const TapeCtx<P> &t, uint32_t vo, uint32_t ao, uint32_t v0, uint32_t a0) {
     Vf<P> O[N * N], G[N * N], H[N * N], M[N * N];
-    for (int i = 0; i < N * N; ++i) { O[i] = t.V(o + i); G[i] = t.A(o + i); M[i] = t.V(i0 + i); }
+    for (int i = 0; i < N * N; ++i) { O[i] = t.V(vo + i); G[i] = t.A(ao + i); M[i] = t.V(v0 + i); }
     Vf<P> det;
     if constexpr (N == 2) det = det_m2(M); else det = det_m3(M);
     // H = O^T G : H(i,l) = sum_k O(k,i) G(k,l)
@@ -154,16 +154,17 @@ __device__ __forceinline__ void inverse_adjoint(const TapeCtx<P> &t, uint32_t o,
             Vf<P> d;
 #pragma unroll
             for (int k = 0; k < P; ++k) d.v[k] = fabsf(det.v[k]) < 1e-9f ? 0.0f : -s.v[k];
-            t.AddA(i0 + N * j + i, d);
+            t.AddA(a0 + N * j + i, d);
         }
 }
 
 // O = A B (N x N, column-major): dA = G B^T, dB = A^T G.
 template <int P, int N>
-__device__ __forceinline__ void rev_mulm(const TapeCtx<P> &t, uint32_t o, uint32_t i0, uint32_t i1) {
+__device__ __forceinline__ void rev_mulm(const TapeCtx<P> &t, uint32_t vo, uint32_t ao, uint32_t v0, uint32_t a0, uint32_t v1,
+                                         uint32_t a1) {
     Vf<P> Am[N * N], Bm[N * N], G[N * N];
 #pragma unroll
-    for (int i = 0; i < N * N; ++i) { Am[i] = t.V(i0 + i); Bm[i] = t.V(i1 + i); G[i] = t.A(o + i); }
+    for (int i = 0; i < N * N; ++i) { Am[i] = t.V(v0 + i); Bm[i] = t.V(v1 + i); G[i] = t.A(ao + i); }
 #pragma unroll
     for (int r = 0; r < N; ++r)
 #pragma unroll
@@ -174,38 +175,40 @@ __device__ __forceinline__ void rev_mulm(const TapeCtx<P> &t, uint32_t o, uint32
                 da = da + G[N * j + r] * Bm[N * j + c];   // G(r,j) B(c,j)
                 db = db + Am[N * r + j] * G[N * c + j];   // A(j,r) G(j,c)
             }
-            t.AddA(i0 + N * c + r, da);
-            t.AddA(i1 + N * c + r, db);
+            t.AddA(a0 + N * c + r, da);
+            t.AddA(a1 + N * c + r, db);
         }
 }
 // o = M v: dM(r,c) += g_r v_c, dv_c += sum_r M(r,c) g_r.
 template <int P, int N>
-__device__ __forceinline__ void rev_mulmv(const TapeCtx<P> &t, uint32_t o, uint32_t i0, uint32_t i1) {
+__device__ __forceinline__ void rev_mulmv(const TapeCtx<P> &t, uint32_t vo, uint32_t ao, uint32_t v0, uint32_t a0, uint32_t v1,
+                                          uint32_t a1) {
     Vf<P> g[N], v[N];
 #pragma unroll
-    for (int i = 0; i < N; ++i) { g[i] = t.A(o + i); v[i] = t.V(i1 + i); }
+    for (int i = 0; i < N; ++i) { g[i] = t.A(ao + i); v[i] = t.V(v1 + i); }
 #pragma unroll
     for (int c = 0; c < N; ++c) {
         Vf<P> dv = splat<P>(0.0f);
 #pragma unroll
         for (int r = 0; r < N; ++r) {
-            t.AddA(i0 + N * c + r, g[r] * v[c]);
-            dv = dv + t.V(i0 + N * c + r) * g[r];
+            t.AddA(a0 + N * c + r, g[r] * v[c]);
+            dv = dv + t.V(v0 + N * c + r) * g[r];
         }
-        t.AddA(i1 + c, dv);
+        t.AddA(a1 + c, dv);
     }
 }
 
 // Reverse sweep of one tape instruction.  gacc: this lane's f32 gradient
 // contributions of the tile (summed over its P points).
 template <int P>
-__device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, uint32_t w0, uint32_t w1, uint32_t w2,
-                                             float *gacc_lane) {
-    const uint32_t op = w0 & 0xFFu, aux = w0 >> 8;
-    const uint32_t o = w1 & 0xFFFFu, i0 = w1 >> 16, i1 = w2 & 0xFFFFu, i2 = w2 >> 16;
+__device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t *w, float *gacc_lane) {
+    const uint32_t op = w[0] & 0xFFu, aux = (w[0] >> 8) & 0xFFFFFu, width = w[0] >> 28;
+    const uint32_t vo = w[1] & 0xFFFFu, ao = w[1] >> 16;
+    const uint32_t v0 = w[2] & 0xFFFFu, a0 = w[2] >> 16, v1 = w[3] & 0xFFFFu, a1 = w[3] >> 16;
+    const uint32_t a2 = w[4] >> 16;
     switch (op) {
         case SLOT_NOP:
-            if (aux & 1u) for (uint32_t i = 0; i < (aux >> 1); ++i) t.AddA(i0 + i, t.A(o + i));
+            if (aux & 1u) for (uint32_t i = 0; i < (aux >> 1); ++i) t.AddA(a0 + i, t.A(ao + i));
             break;
         case LOAD_VAR_F: case LOAD_VAR_V2: case LOAD_VAR_V3: case LOAD_VAR_M2: case LOAD_VAR_M3: break;
         case LOAD_CONST_F: case LOAD_CONST_V2: case LOAD_CONST_V3: case LOAD_CONST_M2: case LOAD_CONST_M3: {
@@ -213,7 +216,7 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, uint32_t w0, u
                         : op == LOAD_CONST_M2 ? 4 : 9;
             for (int i = 0; i < w; ++i) {
                 if (aux + i >= kGradParams) break;
-                const Vf<P> g = t.A(o + i);
+                const Vf<P> g = t.A(ao + i);
                 float s = 0.0f;
 #pragma unroll
                 for (int k = 0; k < P; ++k)  // points past the dataset's end may carry 0*inf = NaN adjoints
@@ -222,115 +225,118 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, uint32_t w0, u
             }
             break;
         }
-        case ADD_F: { const Vf<P> g = t.A(o); t.AddA(i0, g); t.AddA(i1, g); break; }
-        case SUB_F: { const Vf<P> g = t.A(o); t.AddA(i0, g); t.AddA(i1, -g); break; }
-        case MUL_F: { const Vf<P> g = t.A(o); t.AddA(i0, g * t.V(i1)); t.AddA(i1, g * t.V(i0)); break; }
+        case ADD_F: { const Vf<P> g = t.A(ao); t.AddA(a0, g); t.AddA(a1, g); break; }
+        case SUB_F: { const Vf<P> g = t.A(ao); t.AddA(a0, g); t.AddA(a1, -g); break; }
+        case MUL_F: { const Vf<P> g = t.A(ao); t.AddA(a0, g * t.V(v1)); t.AddA(a1, g * t.V(v0)); break; }
         case DIV_F: {
-            const Vf<P> q = t.A(o) / t.V(i1);
-            t.AddA(i0, q);
-            t.AddA(i1, -(q * t.V(o)));
+            const Vf<P> q = t.A(ao) / t.V(v1);
+            t.AddA(a0, q);
+            t.AddA(a1, -(q * t.V(vo)));
             break;
         }
-        case SIN_F: t.AddA(i0, t.A(o) * vcos(t.V(i0))); break;
-        case COS_F: t.AddA(i0, t.A(o) * (-vsin(t.V(i0)))); break;
-        case EXP_F: t.AddA(i0, t.A(o) * t.V(o)); break;
-        case SQR_F: t.AddA(i0, t.A(o) * (splat<P>(2.0f) * t.V(i0))); break;
-        case SQRT_F: t.AddA(i0, t.A(o) / (splat<P>(2.0f) * t.V(o))); break;
-        case LN_F: t.AddA(i0, t.A(o) / t.V(i0)); break;
-        case MAKE_VEC2: t.AddA(i0, t.A(o)); t.AddA(i1, t.A(o + 1)); break;
-        case MAKE_VEC3: t.AddA(i0, t.A(o)); t.AddA(i1, t.A(o + 1)); t.AddA(i2, t.A(o + 2)); break;
-        case GET_X_V2: case GET_X_V3: t.AddA(i0, t.A(o)); break;
-        case GET_Y_V2: case GET_Y_V3: t.AddA(i0 + 1, t.A(o)); break;
-        case GET_Z_V3: t.AddA(i0 + 2, t.A(o)); break;
+        case SIN_F: t.AddA(a0, t.A(ao) * vcos(t.V(v0))); break;
+        case COS_F: t.AddA(a0, t.A(ao) * (-vsin(t.V(v0)))); break;
+        case EXP_F: t.AddA(a0, t.A(ao) * t.V(vo)); break;
+        case SQR_F: t.AddA(a0, t.A(ao) * (splat<P>(2.0f) * t.V(v0))); break;
+        case SQRT_F: t.AddA(a0, t.A(ao) / (splat<P>(2.0f) * t.V(vo))); break;
+        case LN_F: t.AddA(a0, t.A(ao) / t.V(v0)); break;
+        case MAKE_VEC2: t.AddA(a0, t.A(ao)); t.AddA(a1, t.A(ao + 1)); break;
+        case MAKE_VEC3: t.AddA(a0, t.A(ao)); t.AddA(a1, t.A(ao + 1)); t.AddA(a2, t.A(ao + 2)); break;
+        case GET_X_V2: case GET_X_V3: t.AddA(a0, t.A(ao)); break;
+        case GET_Y_V2: case GET_Y_V3: t.AddA(a0 + 1, t.A(ao)); break;
+        case GET_Z_V3: t.AddA(a0 + 2, t.A(ao)); break;
         case ADD_V2: case ADD_V3: case ADD_M2: case ADD_M3: case SUB_V2: case SUB_V3: case SUB_M2: case SUB_M3: {
             const bool sub = op == SUB_V2 || op == SUB_V3 || op == SUB_M2 || op == SUB_M3;
             const int w = (op == ADD_V2 || op == SUB_V2) ? 2 : (op == ADD_V3 || op == SUB_V3) ? 3
                         : (op == ADD_M2 || op == SUB_M2) ? 4 : 9;
             for (int i = 0; i < w; ++i) {
-                const Vf<P> g = t.A(o + i);
-                t.AddA(i0 + i, g);
-                t.AddA(i1 + i, sub ? -g : g);
+                const Vf<P> g = t.A(ao + i);
+                t.AddA(a0 + i, g);
+                t.AddA(a1 + i, sub ? -g : g);
             }
             break;
         }
         case SCALE_V2: case SCALE_V3: case SCALE_M2: case SCALE_M3: {
             const int w = op == SCALE_V2 ? 2 : op == SCALE_V3 ? 3 : op == SCALE_M2 ? 4 : 9;
-            const Vf<P> s = t.V(i0);
+            const Vf<P> s = t.V(v0);
             Vf<P> ds = splat<P>(0.0f);
             for (int i = 0; i < w; ++i) {
-                const Vf<P> g = t.A(o + i);
-                ds = ds + g * t.V(i1 + i);
-                t.AddA(i1 + i, g * s);
+                const Vf<P> g = t.A(ao + i);
+                ds = ds + g * t.V(v1 + i);
+                t.AddA(a1 + i, g * s);
             }
-            t.AddA(i0, ds);
+            t.AddA(a0, ds);
             break;
         }
         case DOT_V2: case DOT_V3: {
             const int w = op == DOT_V2 ? 2 : 3;
-            const Vf<P> g = t.A(o);
+            const Vf<P> g = t.A(ao);
             for (int i = 0; i < w; ++i) {
-                const Vf<P> a = t.V(i0 + i), b = t.V(i1 + i);
-                t.AddA(i0 + i, g * b);
-                t.AddA(i1 + i, g * a);
+                const Vf<P> a = t.V(v0 + i), b = t.V(v1 + i);
+                t.AddA(a0 + i, g * b);
+                t.AddA(a1 + i, g * a);
             }
             break;
         }
         case NORM_V2: case NORM_V3: {
             const int w = op == NORM_V2 ? 2 : 3;
-            const Vf<P> q = t.A(o) / t.V(o);
-            for (int i = 0; i < w; ++i) t.AddA(i0 + i, q * t.V(i0 + i));
+            const Vf<P> q = t.A(ao) / t.V(vo);
+            for (int i = 0; i < w; ++i) t.AddA(a0 + i, q * t.V(v0 + i));
             break;
         }
         case CROSS_V3: {  // o = a x b: da += b x g, db += g x a
             Vf<P> a[3], b[3], g[3], da[3], db[3];
-            for (int i = 0; i < 3; ++i) { a[i] = t.V(i0 + i); b[i] = t.V(i1 + i); g[i] = t.A(o + i); }
+            for (int i = 0; i < 3; ++i) { a[i] = t.V(v0 + i); b[i] = t.V(v1 + i); g[i] = t.A(ao + i); }
             cross3(b, g, da);
             cross3(g, a, db);
-            for (int i = 0; i < 3; ++i) { t.AddA(i0 + i, da[i]); t.AddA(i1 + i, db[i]); }
+            for (int i = 0; i < 3; ++i) { t.AddA(a0 + i, da[i]); t.AddA(a1 + i, db[i]); }
             break;
         }
         case MAKE_MAT2:
-            t.AddA(i0, t.A(o)); t.AddA(i0 + 1, t.A(o + 1)); t.AddA(i1, t.A(o + 2)); t.AddA(i1 + 1, t.A(o + 3));
+            t.AddA(a0, t.A(ao)); t.AddA(a0 + 1, t.A(ao + 1)); t.AddA(a1, t.A(ao + 2)); t.AddA(a1 + 1, t.A(ao + 3));
             break;
         case MAKE_MAT3:
-            for (int i = 0; i < 3; ++i) { t.AddA(i0 + i, t.A(o + i)); t.AddA(i1 + i, t.A(o + 3 + i)); t.AddA(i2 + i, t.A(o + 6 + i)); }
+            for (int i = 0; i < 3; ++i) { t.AddA(a0 + i, t.A(ao + i)); t.AddA(a1 + i, t.A(ao + 3 + i)); t.AddA(a2 + i, t.A(ao + 6 + i)); }
             break;
-        case MUL_M2: rev_mulm<P, 2>(t, o, i0, i1); break;
-        case MUL_M3: rev_mulm<P, 3>(t, o, i0, i1); break;
-        case MUL_M2V2: rev_mulmv<P, 2>(t, o, i0, i1); break;
-        case MUL_M3V3: rev_mulmv<P, 3>(t, o, i0, i1); break;
+        case MUL_M2: rev_mulm<P, 2>(t, vo, ao, v0, a0, v1, a1); break;
+        case MUL_M3: rev_mulm<P, 3>(t, vo, ao, v0, a0, v1, a1); break;
+        case MUL_M2V2: rev_mulmv<P, 2>(t, vo, ao, v0, a0, v1, a1); break;
+        case MUL_M3V3: rev_mulmv<P, 3>(t, vo, ao, v0, a0, v1, a1); break;
         case DET_M2: {
-            const Vf<P> g = t.A(o);
-            t.AddA(i0, g * t.V(i0 + 3));
-            t.AddA(i0 + 3, g * t.V(i0));
-            t.AddA(i0 + 1, -(g * t.V(i0 + 2)));
-            t.AddA(i0 + 2, -(g * t.V(i0 + 1)));
+            const Vf<P> g = t.A(ao);
+            t.AddA(a0, g * t.V(v0 + 3));
+            t.AddA(a0 + 3, g * t.V(v0));
+            t.AddA(a0 + 1, -(g * t.V(v0 + 2)));
+            t.AddA(a0 + 2, -(g * t.V(v0 + 1)));
             break;
         }
         case DET_M3: {  // d det / d m(r,c) = cofactor C(r,c)
-            const Vf<P> g = t.A(o);
+            const Vf<P> g = t.A(ao);
             Vf<P> m[9];
-            for (int i = 0; i < 9; ++i) m[i] = t.V(i0 + i);
+            for (int i = 0; i < 9; ++i) m[i] = t.V(v0 + i);
             for (int r = 0; r < 3; ++r)
                 for (int c = 0; c < 3; ++c) {
                     const int r1 = (r + 1) % 3, r2 = (r + 2) % 3, c1 = (c + 1) % 3, c2 = (c + 2) % 3;
                     const Vf<P> cof = m[3 * c1 + r1] * m[3 * c2 + r2] - m[3 * c2 + r1] * m[3 * c1 + r2];
-                    t.AddA(i0 + 3 * c + r, g * cof);
+                    t.AddA(a0 + 3 * c + r, g * cof);
                 }
             break;
         }
-        case TRACE_M2: { const Vf<P> g = t.A(o); t.AddA(i0, g); t.AddA(i0 + 3, g); break; }
-        case TRACE_M3: { const Vf<P> g = t.A(o); t.AddA(i0, g); t.AddA(i0 + 4, g); t.AddA(i0 + 8, g); break; }
+        case TRACE_M2: { const Vf<P> g = t.A(ao); t.AddA(a0, g); t.AddA(a0 + 3, g); break; }
+        case TRACE_M3: { const Vf<P> g = t.A(ao); t.AddA(a0, g); t.AddA(a0 + 4, g); t.AddA(a0 + 8, g); break; }
         case TRANSPOSE_M2: case TRANSPOSE_M3: {
             const int N = op == TRANSPOSE_M2 ? 2 : 3;
             for (int r = 0; r < N; ++r)
-                for (int c = 0; c < N; ++c) t.AddA(i0 + N * r + c, t.A(o + N * c + r));
+                for (int c = 0; c < N; ++c) t.AddA(a0 + N * r + c, t.A(ao + N * c + r));
             break;
         }
-        case INVERSE_M2: inverse_adjoint<P, 2>(t, o, i0); break;
-        case INVERSE_M3: inverse_adjoint<P, 3>(t, o, i0); break;
+        case INVERSE_M2: inverse_adjoint<P, 2>(t, vo, ao, v0, a0); break;
+        case INVERSE_M3: inverse_adjoint<P, 3>(t, vo, ao, v0, a0); break;
         default: break;
     }
+    // this node's adjoint has been consumed: clear it for the slot's next
+    // holder and for the next tile
+    for (uint32_t i = 0; i < width; ++i) t.adj[(ao + i) * 32 + t.lane] = splat<P>(0.0f);
 }
 
 template <int P>
@@ -341,7 +347,7 @@ __global__ void __launch_bounds__(kGradThreads, 16) grad_kernel(const LaunchArgs
     if (item_id >= a.n_items) return;
     const uint32_t cw = align4g(a.smem_code_words), cf = align4g(a.smem_const_floats);
     const uint32_t gp = min(kGradParams, a.smem_const_floats);
-    const uint32_t region = cw + cf + gp * 32u + 2u * a.smem_slots * 32u * P;
+    const uint32_t region = cw + cf + gp * 32u + (a.smem_slots + a.smem_adj_slots) * 32u * P;
     float *base = smem + (size_t)warp * region;
     uint32_t *scode = reinterpret_cast<uint32_t *>(base);
     float *sconst = base + cw;
@@ -357,17 +363,18 @@ __global__ void __launch_bounds__(kGradThreads, 16) grad_kernel(const LaunchArgs
     for (uint32_t i = lane; i < pd.n_consts; i += 32) sconst[i] = __ldg(a.consts + pd.const_off + i);
     const uint32_t np = min(pd.n_consts, kGradParams);
     for (uint32_t k = 0; k < np; ++k) gacc[k * 32 + lane] = 0.0f;
+    // adjoint slots start at zero; each node's reverse step clears its own
+    const uint32_t n_adj = pd.n_tape >> 16;
+    for (uint32_t s = 0; s < n_adj; ++s) adj[s * 32 + lane] = splat<P>(0.0f);
     __syncwarp();
-    const uint32_t result = scode[0];
-    const uint32_t *code = scode + 1;
-    const uint32_t n_nodes = (pd.uop_len - 1) / 3;
+    const uint32_t result = scode[0], result_adj = scode[1];
+    const uint32_t *code = scode + 2;
+    const uint32_t n_nodes = (pd.uop_len - 2) / 5;
     TapeCtx<P> t{val, adj, sconst, ds.x, ds.stride, 0, ds.n_eval, lane};
     Kahan sse;
     for (uint32_t tile = it.tile_begin; tile < it.tile_end; ++tile) {
         t.p0 = (uint64_t)tile * (32u * P) + (uint64_t)lane * P;
-        // forward sweep, then the adjoints cleared
-        for (uint32_t i = 0; i < n_nodes; ++i) tape_forward<P>(t, code[3 * i], code[3 * i + 1], code[3 * i + 2]);
-        for (uint32_t s = 0; s < pd.n_tape; ++s) adj[s * 32 + lane] = splat<P>(0.0f);
+        for (uint32_t i = 0; i < n_nodes; ++i) tape_forward<P>(t, code + 5 * i);
         const Vf<P> pred = result == 0xFFFFFFFFu ? splat<P>(0.0f) : t.V(result);
         const Vf<P> y = load_pts<P>(ds.y + t.p0);
         Vf<P> seed;
@@ -379,10 +386,9 @@ __global__ void __launch_bounds__(kGradThreads, 16) grad_kernel(const LaunchArgs
             seed.v[k] = valid ? 2.0f * d : 0.0f;  // d(diff^2)/d pred, as in evaluator.rs:207
         }
         if (result == 0xFFFFFFFFu) continue;
-        t.AddA(result, seed);
+        t.AddA(result_adj, seed);
         // reverse sweep; constant loads add their adjoints to gacc
-        for (uint32_t i = n_nodes; i-- > 0;)
-            tape_reverse<P>(t, code[3 * i], code[3 * i + 1], code[3 * i + 2], gacc + lane);
+        for (uint32_t i = n_nodes; i-- > 0;) tape_reverse<P>(t, code + 5 * i, gacc + lane);
     }
     double *out = a.partials + (size_t)(pd.part_off + it.chunk) * (1 + kGradParams);
     const double s = warp_sum(sse.value());
@@ -427,9 +433,11 @@ cudaError_t launch_grad(const LaunchArgs &a, uint32_t wpb, size_t smem, cudaStre
     return a.progs_per_warp >= 2 ? launch_grad_p<2>(a, wpb, smem, st) : launch_grad_p<1>(a, wpb, smem, st);
 }
 
-size_t grad_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t tape_slots) {
+size_t grad_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t val_slots, uint32_t adj_slots,
+                          int P) {
     const uint32_t gp = const_floats < kGradParams ? const_floats : kGradParams;
-    return ((size_t)align4g(code_words) + align4g(const_floats) + gp * 32u + 2u * (size_t)tape_slots * 32u) * 4u;
+    return ((size_t)align4g(code_words) + align4g(const_floats) + gp * 32u +
+            ((size_t)val_slots + adj_slots) * 32u * (size_t)P) * 4u;
 }
 
 cudaError_t launch_finalize_grad(const ProgDesc *progs, const DatasetDesc *ds, const double *partials, uint32_t n,

@@ -145,7 +145,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         if (gradient) {
             // adjoint launches by tape size, so that a block's shared memory
             // follows its own programs' tapes: <= 32, 64, 128, 256, more slots
-            const uint32_t nt = enc[i].n_tape_slots;
+            const uint32_t nt = enc[i].n_tape_val + enc[i].n_tape_adj;
             path[i] = nt <= 32 ? -2 : nt <= 64 ? -3 : nt <= 128 ? -4 : nt <= 256 ? -5 : -6;
         }
         else if (kernel == RSR_KERNEL_PLAIN || enc[i].profile < 0) path[i] = -1;
@@ -185,7 +185,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         const uint64_t n_eval = P.datasets[d.dataset].n_eval;
         d.n_parts = (uint32_t)std::max<uint64_t>(1, (n_eval + kChunkPoints - 1) / kChunkPoints);
         d.part_off = part;
-        d.n_tape = E.n_tape_slots;
+        d.n_tape = E.n_tape_val | (E.n_tape_adj << 16);
         part += d.n_parts;
         P.code.insert(P.code.end(), code.begin(), code.end());
         P.consts.insert(P.consts.end(), E.consts.begin(), E.consts.end());
@@ -230,7 +230,8 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             for (uint32_t q = j; q < k; ++q) {
                 cw += P.progs[q].uop_len + 1;
                 cf += P.progs[q].n_consts;
-                sl = std::max(sl, g.kind == 2 ? P.progs[q].n_tape : P.progs[q].n_slots);
+                sl = std::max(sl, g.kind == 2 ? P.progs[q].n_tape & 0xFFFFu : P.progs[q].n_slots);
+                if (g.kind == 2) g.adj_slots = std::max(g.adj_slots, P.progs[q].n_tape >> 16);
                 len_sum += P.progs[q].uop_len;
                 if (g.kind == 1)
                     for (int t = 0; t < N_STACKS; ++t)
@@ -254,9 +255,8 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             const size_t budget = g.kind == 2 ? 27 * 1024 : 110 * 1024;
             int Pp = g.kind == 2 ? 2 : 4;
             while (Pp > 1) {
-                size_t per = g.kind == 2 ? grad_smem_per_warp(g.code_words, g.const_floats, g.slots)
+                size_t per = g.kind == 2 ? grad_smem_per_warp(g.code_words, g.const_floats, g.slots, g.adj_slots, Pp)
                                          : plain_smem_per_warp(g.code_words, g.const_floats, g.slots, Pp);
-                if (g.kind == 2) per += (size_t)g.slots * 32u * 4u * (Pp - 1) * 2u;
                 if (per <= budget) break;
                 Pp >>= 1;
             }
@@ -384,8 +384,8 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             g.warps_per_block = kRegThreads / 32;
             e = launch_reg(a, g.profile, g.P, g.grid, st);
         } else {
-            size_t per = grad_smem_per_warp(g.code_words, g.const_floats, g.slots);
-            per += (size_t)g.slots * 32u * 4u * (g.P - 1) * 2u;
+            const size_t per = grad_smem_per_warp(g.code_words, g.const_floats, g.slots, g.adj_slots, g.P);
+            a.smem_adj_slots = g.adj_slots;
             // one warp per block: blocks as small as a tape, so an SM packs as
             // many tapes as its shared memory holds
             const uint32_t wpb = 1;

@@ -123,7 +123,7 @@ struct ProgDesc {
     uint32_t dataset;     // index into the launch's dataset table
     uint32_t part_off;    // first partial-sum slot of this program
     uint32_t n_parts;     // partial-sum slots (chunks) of this program
-    uint32_t n_tape;      // adjoint kernel: scalar tape slots
+    uint32_t n_tape;      // adjoint kernel: value slots | adjoint slots << 16
 };
 enum : uint32_t { PF_RESULT_ZERO = 1u, PF_NEEDS_ZERO_INIT = 2u, PF_DIFFERENTIABLE = 4u };
 
