@@ -36,16 +36,14 @@ struct Acc {
 
 template <int P>
 struct AccIO {
-    const float *x;
-    uint64_t stride;
-    uint64_t p0;
+    const float *xl;        // this lane's first point of feature 0 in the current tile
+    uint32_t stride;        // floats between features
     const float *consts;
-    Vf<P> *stk[N_STACKS];  // per-type shared-memory stacks of this warp: [(slot*W + c)*32 + lane]
-    int lane;
-    __device__ __forceinline__ Vf<P> X(uint32_t f) const { return load_pts<P>(x + f * stride + p0); }
+    Vf<P> *stk[N_STACKS];   // per-type shared-memory stacks of this lane: [(slot*W + c)*32]
+    __device__ __forceinline__ Vf<P> X(uint32_t f) const { return load_pts<P>(xl + (size_t)f * stride); }
     __device__ __forceinline__ Vf<P> C(uint32_t i) const { return splat<P>(consts[i]); }
     template <int W>
-    __device__ __forceinline__ Vf<P> &S(int t, uint32_t slot, int c) const { return stk[t][(slot * W + c) * 32 + lane]; }
+    __device__ __forceinline__ Vf<P> &S(int t, uint32_t slot, int c) const { return stk[t][(slot * W + c) * 32]; }
 };
 
 template <int PROF, int P, int t>
@@ -299,8 +297,18 @@ constexpr uint32_t kMaxProgsPerWarp = 8;
 //
 // Shared memory: block header (code | constants | meta | cross-warp sums)
 // then one region per warp (spill stacks | Kahan state).
+// Blocks per SM each instance is compiled for (the register cap follows):
+// as many as its accumulators allow without spilling.
 template <int PROF, int P>
-__global__ void __launch_bounds__(kRegThreads) reg_eval_kernel(const LaunchArgs a) {
+constexpr int reg_min_blocks() {
+    if constexpr (PROF == P_ALL) return P >= 4 ? 1 : 2;
+    else if constexpr (PROF == P_FV3M3) return P >= 4 ? 2 : 3;
+    else if constexpr (PROF == P_F) return P >= 4 ? 3 : 4;
+    else return P >= 8 ? 2 : 3;
+}
+
+template <int PROF, int P>
+__global__ void __launch_bounds__(kRegThreads, reg_min_blocks<PROF, P>()) reg_eval_kernel(const LaunchArgs a) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nw = blockDim.x >> 5;
@@ -313,8 +321,7 @@ __global__ void __launch_bounds__(kRegThreads) reg_eval_kernel(const LaunchArgs 
 
     AccIO<P> io;
 #pragma unroll
-    for (int t = 0; t < N_STACKS; ++t) io.stk[t] = reinterpret_cast<Vf<P> *>(wbase + a.stack_off[t]);
-    io.lane = lane;
+    for (int t = 0; t < N_STACKS; ++t) io.stk[t] = reinterpret_cast<Vf<P> *>(wbase + a.stack_off[t]) + lane;
 
     for (;;) {
         if (threadIdx.x == 0) meta[24] = atomicAdd(a.item_counter, 1u);
@@ -346,29 +353,38 @@ __global__ void __launch_bounds__(kRegThreads) reg_eval_kernel(const LaunchArgs 
         }
         __syncthreads();
         const DatasetDesc ds = a.datasets[a.progs[it.prog_begin].dataset];
-        io.x = ds.x;
-        io.stride = ds.stride;
+        io.stride = (uint32_t)ds.stride;
         Acc<PROF, P> acc;
         for (uint32_t tile = it.tile_begin + warp; tile < it.tile_end; tile += nw) {
-            io.p0 = (uint64_t)tile * (32u * P) + (uint64_t)lane * P;
-            const Vf<P> y = load_pts<P>(ds.y + io.p0);
+            const uint64_t p0 = (uint64_t)tile * (32u * P) + (uint64_t)lane * P;
+            io.xl = ds.x + p0;
+            const Vf<P> y = load_pts<P>(ds.y + p0);
+            const bool full = p0 + P <= ds.n_eval;
             for (uint32_t g = 0; g < G; ++g) {
                 if (a.active && !a.active[it.prog_begin + g]) continue;
                 io.consts = sconst + meta[3 * g + 2];
                 run_program<PROF, P>(acc, io, scode + meta[3 * g], meta[3 * g + 1]);
                 const Vf<P> pred = acc.F[0];
                 if (a.mode == MODE_POINTS) {
-                    store_pts<P>(a.points_out + (uint64_t)(it.prog_begin + g) * a.points_stride + io.p0, pred, io.p0,
+                    store_pts<P>(a.points_out + (uint64_t)(it.prog_begin + g) * a.points_stride + p0, pred, p0,
                                  ds.n_eval);
                 } else {
                     Kahan k;
                     k.s = sacc[(g * 2) * 32 + lane];
                     k.c = sacc[(g * 2 + 1) * 32 + lane];
+                    if (full) {
 #pragma unroll
-                    for (int q = 0; q < P; ++q) {
-                        if (io.p0 + q < ds.n_eval) {
+                        for (int q = 0; q < P; ++q) {
                             const float d = pred.v[q] - y.v[q];
                             k.add(d * d);
+                        }
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < P; ++q) {
+                            if (p0 + q < ds.n_eval) {
+                                const float d = pred.v[q] - y.v[q];
+                                k.add(d * d);
+                            }
                         }
                     }
                     sacc[(g * 2) * 32 + lane] = k.s;
@@ -399,7 +415,7 @@ __global__ void __launch_bounds__(kRegThreads) reg_eval_kernel(const LaunchArgs 
 // Shared-memory layout (floats).  Block header: code | constants | meta (32
 // words) | cross-warp sums (kRegThreads/32 x 8 doubles).  Per warp: stacks
 // (per type) | Kahan state.
-void reg_layout(uint32_t code_words, uint32_t const_floats, const uint32_t *stack_depth, int P,
+void reg_layout(uint32_t code_words, uint32_t const_floats, const uint32_t *stack_depth, int P, int G,
                 uint32_t *stack_off, uint32_t *acc_off, uint32_t *region_floats, uint32_t *block_hdr_floats) {
     *block_hdr_floats = align4r(code_words) + align4r(const_floats) + 32u + 2u * (kRegThreads / 32) * kMaxProgsPerWarp;
     uint32_t off = 0;
@@ -408,13 +424,13 @@ void reg_layout(uint32_t code_words, uint32_t const_floats, const uint32_t *stac
         off += stack_depth[t] * (uint32_t)kStackWidth[t] * 32u * (uint32_t)P;
     }
     *acc_off = off;
-    off += 2u * 32u * kMaxProgsPerWarp;
+    off += 2u * 32u * (uint32_t)G;  // Kahan state of the item's programs
     *region_floats = align4r(off);
 }
 
-size_t reg_smem_bytes(uint32_t code_words, uint32_t const_floats, const uint32_t *stack_depth, int P) {
+size_t reg_smem_bytes(uint32_t code_words, uint32_t const_floats, const uint32_t *stack_depth, int P, int G) {
     uint32_t so[N_STACKS], ao, rf, hf;
-    reg_layout(code_words, const_floats, stack_depth, P, so, &ao, &rf, &hf);
+    reg_layout(code_words, const_floats, stack_depth, P, G, so, &ao, &rf, &hf);
     return ((size_t)hf + (size_t)rf * (kRegThreads / 32)) * 4u;
 }
 

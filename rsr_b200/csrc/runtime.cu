@@ -79,7 +79,7 @@ static int log2_bucket(uint64_t n) {
 static TuneChoice default_choice(int profile) {
     switch (profile) {
         case P_F: return {8, 4};
-        case P_FV3: return {4, 4};
+        case P_FV3: return {8, 4};
         default: return {4, 4};
     }
 }
@@ -155,7 +155,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             uint32_t depth[N_STACKS];
             for (int t = 0; t < N_STACKS; ++t) depth[t] = (uint32_t)enc[i].depth_fast[t];
             const uint32_t cw = (uint32_t)enc[i].reg_code.size() + 1, cf = (uint32_t)enc[i].consts.size();
-            path[i] = reg_smem_bytes(cw, cf, depth, 2) <= kRegSmemBudget / 2 ? enc[i].profile : -1;
+            path[i] = reg_smem_bytes(cw, cf, depth, 2, 1) <= kRegSmemBudget / 2 ? enc[i].profile : -1;
         }
     }
     // group programs by (path, dataset), each group sorted by descending code length
@@ -246,7 +246,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         // register kernel: the tuned points per thread, halved while a block
         // would not fit
         if (g.kind == 1)
-            while (g.P > 2 && reg_smem_bytes(g.code_words, g.const_floats, g.stack_depth, g.P) > kRegSmemBudget)
+            while (g.P > 2 && reg_smem_bytes(g.code_words, g.const_floats, g.stack_depth, g.P, g.G) > kRegSmemBudget)
                 g.P >>= 1;
         // points per thread of slot-file kernels: largest that fits the smem budget
         if (g.kind != 1) {
@@ -374,7 +374,7 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             g.warps_per_block = wpb;
             e = launch_plain(a, g.P, wpb, per * wpb, st);
         } else if (g.kind == 1) {
-            reg_layout(g.code_words, g.const_floats, g.stack_depth, g.P, a.stack_off, &a.acc_off, &a.region_floats,
+            reg_layout(g.code_words, g.const_floats, g.stack_depth, g.P, g.G, a.stack_off, &a.acc_off, &a.region_floats,
                        &a.block_hdr_floats);
             const size_t smem = ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (kRegThreads / 32)) * 4u;
             int bps = std::max(1, reg_max_blocks_per_sm(g.profile, g.P, smem));
