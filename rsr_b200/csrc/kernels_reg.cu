@@ -259,28 +259,44 @@ __device__ __forceinline__ void acc_op(Acc<PROF, P> &a, const AccIO<P> &io, uint
 #define RSR_C4(K) RSR_C(K) RSR_C(K + 1) RSR_C(K + 2) RSR_C(K + 3)
 #define RSR_C9(K) RSR_C4(K) RSR_C4(K + 4) RSR_C(K + 8)
 #define RSR_C27(K) RSR_C9(K) RSR_C9(K + 9) RSR_C9(K + 18)
+#define RSR_BLOCK_F RSR_C27(K_F)     // 0..26
+#define RSR_BLOCK_V2 RSR_C27(K_V2)   // 32..58
+#define RSR_BLOCK_V3 RSR_C27(K_V3) RSR_C4(K_V3 + 27) RSR_C(K_V3 + 31) RSR_C(K_V3 + 32) RSR_C(K_V3 + 33)  // 64..97
+#define RSR_BLOCK_M2 RSR_C27(K_M2)   // 104..130
+#define RSR_BLOCK_M3 RSR_C27(K_M3)   // 136..162
 
 // Runs one program (accumulator form) on this lane's P points; the result
 // is left in A_F.
 template <int PROF, int P>
 __device__ __forceinline__ void run_program(Acc<PROF, P> &a, const AccIO<P> &io, const uint32_t *code,
                                             uint32_t len) {
+    // Each profile's switch lists only its own types' kinds, so the branch
+    // tree the compiler builds for it is as shallow as the profile allows.
     uint32_t w = code[0];
     for (uint32_t pc = 0; pc < len; ++pc) {
         const uint32_t wn = code[pc + 1];
         const uint32_t arg = w >> 8;
-        switch (w & 0xFFu) {
-            RSR_C27(K_F)                     // F block: 0..26
-            RSR_C27(K_V2)                    // V2 block: 32..58
-            RSR_C27(K_V3) RSR_C4(K_V3 + 27) RSR_C(K_V3 + 31) RSR_C(K_V3 + 32) RSR_C(K_V3 + 33)  // 64..97
-            RSR_C27(K_M2)                    // 104..130
-            RSR_C27(K_M3)                    // 136..162
-            default: break;
+        const uint32_t kind = w & 0xFFu;
+        if constexpr (PROF == P_F) {
+            switch (kind) { RSR_BLOCK_F default: break; }
+        } else if constexpr (PROF == P_FV3) {
+            switch (kind) { RSR_BLOCK_F RSR_BLOCK_V3 default: break; }
+        } else if constexpr (PROF == P_FV2M2) {
+            switch (kind) { RSR_BLOCK_F RSR_BLOCK_V2 RSR_BLOCK_M2 default: break; }
+        } else if constexpr (PROF == P_FV3M3) {
+            switch (kind) { RSR_BLOCK_F RSR_BLOCK_V3 RSR_BLOCK_M3 default: break; }
+        } else {
+            switch (kind) { RSR_BLOCK_F RSR_BLOCK_V2 RSR_BLOCK_V3 RSR_BLOCK_M2 RSR_BLOCK_M3 default: break; }
         }
         w = wn;
     }
 }
 
+#undef RSR_BLOCK_F
+#undef RSR_BLOCK_V2
+#undef RSR_BLOCK_V3
+#undef RSR_BLOCK_M2
+#undef RSR_BLOCK_M3
 #undef RSR_C27
 #undef RSR_C9
 #undef RSR_C4
