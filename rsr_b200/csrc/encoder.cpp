@@ -486,7 +486,7 @@ void set_err(std::string *err, const std::string &m) {
 
 int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uint32_t n_consts,
                    const float *params, uint32_t n_params, uint32_t num_features, EncodedProgram *out,
-                   std::string *err, bool fuse) {
+                   std::string *err, bool fuse, unsigned forms) {
     EncodedProgram &E = *out;
     E = EncodedProgram();
     if (len > 0 && !code) { set_err(err, "code is null"); return RSR_EINVAL; }
@@ -598,6 +598,7 @@ int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uin
     E.flops_per_point = flops + kMseEpilogueFlops;
 
     // ---- slot form: reference positions
+    if (forms & FORM_SLOT) {
     uint32_t sbase[N_STACKS], acc = 0;
     for (int t = 0; t < N_STACKS; ++t) {
         sbase[t] = acc;
@@ -618,12 +619,13 @@ int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uin
         E.slot_code.push_back(in[1] | (in[2] << 16));
         if (n.stale) E.needs_zero_init = true;
     }
+    }
 
     // ---- tape form: value and adjoint slots allocated by lifetime
-    emit_tape(nodes, live, root, &E);
+    if (forms & FORM_TAPE) emit_tape(nodes, live, root, &E);
 
     // ---- accumulator form
-    if (root >= 0 && !has_stale_live && n_params < (1u << kLdOffsetBits)) {
+    if ((forms & FORM_ACC) && root >= 0 && !has_stale_live && n_params < (1u << kLdOffsetBits)) {
         AccEmitter em(nodes);
         if (em.analyze(root)) {
             em.gen(root);

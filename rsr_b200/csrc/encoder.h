@@ -49,8 +49,10 @@ struct EncodedProgram {
 
 // Validates and encodes.  num_features == 0 skips feature-range checks.
 // Returns 0 or an rsr_status code, with a message in *err.
+// Device forms to emit (validation and the analysis run for every call).
+enum EncodeForms : unsigned { FORM_SLOT = 1u, FORM_TAPE = 2u, FORM_ACC = 4u, FORM_ALL = 7u };
 int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uint32_t n_consts,
                    const float *params, uint32_t n_params, uint32_t num_features, EncodedProgram *out,
-                   std::string *err, bool fuse_loads = true);
+                   std::string *err, bool fuse_loads = true, unsigned forms = FORM_ALL);
 
 }  // namespace rsr

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <thread>
 #include <numeric>
 
 #include "runtime.h"
@@ -126,19 +127,38 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         }
         prog_ds[i] = f->second;
     }
-    // encode
+    // encode: each program only in the form its kernel needs, in parallel
+    // for large populations
+    for (uint32_t i = 0; i < n; ++i)
+        if (pop.code_off[i + 1] < pop.code_off[i] || pop.kind_off[i + 1] < pop.kind_off[i] ||
+            pop.param_off[i + 1] < pop.param_off[i])
+            return fail(RSR_EINVAL, "population offsets decrease at " + std::to_string(i));
+    const bool fuse = (ctx->opts.flags & RSR_OPT_NO_LOAD_FUSION) == 0;
+    const unsigned forms = gradient ? FORM_TAPE : kernel == RSR_KERNEL_PLAIN ? FORM_SLOT : FORM_ACC;
     std::vector<EncodedProgram> enc(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        const uint64_t c0 = pop.code_off[i], c1 = pop.code_off[i + 1];
-        const uint64_t k0 = pop.kind_off[i], k1 = pop.kind_off[i + 1];
-        const uint64_t p0 = pop.param_off[i], p1 = pop.param_off[i + 1];
-        if (c1 < c0 || k1 < k0 || p1 < p0) return fail(RSR_EINVAL, "population offsets decrease at " + std::to_string(i));
-        std::string err;
-        int rc = encode_program(pop.code + c0, (uint32_t)(c1 - c0), pop.const_kinds + k0, (uint32_t)(k1 - k0),
-                                pop.params + p0, (uint32_t)(p1 - p0), P.datasets[prog_ds[i]].num_features, &enc[i],
-                                &err, (ctx->opts.flags & RSR_OPT_NO_LOAD_FUSION) == 0);
-        if (rc != RSR_OK) return fail(rc, "program " + std::to_string(i) + ": " + err);
+    std::vector<int> erc(n, RSR_OK);
+    std::vector<std::string> emsg(n);
+    auto encode_one = [&](uint32_t i, unsigned f) {
+        const uint64_t c0 = pop.code_off[i], k0 = pop.kind_off[i], p0 = pop.param_off[i];
+        erc[i] = encode_program(pop.code + c0, (uint32_t)(pop.code_off[i + 1] - c0), pop.const_kinds + k0,
+                                (uint32_t)(pop.kind_off[i + 1] - k0), pop.params + p0,
+                                (uint32_t)(pop.param_off[i + 1] - p0), P.datasets[prog_ds[i]].num_features, &enc[i],
+                                &emsg[i], fuse, f);
+    };
+    const uint32_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const uint32_t nthreads = n >= 512 ? hw : 1;
+    if (nthreads > 1) {
+        std::vector<std::thread> th;
+        for (uint32_t t = 0; t < nthreads; ++t)
+            th.emplace_back([&, t] {
+                for (uint32_t i = t; i < n; i += nthreads) encode_one(i, forms);
+            });
+        for (auto &x : th) x.join();
+    } else {
+        for (uint32_t i = 0; i < n; ++i) encode_one(i, forms);
     }
+    for (uint32_t i = 0; i < n; ++i)
+        if (erc[i] != RSR_OK) return fail(erc[i], "program " + std::to_string(i) + ": " + emsg[i]);
     // path per program: -2 adjoint, -1 plain, >= 0 register profile
     std::vector<int> path(n);
     for (uint32_t i = 0; i < n; ++i) {
@@ -156,6 +176,11 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             for (int t = 0; t < N_STACKS; ++t) depth[t] = (uint32_t)enc[i].depth_fast[t];
             const uint32_t cw = (uint32_t)enc[i].reg_code.size() + 1, cf = (uint32_t)enc[i].consts.size();
             path[i] = reg_smem_bytes(cw, cf, depth, 2, 1) <= kRegSmemBudget / 2 ? enc[i].profile : -1;
+        }
+        // programs the register kernel cannot take run on the slot-file kernel
+        if (path[i] == -1 && !(forms & FORM_SLOT)) {
+            encode_one(i, FORM_SLOT);
+            if (erc[i] != RSR_OK) return fail(erc[i], "program " + std::to_string(i) + ": " + emsg[i]);
         }
     }
     // group programs by (path, dataset), each group sorted by descending code length
