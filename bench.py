@@ -36,6 +36,10 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+# DRAM bytes (read + write) of one launch of the dominant kernel on this
+# workload, from one ncu capture (profiles/reg_eval_kernel_vector_1024x100k.md,
+# "Full bench size"): 5,313,024 read + 0 written.
+DOMINANT_KERNEL_DRAM_BYTES = 5_313_024
 METRIC = "program_points_per_sec"
 UNIT = "program*points/s"
 N_PROGRAMS = 4096
@@ -371,7 +375,9 @@ def run_engine(args):
             "plain": {"value": plain_value, "unit": UNIT, "speedup_of_batched": value / plain_value,
                       "ms_per_step": float(np.median(pms))},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": DOMINANT_KERNEL_DRAM_BYTES,
+                         "traffic_note": "ncu dram__bytes_read+write per launch of the dominant kernel; "
+                                         "algorithmic bytes ~4.4 MB (dataset once + programs)",
                          "kernel": f"reg_eval_kernel profile {groups[dom]['profile']} "
                                    f"P={groups[dom]['points_per_thread']} G={groups[dom]['programs_per_warp']}",
                          "peak_source": "measured unfused FP32 lane-op rate of this GPU (rsr_measure_fp32_peak)",
