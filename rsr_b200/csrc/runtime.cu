@@ -64,6 +64,7 @@ void HostBuf::release() {
     cap = 0;
 }
 
+static constexpr int kRegPathStride = 8;          // register path = profile + 8 * spill-depth class
 static constexpr uint64_t kChunkPoints = 4096;   // points per work-item chunk (all P)
 static constexpr uint64_t kStrideAlign = 1024;   // dataset column padding
 static constexpr int kGradSlotDoubles = 33;      // sse + 32 gradient sums
@@ -175,7 +176,17 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             uint32_t depth[N_STACKS];
             for (int t = 0; t < N_STACKS; ++t) depth[t] = (uint32_t)enc[i].depth_fast[t];
             const uint32_t cw = (uint32_t)enc[i].reg_code.size() + 1, cf = (uint32_t)enc[i].consts.size();
-            path[i] = reg_smem_bytes(cw, cf, depth, 2, 1) <= kRegSmemBudget / 2 ? enc[i].profile : -1;
+            if (reg_smem_bytes(cw, cf, depth, 2, 1) > kRegSmemBudget / 2) {
+                path[i] = -1;
+            } else {
+                // launches by spill depth, so that shallow programs (most of
+                // a random population) run with small spill stacks and leave
+                // the SM's unified L1 to their feature loads
+                uint32_t dmax = 0;
+                for (int t = 0; t < N_STACKS; ++t) dmax = std::max(dmax, depth[t]);
+                const int cls = dmax <= 1 ? 0 : dmax <= 2 ? 1 : 2;
+                path[i] = enc[i].profile + kRegPathStride * cls;
+            }
         }
         // programs the register kernel cannot take run on the slot-file kernel
         if (path[i] == -1 && !(forms & FORM_SLOT)) {
@@ -227,7 +238,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         while (end < n && path[order[end]] == pth) ++end;
         Group g;
         g.kind = pth <= -2 ? 2 : pth == -1 ? 0 : 1;
-        g.profile = pth >= 0 ? pth : -1;
+        g.profile = pth >= 0 ? pth % kRegPathStride : -1;
         g.item_begin = (uint32_t)P.items.size();
         if (g.kind == 1) {
             // P and G are per profile and dataset size; one launch uses one P,
@@ -339,8 +350,12 @@ int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st
         return cuda_fail(e, "outputs");
     if ((e = dev->counters.reserve(std::max<size_t>(plan.groups.size(), 1) * sizeof(uint32_t) + 64)) != cudaSuccess)
         return cuda_fail(e, "counters");
-    // the staging buffer may still feed an earlier copy on this stream
-    cudaStreamSynchronize(st);
+    // the staging buffer may still feed this plan's previous copy
+    if (dev->staged) {
+        if ((e = cudaEventSynchronize(dev->staged)) != cudaSuccess) return cuda_fail(e, "staging wait");
+    } else if ((e = cudaEventCreateWithFlags(&dev->staged, cudaEventDisableTiming)) != cudaSuccess) {
+        return cuda_fail(e, "cudaEventCreate");
+    }
     if ((e = dev->staging.reserve(total)) != cudaSuccess) return cuda_fail(e, "cudaHostAlloc");
     char *h = (char *)dev->staging.p;
     memcpy(h + o_progs, plan.progs.data(), n * sizeof(ProgDesc));
@@ -350,6 +365,7 @@ int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st
     memcpy(h + o_consts, plan.consts.data(), plan.consts.size() * sizeof(float));
     if ((e = cudaMemcpyAsync(dev->pool.p, h, total, cudaMemcpyHostToDevice, st)) != cudaSuccess)
         return cuda_fail(e, "plan upload");
+    if ((e = cudaEventRecord(dev->staged, st)) != cudaSuccess) return cuda_fail(e, "staging event");
     ctx->last_h2d = total;
     char *d = (char *)dev->pool.p;
     LaunchArgs &a = dev->base;
@@ -484,8 +500,70 @@ static rsr_population single_pop(const rsr_program *p, uint64_t offs[6]) {
     return pop;
 }
 
+// A large MSE (or MSE + gradient) call in chunks of programs: the host
+// encodes chunk k+1 while the device runs chunk k.  Chunks alternate between
+// two device plans; every launch and copy is on the context's stream, so a
+// plan's buffers are rewritten only after the device is done with them.
+static int run_chunked(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *dsp, uint64_t ds, int kernel,
+                       bool gradient, float *mse, float *grad, uint32_t n_chunks) {
+    const uint32_t n = pop.n_programs, stride = gradient ? 33u : 1u;
+    cudaError_t e;
+    if ((e = ctx->results.reserve((size_t)n * stride * sizeof(float))) != cudaSuccess)
+        return cuda_fail(e, "cudaHostAlloc");
+    float *res = (float *)ctx->results.p;
+    std::vector<Plan> plans(n_chunks);
+    std::vector<uint32_t> start(n_chunks + 1);
+    for (uint32_t k = 0; k <= n_chunks; ++k) start[k] = (uint32_t)((uint64_t)n * k / n_chunks);
+    uint64_t h2d = 0;
+    for (uint32_t k = 0; k < n_chunks; ++k) {
+        const uint32_t s0 = start[k], cnt = start[k + 1] - s0;
+        rsr_population sub = pop;
+        sub.n_programs = cnt;
+        sub.code_off = pop.code_off + s0;
+        sub.kind_off = pop.kind_off + s0;
+        sub.param_off = pop.param_off + s0;
+        int rc = build_plan(ctx, sub, dsp ? dsp + s0 : nullptr, ds, kernel, gradient, MODE_MSE, &plans[k]);
+        if (rc) {
+            // report the program by its index in the caller's population
+            std::string m = rsr_last_error();
+            const size_t at = m.rfind("program ", 0) == 0 ? 8 : std::string::npos;
+            if (at != std::string::npos) {
+                size_t end = m.find(':', at);
+                m = "program " + std::to_string(s0 + std::stoul(m.substr(at, end - at))) + m.substr(end);
+            }
+            cudaStreamSynchronize(ctx->stream);
+            return fail(rc, m);
+        }
+        DevicePlan *dev = &ctx->pipe[k & 1];
+        if ((rc = upload_plan(ctx, plans[k], dev, ctx->stream))) return rc;
+        h2d += ctx->last_h2d;
+        if ((rc = enqueue_plan(ctx, plans[k], dev, ctx->stream, nullptr))) return rc;
+        if ((e = cudaMemcpyAsync(res + (size_t)s0 * stride, dev->out.p, (size_t)cnt * stride * sizeof(float),
+                                 cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess)
+            return cuda_fail(e, "result download");
+    }
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(e, "evaluation");
+    for (uint32_t k = 0; k < n_chunks; ++k) {
+        const uint32_t s0 = start[k], cnt = start[k + 1] - s0;
+        const float *r = res + (size_t)s0 * stride;
+        for (uint32_t li = 0; li < cnt; ++li) {
+            const uint32_t i = s0 + plans[k].orig[li];
+            if (mse) mse[i] = r[li];
+            if (gradient && grad) memcpy(grad + (size_t)i * 32, r + cnt + (size_t)li * 32, 32 * sizeof(float));
+        }
+    }
+    ctx->last_h2d = h2d;
+    ctx->last_d2h = (uint64_t)n * stride * sizeof(float);
+    return RSR_OK;
+}
+
+static constexpr uint32_t kChunkPrograms = 1024;  // programs per chunk of a chunked call
+
 static int run_oneshot(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *dsp, uint64_t ds, int kernel,
                        bool gradient, int mode, float *mse, float *grad, float *points) {
+    if (mode == MODE_MSE && pop.n_programs >= 2 * kChunkPrograms)
+        return run_chunked(ctx, pop, dsp, ds, kernel, gradient, mse, grad,
+                           std::min<uint32_t>(8, pop.n_programs / kChunkPrograms));
     Plan plan;
     int rc = build_plan(ctx, pop, dsp, ds, kernel, gradient, mode, &plan);
     if (rc) return rc;
@@ -558,6 +636,10 @@ int rsr_ctx_destroy(rsr_ctx *ctx) {
     ctx->scratch.out.release();
     ctx->scratch.counters.release();
     ctx->scratch.staging.release();
+    for (DevicePlan &d : ctx->pipe) {
+        d.pool.release(); d.partials.release(); d.out.release(); d.counters.release(); d.staging.release();
+    }
+    ctx->results.release();
     if (ctx->l2buf) cudaFree(ctx->l2buf);
     for (auto &ev : ctx->ev) if (ev) cudaEventDestroy(ev);
     cudaStreamDestroy(ctx->stream);
@@ -958,17 +1040,29 @@ int rsr_autotune(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const 
                 }
             }
             if (rc) break;
+            // a profile may run as several launches (spill-depth classes):
+            // its candidate time is their sum
+            std::map<int, std::pair<float, uint64_t>> per;  // profile -> (ms, largest dataset)
             for (size_t g = 0; g < plan.groups.size(); ++g) {
                 const Group &gr = plan.groups[g];
                 if (gr.kind != 1 || !gr.n_items) continue;
                 uint64_t max_eval = 0;
                 for (uint32_t i = gr.item_begin; i < gr.item_begin + gr.n_items; ++i)
                     max_eval = std::max(max_eval, plan.datasets[plan.progs[plan.items[i].prog_begin].dataset].n_eval);
-                Best &b = best[gr.profile];
-                if (gmin[g] < b.ms) { b.ms = gmin[g]; b.c = TuneChoice{gr.P, gr.G}; b.bucket = log2_bucket(max_eval); }
-                rep += std::string(first ? "" : ", ") + "{\"profile\": " + std::to_string(gr.profile) +
-                       ", \"P\": " + std::to_string(gr.P) + ", \"G\": " + std::to_string(gr.G) +
-                       ", \"ms\": " + std::to_string(gmin[g]) + "}";
+                auto &pp = per[gr.profile];
+                pp.first += gmin[g];
+                pp.second = std::max(pp.second, max_eval);
+            }
+            for (auto &kv : per) {
+                Best &b = best[kv.first];
+                if (kv.second.first < b.ms) {
+                    b.ms = kv.second.first;
+                    b.c = TuneChoice{P, G};
+                    b.bucket = log2_bucket(kv.second.second);
+                }
+                rep += std::string(first ? "" : ", ") + "{\"profile\": " + std::to_string(kv.first) +
+                       ", \"P\": " + std::to_string(P) + ", \"G\": " + std::to_string(G) +
+                       ", \"ms\": " + std::to_string(kv.second.first) + "}";
                 first = false;
             }
         }

@@ -107,8 +107,15 @@ struct DevicePlan {
     DevBuf counters;    // one item counter per group
     DevBuf status;
     HostBuf staging;    // pinned image of the pool, uploaded with one copy
+    cudaEvent_t staged = nullptr;  // recorded after the staging buffer's copy
     LaunchArgs base{};
     float *mse = nullptr, *grad = nullptr;
+    DevicePlan() = default;
+    DevicePlan(const DevicePlan &) = delete;
+    DevicePlan &operator=(const DevicePlan &) = delete;
+    ~DevicePlan() {
+        if (staged) cudaEventDestroy(staged);
+    }
 };
 
 }  // namespace rsr
@@ -125,6 +132,8 @@ struct rsr_ctx {
     std::map<std::pair<int, int>, rsr::TuneChoice> tune;  // (profile, log2 points) -> choice
     rsr::TuneChoice force;     // set while the autotuner measures a candidate
     rsr::DevicePlan scratch;   // for one-shot calls
+    rsr::DevicePlan pipe[2];   // one-shot calls split into chunks, alternating
+    rsr::HostBuf results;      // pinned results of a chunked one-shot call
     void *l2buf = nullptr;
     size_t l2bytes = 0;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
