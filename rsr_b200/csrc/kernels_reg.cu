@@ -460,9 +460,9 @@ static cudaError_t launch_reg_pp(const LaunchArgs &a, uint32_t grid, cudaStream_
     return cudaGetLastError();
 }
 
-// Instantiated points-per-thread values: {2, 4, 8} for the F and F+V3
-// profiles, {2, 4} for the others.
-int reg_max_p(int profile) { return profile == P_F || profile == P_FV3 ? 8 : 4; }
+// Instantiated points-per-thread values: {2, 4, 8} for the F, F+V3 and
+// F+V2+M2 profiles, {2, 4} for the others.
+int reg_max_p(int profile) { return profile == P_F || profile == P_FV3 || profile == P_FV2M2 ? 8 : 4; }
 
 cudaError_t launch_reg(const LaunchArgs &a, int profile, int P, uint32_t grid, cudaStream_t st) {
     switch (profile) {
@@ -470,7 +470,8 @@ cudaError_t launch_reg(const LaunchArgs &a, int profile, int P, uint32_t grid, c
                                                                             : launch_reg_pp<P_F, 2>(a, grid, st);
         case P_FV3: return P >= 8 ? launch_reg_pp<P_FV3, 8>(a, grid, st) : P >= 4 ? launch_reg_pp<P_FV3, 4>(a, grid, st)
                                                                                 : launch_reg_pp<P_FV3, 2>(a, grid, st);
-        case P_FV2M2: return P >= 4 ? launch_reg_pp<P_FV2M2, 4>(a, grid, st) : launch_reg_pp<P_FV2M2, 2>(a, grid, st);
+        case P_FV2M2: return P >= 8 ? launch_reg_pp<P_FV2M2, 8>(a, grid, st) : P >= 4 ? launch_reg_pp<P_FV2M2, 4>(a, grid, st)
+                                                                                : launch_reg_pp<P_FV2M2, 2>(a, grid, st);
         case P_FV3M3: return P >= 4 ? launch_reg_pp<P_FV3M3, 4>(a, grid, st) : launch_reg_pp<P_FV3M3, 2>(a, grid, st);
         default: return P >= 4 ? launch_reg_pp<P_ALL, 4>(a, grid, st) : launch_reg_pp<P_ALL, 2>(a, grid, st);
     }
@@ -491,7 +492,7 @@ int reg_max_blocks_per_sm(int profile, int P, size_t smem) {
     switch (profile) {
         case P_F: return P >= 8 ? occ<P_F, 8>(smem) : P >= 4 ? occ<P_F, 4>(smem) : occ<P_F, 2>(smem);
         case P_FV3: return P >= 8 ? occ<P_FV3, 8>(smem) : P >= 4 ? occ<P_FV3, 4>(smem) : occ<P_FV3, 2>(smem);
-        case P_FV2M2: return P >= 4 ? occ<P_FV2M2, 4>(smem) : occ<P_FV2M2, 2>(smem);
+        case P_FV2M2: return P >= 8 ? occ<P_FV2M2, 8>(smem) : P >= 4 ? occ<P_FV2M2, 4>(smem) : occ<P_FV2M2, 2>(smem);
         case P_FV3M3: return P >= 4 ? occ<P_FV3M3, 4>(smem) : occ<P_FV3M3, 2>(smem);
         default: return P >= 4 ? occ<P_ALL, 4>(smem) : occ<P_ALL, 2>(smem);
     }
