@@ -315,12 +315,15 @@ constexpr uint32_t kMaxProgsPerWarp = 8;
 // then one region per warp (spill stacks | Kahan state).
 // Blocks per SM each instance is compiled for (the register cap follows):
 // as many as its accumulators allow without spilling.
+// At four points per lane a fourth block (64 registers, a few bytes of
+// spill) pays for the F and F+V3 profiles (vector workload: 4.75 ms against
+// 5.14 ms at three blocks); F+V2+M2 spills more there and keeps three.
 template <int PROF, int P>
 constexpr int reg_min_blocks() {
     if constexpr (PROF == P_ALL) return P >= 4 ? 1 : 2;
     else if constexpr (PROF == P_FV3M3) return P >= 4 ? 2 : 3;
-    else if constexpr (PROF == P_F) return P >= 4 ? 3 : 4;
-    else return P >= 8 ? 2 : 3;
+    else if constexpr (PROF == P_FV2M2) return P >= 8 ? 2 : P >= 4 ? 3 : 4;
+    else return P >= 8 ? 2 : 4;
 }
 
 template <int PROF, int P>

@@ -81,7 +81,7 @@ static int log2_bucket(uint64_t n) {
 static TuneChoice default_choice(int profile) {
     switch (profile) {
         case P_F: return {8, 4};
-        case P_FV3: return {8, 4};
+        case P_FV3: return {4, 2};
         default: return {4, 4};
     }
 }
