@@ -430,7 +430,8 @@ static cudaError_t launch_grad_p(const LaunchArgs &a, uint32_t wpb, size_t smem,
 }
 
 cudaError_t launch_grad(const LaunchArgs &a, uint32_t wpb, size_t smem, cudaStream_t st) {
-    return a.progs_per_warp >= 2 ? launch_grad_p<2>(a, wpb, smem, st) : launch_grad_p<1>(a, wpb, smem, st);
+    return a.progs_per_warp >= 4 ? launch_grad_p<4>(a, wpb, smem, st)
+         : a.progs_per_warp >= 2 ? launch_grad_p<2>(a, wpb, smem, st) : launch_grad_p<1>(a, wpb, smem, st);
 }
 
 size_t grad_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t val_slots, uint32_t adj_slots,

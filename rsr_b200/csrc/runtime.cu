@@ -289,7 +289,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             // adjoint: two points per lane while eight warps' tapes still fit
             // an SM; the tape's shared memory bounds the adjoint's occupancy
             const size_t budget = g.kind == 2 ? 27 * 1024 : 110 * 1024;
-            int Pp = g.kind == 2 ? 2 : 4;
+            int Pp = 4;
             while (Pp > 1) {
                 size_t per = g.kind == 2 ? grad_smem_per_warp(g.code_words, g.const_floats, g.slots, g.adj_slots, Pp)
                                          : plain_smem_per_warp(g.code_words, g.const_floats, g.slots, Pp);
