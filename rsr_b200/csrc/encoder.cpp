@@ -114,9 +114,10 @@ struct SlotPool {
 // its definition to its last forward read, or to the reverse step of the
 // last node whose reverse rule reads it; an adjoint slot lives from the
 // reverse step of its latest consumer (its first contribution) to its own
-// reverse step, after which the kernel zeroes it.  Feature loads keep no
-// adjoint: their contributions go to a sink run of 9 slots at 0 that is
-// never read.  Words: header (result value slot, result adjoint slot), then
+// reverse step, after which the kernel zeroes it.  Feature loads have no
+// tape entry: their value slot is kTapeFeature | feature offset, read from
+// the dataset where it is used, and their adjoint contributions go to a sink
+// run of 9 slots at 0 that is never read.  Words: header (result value slot, result adjoint slot), then
 // 5 per node: op | aux << 8 | out_width << 28, vo | ao << 16, and
 // vi | ai << 16 for inputs 0..2.
 void emit_tape(const std::vector<Node> &nodes, const std::vector<char> &live, int root, EncodedProgram *E) {
@@ -154,11 +155,16 @@ void emit_tape(const std::vector<Node> &nodes, const std::vector<char> &live, in
     SlotPool vals, adjs;
     adjs.take(9, -1, 1 << 30);  // the sink
     std::vector<uint32_t> vs(N, 0), as(N, 0);
-    for (int t = 0; t < N; ++t) vs[t] = vals.take(kStackWidth[nodes[idx[t]].out], t, std::max(vend[t], t));
+    auto is_feature = [&](int t) {
+        const Node &n = nodes[idx[t]];
+        return !n.stale && is_load(n.opcode) && !is_const_load(n.opcode) && n.arg < kTapeFeature;
+    };
+    for (int t = 0; t < N; ++t)
+        vs[t] = is_feature(t) ? (kTapeFeature | nodes[idx[t]].arg)  // read from the dataset where used
+                              : vals.take(kStackWidth[nodes[idx[t]].out], t, std::max(vend[t], t));
     for (int t = N - 1; t >= 0; --t) {  // adjoint intervals start in reverse node order
         const Node &n = nodes[idx[t]];
-        const bool feature = !n.stale && is_load(n.opcode) && !is_const_load(n.opcode);
-        if (feature || astart[t] > rev - t) continue;  // sink
+        if (is_feature(t) || astart[t] > rev - t) continue;  // sink
         as[t] = adjs.take(kStackWidth[n.out], astart[t], rev - t);
     }
     E->n_tape_val = (uint32_t)vals.busy_until.size();
@@ -168,6 +174,7 @@ void emit_tape(const std::vector<Node> &nodes, const std::vector<char> &live, in
     E->tape_code.push_back(rt >= 0 ? as[rt] : 0u);
     for (int t = 0; t < N; ++t) {
         const Node &n = nodes[idx[t]];
+        if (is_feature(t)) continue;  // no tape entry: consumers read the dataset
         uint32_t w0, in[3] = {0, 0, 0};
         if (n.stale) {
             // copy of the value left in that slot, or zero; aux = has_alias | width << 1

@@ -34,7 +34,10 @@ struct TapeCtx {
     uint64_t stride, p0;
     uint64_t n_eval;   // points counted (num_batches * 8)
     int lane;
-    __device__ __forceinline__ Vf<P> V(uint32_t s) const { return val[s * 32 + lane]; }
+    // a value slot with kTapeFeature set is a feature column, read in place
+    __device__ __forceinline__ Vf<P> V(uint32_t s) const {
+        return (s & kTapeFeature) ? X(s & (kTapeFeature - 1u)) : val[s * 32 + lane];
+    }
     __device__ __forceinline__ void SV(uint32_t s, const Vf<P> &v) const { val[s * 32 + lane] = v; }
     __device__ __forceinline__ Vf<P> A(uint32_t s) const { return adj[s * 32 + lane]; }
     __device__ __forceinline__ void AddA(uint32_t s, const Vf<P> &v) const {

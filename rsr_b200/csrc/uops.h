@@ -106,6 +106,10 @@ RSR_HD static inline constexpr uint32_t push_load_arg(uint32_t slot, uint32_t ty
 }
 
 // Register-kernel profiles: the accumulator types a kernel instance holds.
+// Tape value slot that stands for a feature column (adjoint kernel): the
+// low 15 bits are the feature offset.
+constexpr uint32_t kTapeFeature = 0x8000u;
+
 enum Profile : int { P_F = 0, P_FV3 = 1, P_FV2M2 = 2, P_FV3M3 = 3, P_ALL = 4, N_PROFILES = 5 };
 static constexpr uint32_t kProfileTypes[N_PROFILES] = {
     1u << SF, (1u << SF) | (1u << SV3), (1u << SF) | (1u << SV2) | (1u << SM2), (1u << SF) | (1u << SV3) | (1u << SM3),
