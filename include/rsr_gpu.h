@@ -256,6 +256,18 @@ RSR_API int rsr_wait(rsr_server *srv, uint64_t ticket, uint64_t timeout_us, rsr_
 RSR_API int rsr_cancel(rsr_server *srv, uint64_t ticket);
 RSR_API int rsr_server_stats(rsr_server *srv, rsr_serving_stats *stats, int reset);
 
+/* run_nelder_mead (src/engine/optimize/nelder_mead.rs:9-165) for a whole
+ * population: a simplex over each program's Float constants (at most 32),
+ * objective mse + 0.01 * sum |c|, up to max_iterations iterations; each
+ * phase (reflection; expansion or contraction; each shrink vertex) is one
+ * launch for all programs in it.  params_out gets the best vertex's
+ * constants (other parameters unchanged), mse_out its MSE.  Vertices of
+ * equal fitness keep their order (a stable sort; the reference's order for
+ * ties is unspecified). */
+RSR_API int rsr_fit_nelder_mead(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds,
+                                const rsr_dataset *ds_per_program, uint32_t max_iterations, float *params_out,
+                                float *mse_out, rsr_fit_stats *stats);
+
 /* -------------------------------------------------- prepared batches */
 /* A population encoded and uploaded once, then run many times with inputs
  * resident on the device (the timed unit of the benchmark).  run() enqueues

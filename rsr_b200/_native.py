@@ -116,6 +116,8 @@ _SIGS = {
                                       C.c_void_p]),
     "rsr_finalize_sums": (C.c_int, [C.c_uint32, C.c_int, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     "rsr_compute_mse_noalloc": (C.c_int, [C.c_void_p, C.POINTER(Program), C.c_uint64, C.POINTER(C.c_float)]),
+    "rsr_fit_nelder_mead": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_uint32,
+                                      C.c_void_p, C.c_void_p, C.POINTER(FitStats)]),
     "rsr_fit_lbfgs": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p,
                                 C.c_void_p, C.POINTER(FitStats)]),
     "rsr_batch_prepare": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_int, C.c_int,

@@ -174,6 +174,21 @@ class Engine:
                                               "gradient_evaluations": st.gradient_evaluations,
                                               "mse_evaluations": st.mse_evaluations}
 
+    def fit_nelder_mead(self, programs: PopulationLike, dataset=None, max_iterations: int = 50, datasets=None):
+        """run_nelder_mead (src/engine/optimize/nelder_mead.rs:9-165) for
+        every program at once.  Returns (fitted flat params, best mse, stats)."""
+        pk = _packed(programs)
+        s, keep = _as_population(pk)
+        h, dsp = self._handles(pk.n, dataset, datasets)
+        params = np.zeros(max(1, len(pk.params)), np.float32)
+        mse = np.zeros(pk.n, np.float32)
+        st = N.FitStats()
+        N.check(N.lib().rsr_fit_nelder_mead(self.ctx, C.byref(s), h, dsp.ctypes.data if dsp is not None else None,
+                                            max_iterations, params.ctypes.data, mse.ctypes.data, C.byref(st)))
+        return params[:len(pk.params)], mse, {"iterations": st.iterations,
+                                              "gradient_evaluations": st.gradient_evaluations,
+                                              "mse_evaluations": st.mse_evaluations}
+
     def eval_points_batch(self, programs: PopulationLike, dataset, kernel: int = N.KERNEL_AUTO) -> np.ndarray:
         pk = _packed(programs)
         s, keep = _as_population(pk)

@@ -128,3 +128,42 @@ def test_fit_agrees_with_oracle(engine):
     # branch; most programs still land on the same fitness
     assert ok >= 0.8 * total, (ok, total)
     assert st["iterations"] <= 15
+
+
+# ---------------------------------------------------------------- Nelder-Mead
+from oracle import nelder_mead as ONM  # noqa: E402
+
+
+def test_oracle_nelder_mead_reduces_quadratic_error():
+    prog, ds = _quadratic()
+    from oracle import binding as B
+    m0 = B.mse_ref32(prog, ds)
+    x, m, st = ONM.run_nelder_mead(prog, ds, 200)
+    # the L1 term (0.01 * sum |c|) pulls the optimum slightly off (2.5, 1.2)
+    assert m < 1e-3 * m0 and abs(x[0] - 2.5) < 0.05 and abs(x[1] - 1.2) < 0.1
+    assert st["iterations"] > 10
+
+
+@pytest.mark.gpu
+def test_nelder_mead_matches_sequential_restatement():
+    """Same evaluations in -> same simplex steps out: the batched fit against
+    run_nelder_mead driven by single-program calls of the same engine."""
+    from rsr_b200.evaluator import Engine
+    pop, ds = _fit_population()
+    with Engine(points_per_thread=4, programs_per_warp=4) as eng:
+        d = eng.upload(ds)
+        params, mse, _ = eng.fit_nelder_mead(pop, d, 12)
+        pk = I.pack(pop)
+        for i, p in enumerate(pop):
+            q = Program(list(p.code), [Scalar(c.kind, c.values) for c in p.constants])
+            x, m, _ = ONM.run_nelder_mead(q, ds, 12, mse_fn=lambda pr: eng.compute_mse(pr, d))
+            got = params[pk.param_off[i]:pk.param_off[i + 1]]
+            np.testing.assert_array_equal(got, x, err_msg=f"program {i}")
+            assert np.float32(mse[i]) == np.float32(m)
+
+
+@pytest.mark.gpu
+def test_nelder_mead_quadratic(engine):
+    prog, ds = _quadratic()
+    x, m, st = engine.fit_nelder_mead([prog], ds, 200)
+    assert abs(x[0] - 2.5) < 0.05 and abs(x[1] - 1.2) < 0.1 and m[0] < 1e-2
