@@ -349,6 +349,16 @@ __global__ void __launch_bounds__(kRegThreads, reg_min_blocks<PROF, P>()) reg_ev
         if (item_id >= a.n_items) break;
         const WorkItem it = a.items[item_id];
         const uint32_t G = it.n_progs;
+        if (a.active) {
+            // an item whose programs have all finished (fits) is skipped whole;
+            // the flags are the same for every thread of the block
+            bool any = false;
+            for (uint32_t g = 0; g < G; ++g) any |= a.active[it.prog_begin + g] != 0;
+            if (!any) {
+                __syncthreads();  // meta[24] is rewritten by the next item fetch
+                continue;
+            }
+        }
         if (threadIdx.x == 0) {
             uint32_t coff = 0, koff = 0;
             for (uint32_t g = 0; g < G; ++g) {
