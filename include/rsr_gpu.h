@@ -117,6 +117,21 @@ RSR_API int rsr_dataset_upload(rsr_ctx *ctx, const float *feature_flat, const fl
  * to a multiple of 8 with zeros as Dataset::new does (dataset.rs:96-154). */
 RSR_API int rsr_dataset_upload_columns(rsr_ctx *ctx, const float *features, const float *targets, uint32_t num_features,
                                uint64_t n, rsr_dataset *out);
+/* Dataset::new (src/engine/data/dataset.rs:37-169) on the device: raw rows
+ * x_rows[num_samples][num_features] and y[num_samples]; with normalize != 0
+ * every column is z-scored with the reference's sequential f32 sums (means,
+ * deviations and normalised values bit-identical to the reference's).
+ * stats_out (optional, 2*(num_features+1) floats): the feature means then the
+ * target mean, the feature deviations then the target deviation. */
+RSR_API int rsr_dataset_upload_rows(rsr_ctx *ctx, const float *x_rows, const float *y, uint32_t num_features,
+                                    uint64_t num_samples, int normalize, float *stats_out, rsr_dataset *out);
+/* Dataset::subset (dataset.rs:360-447) of a resident dataset, as a new
+ * resident dataset: min(target_samples, num_samples) evenly spaced points
+ * (the engine's mini-batch, src/engine/search/engine.rs:49). */
+RSR_API int rsr_dataset_subset(rsr_ctx *ctx, rsr_dataset src, uint64_t target_samples, rsr_dataset *out);
+/* A resident dataset back in the AoSoA layout: feature_flat
+ * [num_batches*num_features*8], target_batches [num_batches*8]. */
+RSR_API int rsr_dataset_download(rsr_ctx *ctx, rsr_dataset ds, float *feature_flat, float *target_batches);
 RSR_API int rsr_dataset_release(rsr_ctx *ctx, rsr_dataset ds);
 RSR_API int rsr_dataset_info(rsr_ctx *ctx, rsr_dataset ds, uint32_t *num_features, uint64_t *num_batches,
                      uint64_t *num_samples);

@@ -116,6 +116,10 @@ _SIGS = {
                                       C.c_void_p]),
     "rsr_finalize_sums": (C.c_int, [C.c_uint32, C.c_int, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     "rsr_compute_mse_noalloc": (C.c_int, [C.c_void_p, C.POINTER(Program), C.c_uint64, C.POINTER(C.c_float)]),
+    "rsr_dataset_upload_rows": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_int,
+                                          C.c_void_p, C.POINTER(C.c_uint64)]),
+    "rsr_dataset_subset": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "rsr_dataset_download": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     "rsr_fit_nelder_mead": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_uint32,
                                       C.c_void_p, C.c_void_p, C.POINTER(FitStats)]),
     "rsr_fit_lbfgs": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p,

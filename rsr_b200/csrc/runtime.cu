@@ -575,6 +575,38 @@ static int run_oneshot(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *
     return fetch_results(ctx, plan, ctx->scratch, ctx->stream, mse, grad, points);
 }
 
+int alloc_dataset(rsr_ctx *ctx, uint32_t nf, uint64_t nbatch, uint64_t nsamples, std::unique_ptr<DatasetRec> *out) {
+    if (nbatch == 0 || nsamples == 0 || nsamples > nbatch * 8 || nsamples <= (nbatch - 1) * 8)
+        return fail(RSR_EINVAL, "num_samples must satisfy 8*(num_batches-1) < num_samples <= 8*num_batches");
+    if (nf > 255) return fail(RSR_EINVAL, "at most 255 features (LoadVar operands are u8)");
+    const uint64_t n_eval = nbatch * 8;
+    const uint64_t stride = round_up(n_eval, kStrideAlign);
+    const size_t xbytes = (size_t)stride * std::max<uint32_t>(nf, 1) * sizeof(float);
+    const size_t ybytes = (size_t)stride * sizeof(float);
+    if (ctx->mem_in_use + xbytes + ybytes > ctx->opts.mem_budget_bytes)
+        return fail(RSR_ENOMEM, "dataset exceeds the context's memory budget");
+    auto rec = std::make_unique<DatasetRec>();
+    cudaError_t e;
+    if ((e = cudaMalloc(&rec->x, xbytes)) != cudaSuccess) return cuda_fail(e, "dataset features");
+    if ((e = cudaMalloc(&rec->y, ybytes)) != cudaSuccess) { cudaFree(rec->x); return cuda_fail(e, "dataset targets"); }
+    cudaMemsetAsync(rec->x, 0, xbytes, ctx->stream);
+    cudaMemsetAsync(rec->y, 0, ybytes, ctx->stream);
+    rec->num_features = nf;
+    rec->num_batches = nbatch;
+    rec->num_samples = nsamples;
+    rec->stride = stride;
+    rec->bytes = xbytes + ybytes;
+    *out = std::move(rec);
+    return RSR_OK;
+}
+
+rsr_dataset register_dataset(rsr_ctx *ctx, std::unique_ptr<DatasetRec> rec) {
+    ctx->mem_in_use += rec->bytes;
+    const uint64_t h = ctx->next_handle++;
+    ctx->datasets.emplace(h, std::move(rec));
+    return h;
+}
+
 }  // namespace rsr
 
 using namespace rsr;
@@ -650,27 +682,12 @@ int rsr_ctx_destroy(rsr_ctx *ctx) {
 static int upload_soa(rsr_ctx *ctx, const float *ff, const float *tb, bool aosoa, uint32_t nf, uint64_t nbatch,
                       uint64_t nsamples, rsr_dataset *out) {
     if (!out) return fail(RSR_EINVAL, "out is null");
-    if (nbatch == 0 || nsamples == 0 || nsamples > nbatch * 8 || nsamples <= (nbatch - 1) * 8)
-        return fail(RSR_EINVAL, "num_samples must satisfy 8*(num_batches-1) < num_samples <= 8*num_batches");
-    if (nf > 255) return fail(RSR_EINVAL, "at most 255 features (LoadVar operands are u8)");
     if ((nf && !ff) || !tb) return fail(RSR_EINVAL, "feature or target pointer is null");
-    const uint64_t n_eval = nbatch * 8;
-    const uint64_t stride = round_up(n_eval, kStrideAlign);
-    const size_t xbytes = (size_t)stride * std::max<uint32_t>(nf, 1) * sizeof(float);
-    const size_t ybytes = (size_t)stride * sizeof(float);
-    if (ctx->mem_in_use + xbytes + ybytes > ctx->opts.mem_budget_bytes)
-        return fail(RSR_ENOMEM, "dataset exceeds the context's memory budget");
-    auto rec = std::make_unique<DatasetRec>();
+    std::unique_ptr<DatasetRec> rec;
+    int rc = alloc_dataset(ctx, nf, nbatch, nsamples, &rec);
+    if (rc) return rc;
+    const uint64_t stride = rec->stride;
     cudaError_t e;
-    if ((e = cudaMalloc(&rec->x, xbytes)) != cudaSuccess) return cuda_fail(e, "dataset features");
-    if ((e = cudaMalloc(&rec->y, ybytes)) != cudaSuccess) { cudaFree(rec->x); return cuda_fail(e, "dataset targets"); }
-    cudaMemsetAsync(rec->x, 0, xbytes, ctx->stream);
-    cudaMemsetAsync(rec->y, 0, ybytes, ctx->stream);
-    rec->num_features = nf;
-    rec->num_batches = nbatch;
-    rec->num_samples = nsamples;
-    rec->stride = stride;
-    rec->bytes = xbytes + ybytes;
     if (aosoa) {
         // raw AoSoA upload, transposed on the device
         const size_t rawx = (size_t)nbatch * nf * 8 * sizeof(float), rawy = (size_t)nbatch * 8 * sizeof(float);
@@ -699,10 +716,7 @@ static int upload_soa(rsr_ctx *ctx, const float *ff, const float *tb, bool aosoa
         cudaFree(rec->x); cudaFree(rec->y);
         return cuda_fail(e, "dataset upload");
     }
-    ctx->mem_in_use += rec->bytes;
-    uint64_t h = ctx->next_handle++;
-    ctx->datasets.emplace(h, std::move(rec));
-    *out = h;
+    *out = register_dataset(ctx, std::move(rec));
     return RSR_OK;
 }
 

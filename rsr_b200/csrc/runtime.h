@@ -158,6 +158,10 @@ namespace rsr {
 int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_prog, uint64_t ds_all, int kernel,
                bool gradient, int mode, Plan *plan);
 int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st);
+// A zero-filled resident dataset of the given shape (columns padded to the
+// stride), and its registration in the context's table (caller holds ctx->mu).
+int alloc_dataset(rsr_ctx *ctx, uint32_t nf, uint64_t nbatch, uint64_t nsamples, std::unique_ptr<DatasetRec> *out);
+rsr_dataset register_dataset(rsr_ctx *ctx, std::unique_ptr<DatasetRec> rec);
 // Batched L-BFGS (lbfgs.cu) on stream st.  plan_mu, when given, is held while
 // plans are built (they read the context's dataset and tuning tables);
 // cancel, when set, stops the fit between iterations with RSR_ECANCELED.

@@ -109,6 +109,38 @@ class Engine:
         self._cache[key] = (ds, d)
         return d
 
+    def upload_rows(self, x_rows, y, normalize: bool = False):
+        """Dataset::new on the device (src/engine/data/dataset.rs:37-169):
+        raw rows in, a resident dataset out, z-scored on the device when
+        asked.  Returns (DeviceDataset, {"means", "stds"}) -- the last entry
+        of each is the target's."""
+        x = np.ascontiguousarray(x_rows, np.float32)
+        yy = np.ascontiguousarray(y, np.float32)
+        n = len(yy)
+        nf = x.shape[1] if x.ndim == 2 else 0
+        stats = np.zeros(2 * (nf + 1), np.float32)
+        h = C.c_uint64()
+        N.check(N.lib().rsr_dataset_upload_rows(self.ctx, x.ctypes.data if nf else None, yy.ctypes.data, nf, n,
+                                                int(normalize), stats.ctypes.data, C.byref(h)))
+        d = DeviceDataset(self, h.value, nf, (n + 7) // 8, n)
+        return d, {"means": stats[:nf + 1], "stds": stats[nf + 1:]}
+
+    def subset(self, dataset, target_samples: int) -> DeviceDataset:
+        """Dataset::subset (dataset.rs:360-447) of a resident dataset, resident."""
+        src = self._ds(dataset)
+        h = C.c_uint64()
+        N.check(N.lib().rsr_dataset_subset(self.ctx, src.handle, target_samples, C.byref(h)))
+        m = min(target_samples, src.num_samples)
+        return DeviceDataset(self, h.value, src.num_features, (m + 7) // 8, m)
+
+    def download(self, dataset):
+        """A resident dataset in the AoSoA layout: (feature_flat, target_batches)."""
+        d = self._ds(dataset)
+        ff = np.zeros(max(1, d.num_batches * d.num_features * 8), np.float32)
+        tb = np.zeros(d.num_batches * 8, np.float32)
+        N.check(N.lib().rsr_dataset_download(self.ctx, d.handle, ff.ctypes.data, tb.ctypes.data))
+        return ff[:d.num_batches * d.num_features * 8], tb
+
     def _ds(self, ds) -> DeviceDataset:
         return ds if isinstance(ds, DeviceDataset) else self.upload(ds)
 
