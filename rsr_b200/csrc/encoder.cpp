@@ -603,6 +603,13 @@ int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uin
         if (nodes[i].stale) has_stale_live = true;
     }
     E.flops_per_point = flops + kMseEpilogueFlops;
+    {
+        uint32_t types = 1u << SF;
+        for (size_t i = 0; i < nodes.size(); ++i)
+            if (live[i]) types |= 1u << nodes[i].out;
+        for (int p = 0; p < N_PROFILES; ++p)
+            if ((types & ~kProfileTypes[p]) == 0) { E.tape_profile = p; break; }
+    }
 
     // ---- slot form: reference positions
     if (forms & FORM_SLOT) {

@@ -45,6 +45,7 @@ struct EncodedProgram {
     // adjoint (slot form with one slot range per value, never reused)
     std::vector<uint32_t> tape_code;      // 2 header words + 5 words per live node
     uint32_t n_tape_val = 0, n_tape_adj = 0;  // scalar value / adjoint slots
+    int tape_profile = P_ALL;             // smallest kernel profile covering the live values' types
 };
 
 // Validates and encodes.  num_features == 0 skips feature-range checks.

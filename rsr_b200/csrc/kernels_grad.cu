@@ -25,6 +25,16 @@ namespace rsr {
 __host__ __device__ __forceinline__ uint32_t align4g(uint32_t v) { return (v + 3u) & ~3u; }
 constexpr uint32_t kGradParams = 32;
 
+// Per-profile kernels: an opcode whose value type the profile lacks gets a
+// case label outside the opcode range, so its handler is dropped and the
+// kernel's code (and its instruction-cache footprint) shrinks.
+#define RSR_PROFILE_TYPES(PROF)                                                    \
+    constexpr uint32_t kTypes = kProfileTypes[PROF];                               \
+    constexpr bool HV2 = (kTypes >> SV2) & 1u, HV3 = (kTypes >> SV3) & 1u;         \
+    constexpr bool HM2 = (kTypes >> SM2) & 1u, HM3 = (kTypes >> SM3) & 1u;         \
+    (void)HV2; (void)HV3; (void)HM2; (void)HM3;
+#define RSR_GATE(OP, HAS) ((HAS) ? (int)(OP) : 0x1000 + (int)(OP))
+
 template <int P>
 struct TapeCtx {
     Vf<P> *val;   // [slot][lane]
@@ -62,8 +72,9 @@ __device__ __forceinline__ void fwd_scale(const TapeCtx<P> &t, uint32_t o, uint3
 }
 
 // Forward value of one tape instruction (same semantics as the slot kernel).
-template <int P>
+template <int PROF, int P>
 __device__ __forceinline__ void tape_forward(const TapeCtx<P> &t, const uint32_t *w) {
+    RSR_PROFILE_TYPES(PROF)
     const uint32_t op = w[0] & 0xFFu, aux = (w[0] >> 8) & 0xFFFFFu;
     const uint32_t o = w[1] & 0xFFFFu, i0 = w[2] & 0xFFFFu, i1 = w[3] & 0xFFFFu, i2 = w[4] & 0xFFFFu;
     Vf<P> A[9], B[9], R[9];
@@ -76,15 +87,15 @@ __device__ __forceinline__ void tape_forward(const TapeCtx<P> &t, const uint32_t
             break;
         }
         case LOAD_VAR_F: t.SV(o, t.X(aux)); break;
-        case LOAD_VAR_V2: for (int i = 0; i < 2; ++i) t.SV(o + i, t.X(aux + i)); break;
-        case LOAD_VAR_V3: for (int i = 0; i < 3; ++i) t.SV(o + i, t.X(aux + i)); break;
-        case LOAD_VAR_M2: for (int i = 0; i < 4; ++i) t.SV(o + i, t.X(aux + i)); break;
-        case LOAD_VAR_M3: for (int i = 0; i < 9; ++i) t.SV(o + i, t.X(aux + i)); break;
+        case RSR_GATE(LOAD_VAR_V2, HV2): for (int i = 0; i < 2; ++i) t.SV(o + i, t.X(aux + i)); break;
+        case RSR_GATE(LOAD_VAR_V3, HV3): for (int i = 0; i < 3; ++i) t.SV(o + i, t.X(aux + i)); break;
+        case RSR_GATE(LOAD_VAR_M2, HM2): for (int i = 0; i < 4; ++i) t.SV(o + i, t.X(aux + i)); break;
+        case RSR_GATE(LOAD_VAR_M3, HM3): for (int i = 0; i < 9; ++i) t.SV(o + i, t.X(aux + i)); break;
         case LOAD_CONST_F: t.SV(o, splat<P>(t.consts[aux])); break;
-        case LOAD_CONST_V2: for (int i = 0; i < 2; ++i) t.SV(o + i, splat<P>(t.consts[aux + i])); break;
-        case LOAD_CONST_V3: for (int i = 0; i < 3; ++i) t.SV(o + i, splat<P>(t.consts[aux + i])); break;
-        case LOAD_CONST_M2: for (int i = 0; i < 4; ++i) t.SV(o + i, splat<P>(t.consts[aux + i])); break;
-        case LOAD_CONST_M3: for (int i = 0; i < 9; ++i) t.SV(o + i, splat<P>(t.consts[aux + i])); break;
+        case RSR_GATE(LOAD_CONST_V2, HV2): for (int i = 0; i < 2; ++i) t.SV(o + i, splat<P>(t.consts[aux + i])); break;
+        case RSR_GATE(LOAD_CONST_V3, HV3): for (int i = 0; i < 3; ++i) t.SV(o + i, splat<P>(t.consts[aux + i])); break;
+        case RSR_GATE(LOAD_CONST_M2, HM2): for (int i = 0; i < 4; ++i) t.SV(o + i, splat<P>(t.consts[aux + i])); break;
+        case RSR_GATE(LOAD_CONST_M3, HM3): for (int i = 0; i < 9; ++i) t.SV(o + i, splat<P>(t.consts[aux + i])); break;
         case ADD_F: t.SV(o, t.V(i0) + t.V(i1)); break;
         case SUB_F: t.SV(o, t.V(i0) - t.V(i1)); break;
         case MUL_F: t.SV(o, t.V(i0) * t.V(i1)); break;
@@ -97,40 +108,40 @@ __device__ __forceinline__ void tape_forward(const TapeCtx<P> &t, const uint32_t
         case LN_F: t.SV(o, vlog(t.V(i0))); break;
         case MAKE_VEC2: A[0] = t.V(i0); A[1] = t.V(i1); Sn(o, A, 2); break;
         case MAKE_VEC3: A[0] = t.V(i0); A[1] = t.V(i1); A[2] = t.V(i2); Sn(o, A, 3); break;
-        case GET_X_V2: case GET_X_V3: t.SV(o, t.V(i0)); break;
-        case GET_Y_V2: case GET_Y_V3: t.SV(o, t.V(i0 + 1)); break;
-        case GET_Z_V3: t.SV(o, t.V(i0 + 2)); break;
-        case ADD_V2: fwd_addsub<P, 2, false>(t, o, i0, i1); break;
-        case ADD_V3: fwd_addsub<P, 3, false>(t, o, i0, i1); break;
-        case ADD_M2: fwd_addsub<P, 4, false>(t, o, i0, i1); break;
-        case ADD_M3: fwd_addsub<P, 9, false>(t, o, i0, i1); break;
-        case SUB_V2: fwd_addsub<P, 2, true>(t, o, i0, i1); break;
-        case SUB_V3: fwd_addsub<P, 3, true>(t, o, i0, i1); break;
-        case SUB_M2: fwd_addsub<P, 4, true>(t, o, i0, i1); break;
-        case SUB_M3: fwd_addsub<P, 9, true>(t, o, i0, i1); break;
-        case SCALE_V2: fwd_scale<P, 2>(t, o, i0, i1); break;
-        case SCALE_V3: fwd_scale<P, 3>(t, o, i0, i1); break;
-        case SCALE_M2: fwd_scale<P, 4>(t, o, i0, i1); break;
-        case SCALE_M3: fwd_scale<P, 9>(t, o, i0, i1); break;
-        case DOT_V2: Ln(A, i0, 2); Ln(B, i1, 2); t.SV(o, dot2(A, B)); break;
-        case DOT_V3: Ln(A, i0, 3); Ln(B, i1, 3); t.SV(o, dot3(A, B)); break;
-        case NORM_V2: Ln(A, i0, 2); t.SV(o, norm2(A)); break;
-        case NORM_V3: Ln(A, i0, 3); t.SV(o, norm3(A)); break;
-        case CROSS_V3: Ln(A, i0, 3); Ln(B, i1, 3); cross3(A, B, R); Sn(o, R, 3); break;
-        case MAKE_MAT2: Ln(A, i0, 2); Ln(A + 2, i1, 2); Sn(o, A, 4); break;
-        case MUL_M2: Ln(A, i0, 4); Ln(B, i1, 4); mul_m2(A, B, R); Sn(o, R, 4); break;
-        case MUL_M2V2: Ln(A, i0, 4); Ln(B, i1, 2); mul_m2v2(A, B, R); Sn(o, R, 2); break;
-        case DET_M2: Ln(A, i0, 4); t.SV(o, det_m2(A)); break;
-        case TRACE_M2: Ln(A, i0, 4); t.SV(o, trace_m2(A)); break;
-        case TRANSPOSE_M2: Ln(A, i0, 4); transpose_m2(A, R); Sn(o, R, 4); break;
-        case INVERSE_M2: Ln(A, i0, 4); inverse_m2(A, R); Sn(o, R, 4); break;
-        case MAKE_MAT3: Ln(A, i0, 3); Ln(A + 3, i1, 3); Ln(A + 6, i2, 3); Sn(o, A, 9); break;
-        case MUL_M3: Ln(A, i0, 9); Ln(B, i1, 9); mul_m3(A, B, R); Sn(o, R, 9); break;
-        case MUL_M3V3: Ln(A, i0, 9); Ln(B, i1, 3); mul_m3v3(A, B, R); Sn(o, R, 3); break;
-        case DET_M3: Ln(A, i0, 9); t.SV(o, det_m3(A)); break;
-        case TRACE_M3: Ln(A, i0, 9); t.SV(o, trace_m3(A)); break;
-        case TRANSPOSE_M3: Ln(A, i0, 9); transpose_m3(A, R); Sn(o, R, 9); break;
-        case INVERSE_M3: Ln(A, i0, 9); inverse_m3(A, R); Sn(o, R, 9); break;
+        case RSR_GATE(GET_X_V2, HV2): case RSR_GATE(GET_X_V3, HV3): t.SV(o, t.V(i0)); break;
+        case RSR_GATE(GET_Y_V2, HV2): case RSR_GATE(GET_Y_V3, HV3): t.SV(o, t.V(i0 + 1)); break;
+        case RSR_GATE(GET_Z_V3, HV3): t.SV(o, t.V(i0 + 2)); break;
+        case RSR_GATE(ADD_V2, HV2): fwd_addsub<P, 2, false>(t, o, i0, i1); break;
+        case RSR_GATE(ADD_V3, HV3): fwd_addsub<P, 3, false>(t, o, i0, i1); break;
+        case RSR_GATE(ADD_M2, HM2): fwd_addsub<P, 4, false>(t, o, i0, i1); break;
+        case RSR_GATE(ADD_M3, HM3): fwd_addsub<P, 9, false>(t, o, i0, i1); break;
+        case RSR_GATE(SUB_V2, HV2): fwd_addsub<P, 2, true>(t, o, i0, i1); break;
+        case RSR_GATE(SUB_V3, HV3): fwd_addsub<P, 3, true>(t, o, i0, i1); break;
+        case RSR_GATE(SUB_M2, HM2): fwd_addsub<P, 4, true>(t, o, i0, i1); break;
+        case RSR_GATE(SUB_M3, HM3): fwd_addsub<P, 9, true>(t, o, i0, i1); break;
+        case RSR_GATE(SCALE_V2, HV2): fwd_scale<P, 2>(t, o, i0, i1); break;
+        case RSR_GATE(SCALE_V3, HV3): fwd_scale<P, 3>(t, o, i0, i1); break;
+        case RSR_GATE(SCALE_M2, HM2): fwd_scale<P, 4>(t, o, i0, i1); break;
+        case RSR_GATE(SCALE_M3, HM3): fwd_scale<P, 9>(t, o, i0, i1); break;
+        case RSR_GATE(DOT_V2, HV2): Ln(A, i0, 2); Ln(B, i1, 2); t.SV(o, dot2(A, B)); break;
+        case RSR_GATE(DOT_V3, HV3): Ln(A, i0, 3); Ln(B, i1, 3); t.SV(o, dot3(A, B)); break;
+        case RSR_GATE(NORM_V2, HV2): Ln(A, i0, 2); t.SV(o, norm2(A)); break;
+        case RSR_GATE(NORM_V3, HV3): Ln(A, i0, 3); t.SV(o, norm3(A)); break;
+        case RSR_GATE(CROSS_V3, HV3): Ln(A, i0, 3); Ln(B, i1, 3); cross3(A, B, R); Sn(o, R, 3); break;
+        case RSR_GATE(MAKE_MAT2, HM2): Ln(A, i0, 2); Ln(A + 2, i1, 2); Sn(o, A, 4); break;
+        case RSR_GATE(MUL_M2, HM2): Ln(A, i0, 4); Ln(B, i1, 4); mul_m2(A, B, R); Sn(o, R, 4); break;
+        case RSR_GATE(MUL_M2V2, HM2): Ln(A, i0, 4); Ln(B, i1, 2); mul_m2v2(A, B, R); Sn(o, R, 2); break;
+        case RSR_GATE(DET_M2, HM2): Ln(A, i0, 4); t.SV(o, det_m2(A)); break;
+        case RSR_GATE(TRACE_M2, HM2): Ln(A, i0, 4); t.SV(o, trace_m2(A)); break;
+        case RSR_GATE(TRANSPOSE_M2, HM2): Ln(A, i0, 4); transpose_m2(A, R); Sn(o, R, 4); break;
+        case RSR_GATE(INVERSE_M2, HM2): Ln(A, i0, 4); inverse_m2(A, R); Sn(o, R, 4); break;
+        case RSR_GATE(MAKE_MAT3, HM3): Ln(A, i0, 3); Ln(A + 3, i1, 3); Ln(A + 6, i2, 3); Sn(o, A, 9); break;
+        case RSR_GATE(MUL_M3, HM3): Ln(A, i0, 9); Ln(B, i1, 9); mul_m3(A, B, R); Sn(o, R, 9); break;
+        case RSR_GATE(MUL_M3V3, HM3): Ln(A, i0, 9); Ln(B, i1, 3); mul_m3v3(A, B, R); Sn(o, R, 3); break;
+        case RSR_GATE(DET_M3, HM3): Ln(A, i0, 9); t.SV(o, det_m3(A)); break;
+        case RSR_GATE(TRACE_M3, HM3): Ln(A, i0, 9); t.SV(o, trace_m3(A)); break;
+        case RSR_GATE(TRANSPOSE_M3, HM3): Ln(A, i0, 9); transpose_m3(A, R); Sn(o, R, 9); break;
+        case RSR_GATE(INVERSE_M3, HM3): Ln(A, i0, 9); inverse_m3(A, R); Sn(o, R, 9); break;
         default: break;
     }
 }
@@ -203,8 +214,9 @@ __device__ __forceinline__ void rev_mulmv(const TapeCtx<P> &t, uint32_t vo, uint
 
 // Reverse sweep of one tape instruction.  gacc: this lane's f32 gradient
 // contributions of the tile (summed over its P points).
-template <int P>
+template <int PROF, int P>
 __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t *w, float *gacc_lane) {
+    RSR_PROFILE_TYPES(PROF)
     const uint32_t op = w[0] & 0xFFu, aux = (w[0] >> 8) & 0xFFFFFu, width = w[0] >> 28;
     const uint32_t vo = w[1] & 0xFFFFu, ao = w[1] >> 16;
     const uint32_t v0 = w[2] & 0xFFFFu, a0 = w[2] >> 16, v1 = w[3] & 0xFFFFu, a1 = w[3] >> 16;
@@ -213,8 +225,8 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t
         case SLOT_NOP:
             if (aux & 1u) for (uint32_t i = 0; i < (aux >> 1); ++i) t.AddA(a0 + i, t.A(ao + i));
             break;
-        case LOAD_VAR_F: case LOAD_VAR_V2: case LOAD_VAR_V3: case LOAD_VAR_M2: case LOAD_VAR_M3: break;
-        case LOAD_CONST_F: case LOAD_CONST_V2: case LOAD_CONST_V3: case LOAD_CONST_M2: case LOAD_CONST_M3: {
+        case LOAD_VAR_F: case RSR_GATE(LOAD_VAR_V2, HV2): case RSR_GATE(LOAD_VAR_V3, HV3): case RSR_GATE(LOAD_VAR_M2, HM2): case RSR_GATE(LOAD_VAR_M3, HM3): break;
+        case LOAD_CONST_F: case RSR_GATE(LOAD_CONST_V2, HV2): case RSR_GATE(LOAD_CONST_V3, HV3): case RSR_GATE(LOAD_CONST_M2, HM2): case RSR_GATE(LOAD_CONST_M3, HM3): {
             const int w = op == LOAD_CONST_F ? 1 : op == LOAD_CONST_V2 ? 2 : op == LOAD_CONST_V3 ? 3
                         : op == LOAD_CONST_M2 ? 4 : 9;
             for (int i = 0; i < w; ++i) {
@@ -245,10 +257,10 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t
         case LN_F: t.AddA(a0, t.A(ao) / t.V(v0)); break;
         case MAKE_VEC2: t.AddA(a0, t.A(ao)); t.AddA(a1, t.A(ao + 1)); break;
         case MAKE_VEC3: t.AddA(a0, t.A(ao)); t.AddA(a1, t.A(ao + 1)); t.AddA(a2, t.A(ao + 2)); break;
-        case GET_X_V2: case GET_X_V3: t.AddA(a0, t.A(ao)); break;
-        case GET_Y_V2: case GET_Y_V3: t.AddA(a0 + 1, t.A(ao)); break;
-        case GET_Z_V3: t.AddA(a0 + 2, t.A(ao)); break;
-        case ADD_V2: case ADD_V3: case ADD_M2: case ADD_M3: case SUB_V2: case SUB_V3: case SUB_M2: case SUB_M3: {
+        case RSR_GATE(GET_X_V2, HV2): case RSR_GATE(GET_X_V3, HV3): t.AddA(a0, t.A(ao)); break;
+        case RSR_GATE(GET_Y_V2, HV2): case RSR_GATE(GET_Y_V3, HV3): t.AddA(a0 + 1, t.A(ao)); break;
+        case RSR_GATE(GET_Z_V3, HV3): t.AddA(a0 + 2, t.A(ao)); break;
+        case RSR_GATE(ADD_V2, HV2): case RSR_GATE(ADD_V3, HV3): case RSR_GATE(ADD_M2, HM2): case RSR_GATE(ADD_M3, HM3): case RSR_GATE(SUB_V2, HV2): case RSR_GATE(SUB_V3, HV3): case RSR_GATE(SUB_M2, HM2): case RSR_GATE(SUB_M3, HM3): {
             const bool sub = op == SUB_V2 || op == SUB_V3 || op == SUB_M2 || op == SUB_M3;
             const int w = (op == ADD_V2 || op == SUB_V2) ? 2 : (op == ADD_V3 || op == SUB_V3) ? 3
                         : (op == ADD_M2 || op == SUB_M2) ? 4 : 9;
@@ -259,7 +271,7 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t
             }
             break;
         }
-        case SCALE_V2: case SCALE_V3: case SCALE_M2: case SCALE_M3: {
+        case RSR_GATE(SCALE_V2, HV2): case RSR_GATE(SCALE_V3, HV3): case RSR_GATE(SCALE_M2, HM2): case RSR_GATE(SCALE_M3, HM3): {
             const int w = op == SCALE_V2 ? 2 : op == SCALE_V3 ? 3 : op == SCALE_M2 ? 4 : 9;
             const Vf<P> s = t.V(v0);
             Vf<P> ds = splat<P>(0.0f);
@@ -271,7 +283,7 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t
             t.AddA(a0, ds);
             break;
         }
-        case DOT_V2: case DOT_V3: {
+        case RSR_GATE(DOT_V2, HV2): case RSR_GATE(DOT_V3, HV3): {
             const int w = op == DOT_V2 ? 2 : 3;
             const Vf<P> g = t.A(ao);
             for (int i = 0; i < w; ++i) {
@@ -281,13 +293,13 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t
             }
             break;
         }
-        case NORM_V2: case NORM_V3: {
+        case RSR_GATE(NORM_V2, HV2): case RSR_GATE(NORM_V3, HV3): {
             const int w = op == NORM_V2 ? 2 : 3;
             const Vf<P> q = t.A(ao) / t.V(vo);
             for (int i = 0; i < w; ++i) t.AddA(a0 + i, q * t.V(v0 + i));
             break;
         }
-        case CROSS_V3: {  // o = a x b: da += b x g, db += g x a
+        case RSR_GATE(CROSS_V3, HV3): {  // o = a x b: da += b x g, db += g x a
             Vf<P> a[3], b[3], g[3], da[3], db[3];
             for (int i = 0; i < 3; ++i) { a[i] = t.V(v0 + i); b[i] = t.V(v1 + i); g[i] = t.A(ao + i); }
             cross3(b, g, da);
@@ -295,17 +307,17 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t
             for (int i = 0; i < 3; ++i) { t.AddA(a0 + i, da[i]); t.AddA(a1 + i, db[i]); }
             break;
         }
-        case MAKE_MAT2:
+        case RSR_GATE(MAKE_MAT2, HM2):
             t.AddA(a0, t.A(ao)); t.AddA(a0 + 1, t.A(ao + 1)); t.AddA(a1, t.A(ao + 2)); t.AddA(a1 + 1, t.A(ao + 3));
             break;
-        case MAKE_MAT3:
+        case RSR_GATE(MAKE_MAT3, HM3):
             for (int i = 0; i < 3; ++i) { t.AddA(a0 + i, t.A(ao + i)); t.AddA(a1 + i, t.A(ao + 3 + i)); t.AddA(a2 + i, t.A(ao + 6 + i)); }
             break;
-        case MUL_M2: rev_mulm<P, 2>(t, vo, ao, v0, a0, v1, a1); break;
-        case MUL_M3: rev_mulm<P, 3>(t, vo, ao, v0, a0, v1, a1); break;
-        case MUL_M2V2: rev_mulmv<P, 2>(t, vo, ao, v0, a0, v1, a1); break;
-        case MUL_M3V3: rev_mulmv<P, 3>(t, vo, ao, v0, a0, v1, a1); break;
-        case DET_M2: {
+        case RSR_GATE(MUL_M2, HM2): rev_mulm<P, 2>(t, vo, ao, v0, a0, v1, a1); break;
+        case RSR_GATE(MUL_M3, HM3): rev_mulm<P, 3>(t, vo, ao, v0, a0, v1, a1); break;
+        case RSR_GATE(MUL_M2V2, HM2): rev_mulmv<P, 2>(t, vo, ao, v0, a0, v1, a1); break;
+        case RSR_GATE(MUL_M3V3, HM3): rev_mulmv<P, 3>(t, vo, ao, v0, a0, v1, a1); break;
+        case RSR_GATE(DET_M2, HM2): {
             const Vf<P> g = t.A(ao);
             t.AddA(a0, g * t.V(v0 + 3));
             t.AddA(a0 + 3, g * t.V(v0));
@@ -313,7 +325,7 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t
             t.AddA(a0 + 2, -(g * t.V(v0 + 1)));
             break;
         }
-        case DET_M3: {  // d det / d m(r,c) = cofactor C(r,c)
+        case RSR_GATE(DET_M3, HM3): {  // d det / d m(r,c) = cofactor C(r,c)
             const Vf<P> g = t.A(ao);
             Vf<P> m[9];
             for (int i = 0; i < 9; ++i) m[i] = t.V(v0 + i);
@@ -325,16 +337,16 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t
                 }
             break;
         }
-        case TRACE_M2: { const Vf<P> g = t.A(ao); t.AddA(a0, g); t.AddA(a0 + 3, g); break; }
-        case TRACE_M3: { const Vf<P> g = t.A(ao); t.AddA(a0, g); t.AddA(a0 + 4, g); t.AddA(a0 + 8, g); break; }
-        case TRANSPOSE_M2: case TRANSPOSE_M3: {
+        case RSR_GATE(TRACE_M2, HM2): { const Vf<P> g = t.A(ao); t.AddA(a0, g); t.AddA(a0 + 3, g); break; }
+        case RSR_GATE(TRACE_M3, HM3): { const Vf<P> g = t.A(ao); t.AddA(a0, g); t.AddA(a0 + 4, g); t.AddA(a0 + 8, g); break; }
+        case RSR_GATE(TRANSPOSE_M2, HM2): case RSR_GATE(TRANSPOSE_M3, HM3): {
             const int N = op == TRANSPOSE_M2 ? 2 : 3;
             for (int r = 0; r < N; ++r)
                 for (int c = 0; c < N; ++c) t.AddA(a0 + N * r + c, t.A(ao + N * c + r));
             break;
         }
-        case INVERSE_M2: inverse_adjoint<P, 2>(t, vo, ao, v0, a0); break;
-        case INVERSE_M3: inverse_adjoint<P, 3>(t, vo, ao, v0, a0); break;
+        case RSR_GATE(INVERSE_M2, HM2): inverse_adjoint<P, 2>(t, vo, ao, v0, a0); break;
+        case RSR_GATE(INVERSE_M3, HM3): inverse_adjoint<P, 3>(t, vo, ao, v0, a0); break;
         default: break;
     }
     // this node's adjoint has been consumed: clear it for the slot's next
@@ -342,7 +354,7 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t
     for (uint32_t i = 0; i < width; ++i) t.adj[(ao + i) * 32 + t.lane] = splat<P>(0.0f);
 }
 
-template <int P>
+template <int PROF, int P>
 __global__ void __launch_bounds__(kGradThreads, 16) grad_kernel(const LaunchArgs a) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -377,7 +389,7 @@ __global__ void __launch_bounds__(kGradThreads, 16) grad_kernel(const LaunchArgs
     Kahan sse;
     for (uint32_t tile = it.tile_begin; tile < it.tile_end; ++tile) {
         t.p0 = (uint64_t)tile * (32u * P) + (uint64_t)lane * P;
-        for (uint32_t i = 0; i < n_nodes; ++i) tape_forward<P>(t, code + 5 * i);
+        for (uint32_t i = 0; i < n_nodes; ++i) tape_forward<PROF, P>(t, code + 5 * i);
         const Vf<P> pred = result == 0xFFFFFFFFu ? splat<P>(0.0f) : t.V(result);
         const Vf<P> y = load_pts<P>(ds.y + t.p0);
         Vf<P> seed;
@@ -391,7 +403,7 @@ __global__ void __launch_bounds__(kGradThreads, 16) grad_kernel(const LaunchArgs
         if (result == 0xFFFFFFFFu) continue;
         t.AddA(result_adj, seed);
         // reverse sweep; constant loads add their adjoints to gacc
-        for (uint32_t i = n_nodes; i-- > 0;) tape_reverse<P>(t, code + 5 * i, gacc + lane);
+        for (uint32_t i = n_nodes; i-- > 0;) tape_reverse<PROF, P>(t, code + 5 * i, gacc + lane);
     }
     double *out = a.partials + (size_t)(pd.part_off + it.chunk) * (1 + kGradParams);
     const double s = warp_sum(sse.value());
@@ -423,18 +435,29 @@ __global__ void finalize_grad_kernel(const ProgDesc *progs, const DatasetDesc *d
     for (uint32_t k = 0; k < kGradParams; ++k) grad_out[(size_t)p * kGradParams + k] = (bad || k >= np) ? 0.0f : (float)(g[k] / n);
 }
 
-template <int P>
+template <int PROF, int P>
 static cudaError_t launch_grad_p(const LaunchArgs &a, uint32_t wpb, size_t smem, cudaStream_t st) {
-    auto k = grad_kernel<P>;
+    auto k = grad_kernel<PROF, P>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin);
     if (e != cudaSuccess) return e;
     k<<<(a.n_items + wpb - 1) / wpb, wpb * 32, smem, st>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_grad(const LaunchArgs &a, uint32_t wpb, size_t smem, cudaStream_t st) {
-    return a.progs_per_warp >= 4 ? launch_grad_p<4>(a, wpb, smem, st)
-         : a.progs_per_warp >= 2 ? launch_grad_p<2>(a, wpb, smem, st) : launch_grad_p<1>(a, wpb, smem, st);
+template <int PROF>
+static cudaError_t launch_grad_prof(const LaunchArgs &a, uint32_t wpb, size_t smem, cudaStream_t st) {
+    return a.progs_per_warp >= 4 ? launch_grad_p<PROF, 4>(a, wpb, smem, st)
+         : a.progs_per_warp >= 2 ? launch_grad_p<PROF, 2>(a, wpb, smem, st) : launch_grad_p<PROF, 1>(a, wpb, smem, st);
+}
+
+cudaError_t launch_grad(const LaunchArgs &a, int profile, uint32_t wpb, size_t smem, cudaStream_t st) {
+    switch (profile) {
+        case P_F: return launch_grad_prof<P_F>(a, wpb, smem, st);
+        case P_FV3: return launch_grad_prof<P_FV3>(a, wpb, smem, st);
+        case P_FV2M2: return launch_grad_prof<P_FV2M2>(a, wpb, smem, st);
+        case P_FV3M3: return launch_grad_prof<P_FV3M3>(a, wpb, smem, st);
+        default: return launch_grad_prof<P_ALL>(a, wpb, smem, st);
+    }
 }
 
 size_t grad_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t val_slots, uint32_t adj_slots,

@@ -167,7 +167,9 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             // adjoint launches by tape size, so that a block's shared memory
             // follows its own programs' tapes: <= 32, 64, 128, 256, more slots
             const uint32_t nt = enc[i].n_tape_val + enc[i].n_tape_adj;
-            path[i] = nt <= 32 ? -2 : nt <= 64 ? -3 : nt <= 128 ? -4 : nt <= 256 ? -5 : -6;
+            const int bucket = nt <= 32 ? 0 : nt <= 64 ? 1 : nt <= 128 ? 2 : nt <= 256 ? 3 : 4;
+            // one launch per (tape-size bucket, kernel profile)
+            path[i] = -2 - (bucket * N_PROFILES + enc[i].tape_profile);
         }
         else if (kernel == RSR_KERNEL_PLAIN || enc[i].profile < 0) path[i] = -1;
         else {
@@ -238,7 +240,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         while (end < n && path[order[end]] == pth) ++end;
         Group g;
         g.kind = pth <= -2 ? 2 : pth == -1 ? 0 : 1;
-        g.profile = pth >= 0 ? pth % kRegPathStride : -1;
+        g.profile = pth >= 0 ? pth % kRegPathStride : pth <= -2 ? (-2 - pth) % N_PROFILES : -1;
         g.item_begin = (uint32_t)P.items.size();
         if (g.kind == 1) {
             // P and G are per profile and dataset size; one launch uses one P,
@@ -434,7 +436,7 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             g.grid = (g.n_items + wpb - 1) / wpb;
             g.smem = per * wpb;
             g.warps_per_block = wpb;
-            e = launch_grad(a, wpb, per * wpb, st);
+            e = launch_grad(a, g.profile, wpb, per * wpb, st);
         }
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
         if (group_events) cudaEventRecord(group_events[2 * gi + 1], st);
