@@ -59,6 +59,7 @@ int fit_population(rsr_ctx *ctx, const rsr_population *pop, const uint64_t *dsp,
                    uint32_t max_iterations, cudaStream_t stream, std::mutex *plan_mu,
                    const std::atomic<bool> *cancel, FitWorkspace *ws, float *params_out, float *mse_out,
                    rsr_fit_stats *stats) {
+    NvtxRange nvtx_range("rsr: L-BFGS fit");
     const uint32_t N = pop->n_programs;
     rsr_fit_stats local{};
     if (N == 0) {

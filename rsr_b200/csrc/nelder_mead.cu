@@ -69,6 +69,7 @@ void sort_simplex(NmState &s) {
 int fit_nelder_mead(rsr_ctx *ctx, const rsr_population *pop, const uint64_t *dsp, uint64_t ds,
                     uint32_t max_iterations, cudaStream_t stream, float *params_out, float *mse_out,
                     rsr_fit_stats *stats) {
+    NvtxRange nvtx_range("rsr: Nelder-Mead fit");
     const uint32_t N = pop->n_programs;
     rsr_fit_stats local{};
     if (N == 0) {

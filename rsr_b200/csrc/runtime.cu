@@ -105,6 +105,7 @@ static uint32_t align4h(uint32_t v) { return (v + 3u) & ~3u; }
 
 int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_prog, uint64_t ds_all, int kernel,
                bool gradient, int mode, Plan *plan) {
+    NvtxRange nvtx_range("rsr: encode + plan");
     Plan &P = *plan;
     P = Plan();
     P.gradient = gradient;
@@ -334,6 +335,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
 }
 
 int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st) {
+    NvtxRange nvtx_range("rsr: upload");
     const size_t n = plan.progs.size();
     auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
     const size_t o_progs = 0;
@@ -388,6 +390,7 @@ int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st
 
 int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st, cudaEvent_t ev_mid,
                  cudaEvent_t *group_events) {
+    NvtxRange nvtx_range("rsr: launch");
     const uint32_t n = (uint32_t)plan.progs.size();
     if (n == 0) {
         if (ev_mid) cudaEventRecord(ev_mid, st);
@@ -462,6 +465,7 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
 // Copy results back in caller order.
 static int fetch_results(rsr_ctx *ctx, const Plan &plan, DevicePlan &dev, cudaStream_t st, float *mse_out,
                          float *grad_out, float *points_out) {
+    NvtxRange nvtx_range("rsr: download");
     const size_t n = plan.progs.size();
     if (n == 0) return RSR_OK;
     cudaError_t e;
@@ -508,6 +512,7 @@ static rsr_population single_pop(const rsr_program *p, uint64_t offs[6]) {
 // plan's buffers are rewritten only after the device is done with them.
 static int run_chunked(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *dsp, uint64_t ds, int kernel,
                        bool gradient, float *mse, float *grad, uint32_t n_chunks) {
+    NvtxRange nvtx_range("rsr: chunked call");
     const uint32_t n = pop.n_programs, stride = gradient ? 33u : 1u;
     cudaError_t e;
     if ((e = ctx->results.reserve((size_t)n * stride * sizeof(float))) != cudaSuccess)

@@ -10,12 +10,22 @@
 #include <unordered_map>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/rsr_gpu.h"
 #include "encoder.h"
 #include "kernels.h"
 #include "uops.h"
 
 namespace rsr {
+
+// NVTX range for profiler timelines (a no-op unless a profiler is attached).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 void set_error(const std::string &msg);
 int fail(int code, const std::string &msg);

@@ -155,6 +155,7 @@ std::string thread_error() {
 // One launch over the merged population of `batch` (all MSE or all
 // MSE+gradient); writes every job's outputs.  Returns the launch status.
 int run_eval(rsr_server *S, Slot &slot, const std::vector<JobPtr> &batch) {
+    NvtxRange nvtx_range("rsr: serving batch");
     rsr_ctx *ctx = S->ctx;
     const bool gradient = batch[0]->kind == RSR_JOB_MSE_GRAD;
     std::vector<uint32_t> code;
