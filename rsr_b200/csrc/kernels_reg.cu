@@ -402,11 +402,19 @@ __global__ void __launch_bounds__(kRegThreads, reg_min_blocks<PROF, P>()) reg_ev
                     k.s = sacc[(g * 2) * 32 + lane];
                     k.c = sacc[(g * 2 + 1) * 32 + lane];
                     if (full) {
+                        // the lane's P squared errors summed pairwise, then one
+                        // compensated add per tile
+                        float sq[P];
 #pragma unroll
                         for (int q = 0; q < P; ++q) {
                             const float d = pred.v[q] - y.v[q];
-                            k.add(d * d);
+                            sq[q] = d * d;
                         }
+#pragma unroll
+                        for (int h = P / 2; h > 0; h /= 2)
+#pragma unroll
+                            for (int q = 0; q < h; ++q) sq[q] = sq[q] + sq[q + h];
+                        k.add(sq[0]);
                     } else {
 #pragma unroll
                         for (int q = 0; q < P; ++q) {
