@@ -64,6 +64,57 @@ void HostBuf::release() {
     cap = 0;
 }
 
+TaskPool::TaskPool(unsigned threads) {
+    for (unsigned i = 1; i < threads; ++i) threads_.emplace_back([this] { work(); });
+}
+
+TaskPool::~TaskPool() {
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto &t : threads_) t.join();
+}
+
+void TaskPool::work() {
+    uint64_t seen = 0;
+    for (;;) {
+        const std::function<void(uint32_t)> *f;
+        uint32_t n;
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] { return stop_ || epoch_ != seen; });
+            if (stop_) return;
+            seen = epoch_;
+            f = task_;
+            n = n_;
+        }
+        for (uint32_t i = next_.fetch_add(1); i < n; i = next_.fetch_add(1)) (*f)(i);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            if (++finished_ == threads_.size()) done_cv_.notify_all();
+        }
+    }
+}
+
+void TaskPool::run(uint32_t n, const std::function<void(uint32_t)> &f) {
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        task_ = &f;
+        n_ = n;
+        next_.store(0);
+        finished_ = 0;
+        ++epoch_;
+    }
+    cv_.notify_all();
+    for (uint32_t i = next_.fetch_add(1); i < n; i = next_.fetch_add(1)) f(i);
+    // every worker takes part in every run and has left it before the next
+    // one starts, so none can pick up this run's task or counter late
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&] { return finished_ == threads_.size(); });
+}
+
 static constexpr int kRegPathStride = 8;          // register path = profile + 8 * spill-depth class
 static constexpr uint64_t kChunkPoints = 4096;   // points per work-item chunk (all P)
 static constexpr uint64_t kStrideAlign = 1024;   // dataset column padding
@@ -147,15 +198,14 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                                 (uint32_t)(pop.param_off[i + 1] - p0), P.datasets[prog_ds[i]].num_features, &enc[i],
                                 &emsg[i], fuse, f);
     };
-    const uint32_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    const uint32_t nthreads = n >= 512 ? hw : 1;
-    if (nthreads > 1) {
-        std::vector<std::thread> th;
-        for (uint32_t t = 0; t < nthreads; ++t)
-            th.emplace_back([&, t] {
-                for (uint32_t i = t; i < n; i += nthreads) encode_one(i, forms);
-            });
-        for (auto &x : th) x.join();
+    if (n >= 256) {
+        if (!ctx->encoders)
+            ctx->encoders = std::make_unique<TaskPool>(std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+        // programs in blocks of 16 per task
+        const uint32_t nb = (n + 15) / 16;
+        ctx->encoders->run(nb, [&](uint32_t b) {
+            for (uint32_t i = b * 16; i < std::min(n, b * 16 + 16); ++i) encode_one(i, forms);
+        });
     } else {
         for (uint32_t i = 0; i < n; ++i) encode_one(i, forms);
     }

@@ -3,6 +3,9 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <condition_variable>
+#include <functional>
+#include <thread>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -18,6 +21,30 @@
 #include "uops.h"
 
 namespace rsr {
+
+// A fixed set of host threads for data-parallel host work (program
+// encoding): run(n, f) calls f(0..n-1) across the threads and returns when
+// all calls are done.  One caller at a time (build_plan runs under the
+// context's lock).
+class TaskPool {
+  public:
+    explicit TaskPool(unsigned threads);
+    ~TaskPool();
+    unsigned size() const { return (unsigned)threads_.size() + 1; }
+    void run(uint32_t n, const std::function<void(uint32_t)> &f);
+
+  private:
+    void work();
+    std::vector<std::thread> threads_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void(uint32_t)> *task_ = nullptr;
+    uint32_t n_ = 0;
+    std::atomic<uint32_t> next_{0};
+    size_t finished_ = 0;
+    uint64_t epoch_ = 0;
+    bool stop_ = false;
+};
 
 // NVTX range for profiler timelines (a no-op unless a profiler is attached).
 struct NvtxRange {
@@ -144,6 +171,7 @@ struct rsr_ctx {
     rsr::DevicePlan scratch;   // for one-shot calls
     rsr::DevicePlan pipe[2];   // one-shot calls split into chunks, alternating
     rsr::HostBuf results;      // pinned results of a chunked one-shot call
+    std::unique_ptr<rsr::TaskPool> encoders;  // host threads for program encoding
     void *l2buf = nullptr;
     size_t l2bytes = 0;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
