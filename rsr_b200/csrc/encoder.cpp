@@ -109,6 +109,23 @@ struct SlotPool {
     }
 };
 
+// Working storage of one encoding thread, kept between programs so that an
+// encoding allocates only while a program is larger than any before it.
+struct Scratch {
+    std::vector<uint32_t> flat;
+    std::vector<Node> nodes;
+    std::vector<int> instr_node, work;
+    std::vector<char> live;
+    // accumulator form
+    std::vector<uint32_t> writes, code;
+    std::vector<int> size;
+    // tape form
+    std::vector<int> idx, pos, vend, astart;
+    std::vector<uint32_t> vs, as;
+    SlotPool vals, adjs;
+};
+thread_local Scratch tls;
+
 // Tape form for the adjoint kernel.  Live nodes in program order; node t runs
 // forward at time t and in reverse at time 2N-1-t.  A value slot lives from
 // its definition to its last forward read, or to the reverse step of the
@@ -121,8 +138,10 @@ struct SlotPool {
 // 5 per node: op | aux << 8 | out_width << 28, vo | ao << 16, and
 // vi | ai << 16 for inputs 0..2.
 void emit_tape(const std::vector<Node> &nodes, const std::vector<char> &live, int root, EncodedProgram *E) {
-    std::vector<int> idx;  // tape order -> node id
-    std::vector<int> pos(nodes.size(), -1);
+    std::vector<int> &idx = tls.idx;  // tape order -> node id
+    std::vector<int> &pos = tls.pos;
+    idx.clear();
+    pos.assign(nodes.size(), -1);
     for (size_t i = 0; i < nodes.size(); ++i)
         if (live[i]) {
             pos[i] = (int)idx.size();
@@ -130,7 +149,9 @@ void emit_tape(const std::vector<Node> &nodes, const std::vector<char> &live, in
         }
     const int N = (int)idx.size();
     const int rev = 2 * N - 1;
-    std::vector<int> vend(N, -1), astart(N, 1 << 30);
+    std::vector<int> &vend = tls.vend, &astart = tls.astart;
+    vend.assign(N, -1);
+    astart.assign(N, 1 << 30);
     for (int t = 0; t < N; ++t) {
         const Node &n = nodes[idx[t]];
         const int rr = n.stale ? 0 : reverse_reads(n.opcode);
@@ -152,9 +173,13 @@ void emit_tape(const std::vector<Node> &nodes, const std::vector<char> &live, in
         vend[rt] = std::max(vend[rt], N);          // read for the prediction
         astart[rt] = std::min(astart[rt], N - 1);  // seeded before the reverse sweep
     }
-    SlotPool vals, adjs;
+    SlotPool &vals = tls.vals, &adjs = tls.adjs;
+    vals.busy_until.clear();
+    adjs.busy_until.clear();
     adjs.take(9, -1, 1 << 30);  // the sink
-    std::vector<uint32_t> vs(N, 0), as(N, 0);
+    std::vector<uint32_t> &vs = tls.vs, &as = tls.as;
+    vs.assign(N, 0);
+    as.assign(N, 0);
     auto is_feature = [&](int t) {
         const Node &n = nodes[idx[t]];
         return !n.stale && is_load(n.opcode) && !is_const_load(n.opcode) && n.arg < kTapeFeature;
@@ -257,7 +282,11 @@ BinIdx bin_index(int opcode) {
 class AccEmitter {
    public:
     explicit AccEmitter(const std::vector<Node> &nodes)
-        : nodes_(nodes), writes_(nodes.size(), 0), size_(nodes.size(), 0) {}
+        : code(tls.code), nodes_(nodes), writes_(tls.writes), size_(tls.size) {
+        code.clear();
+        writes_.assign(nodes.size(), 0);
+        size_.assign(nodes.size(), 0);
+    }
 
     bool analyze(int id) {  // accumulator write sets and subtree sizes; false if unsupported
         const Node &n = nodes_[id];
@@ -383,7 +412,7 @@ class AccEmitter {
         }
     }
 
-    std::vector<uint32_t> code;
+    std::vector<uint32_t> &code;
     int max_sp[N_STACKS] = {0, 0, 0, 0, 0};
     uint32_t types_ = 0;  // accumulator types used
 
@@ -423,8 +452,8 @@ class AccEmitter {
     void emit(int kind, uint32_t arg) { code.push_back(uop_word((uint32_t)kind, arg)); }
 
     const std::vector<Node> &nodes_;
-    std::vector<uint32_t> writes_;
-    std::vector<int> size_;
+    std::vector<uint32_t> &writes_;
+    std::vector<int> &size_;
     int sp_[N_STACKS] = {0, 0, 0, 0, 0};
 };
 
@@ -449,40 +478,43 @@ int post_op_of(int kind, int t) {
 
 bool is_unary_kind(int kind, int t) { return post_op_of(kind, t) != 0; }
 
+// Both passes rewrite the code in place: a word is written at or before the
+// position just read, after the words it depends on were read.
 void fuse_loads(std::vector<uint32_t> *code) {
-    const std::vector<uint32_t> &c = *code;
+    std::vector<uint32_t> &c = *code;
     // 1. a load directly followed by a unary op on the loaded value
-    std::vector<uint32_t> out;
+    size_t w = 0;
     for (size_t i = 0; i < c.size(); ++i) {
         const int kind = (int)(c[i] & 0xFFu);
         const int t = kind_block(kind), k = kind - kBlockBase[t];
         if ((k == KV_LDX || k == KV_LDC) && i + 1 < c.size()) {
             const int kn = (int)(c[i + 1] & 0xFFu);
             if (kind_block(kn) == t && is_unary_kind(kn, t)) {
-                out.push_back(uop_word((uint32_t)kn, unary_load_arg(c[i] >> 8, k == KV_LDX ? 1u : 2u)));
+                c[w++] = uop_word((uint32_t)kn, unary_load_arg(c[i] >> 8, k == KV_LDX ? 1u : 2u));
                 ++i;
                 continue;
             }
         }
-        out.push_back(c[i]);
+        c[w++] = c[i];
     }
+    c.resize(w);
     // 2. a PUSH directly followed by a load
-    std::vector<uint32_t> fin;
-    for (size_t i = 0; i < out.size(); ++i) {
-        const int kind = (int)(out[i] & 0xFFu);
+    w = 0;
+    for (size_t i = 0; i < c.size(); ++i) {
+        const int kind = (int)(c[i] & 0xFFu);
         const int t = kind_block(kind), k = kind - kBlockBase[t];
-        if (k == KV_PUSH && i + 1 < out.size()) {
-            const int kn = (int)(out[i + 1] & 0xFFu), tn = kind_block(kn), kk = kn - kBlockBase[tn];
+        if (k == KV_PUSH && i + 1 < c.size()) {
+            const int kn = (int)(c[i + 1] & 0xFFu), tn = kind_block(kn), kk = kn - kBlockBase[tn];
             if (kk == KV_LDX || kk == KV_LDC) {
-                fin.push_back(uop_word((uint32_t)kind, push_load_arg(out[i] >> 8, (uint32_t)tn + 1u,
-                                                                     kk == KV_LDC ? 1u : 0u, out[i + 1] >> 8)));
+                c[w++] = uop_word((uint32_t)kind, push_load_arg(c[i] >> 8, (uint32_t)tn + 1u, kk == KV_LDC ? 1u : 0u,
+                                                               c[i + 1] >> 8));
                 ++i;
                 continue;
             }
         }
-        fin.push_back(out[i]);
+        c[w++] = c[i];
     }
-    *code = std::move(fin);
+    c.resize(w);
 }
 
 void set_err(std::string *err, const std::string &m) {
@@ -495,12 +527,13 @@ int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uin
                    const float *params, uint32_t n_params, uint32_t num_features, EncodedProgram *out,
                    std::string *err, bool fuse, unsigned forms) {
     EncodedProgram &E = *out;
-    E = EncodedProgram();
+    E.reset();
     if (len > 0 && !code) { set_err(err, "code is null"); return RSR_EINVAL; }
     if (n_consts > 0 && !kinds) { set_err(err, "const_kinds is null"); return RSR_EINVAL; }
     if (n_params > 0 && !params) { set_err(err, "params is null"); return RSR_EINVAL; }
     // flat parameter offsets (get_flat_start_idx, evaluator.rs:232-245)
-    std::vector<uint32_t> flat(n_consts + 1, 0);
+    std::vector<uint32_t> &flat = tls.flat;
+    flat.assign(n_consts + 1, 0);
     for (uint32_t c = 0; c < n_consts; ++c) {
         if (kinds[c] > 6) { set_err(err, "constant " + std::to_string(c) + " has unknown kind"); return RSR_EPROGRAM; }
         flat[c + 1] = flat[c] + kKindWidth[kinds[c]];
@@ -514,10 +547,13 @@ int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uin
     E.consts.assign(params, params + n_params);
 
     // ---- replay the stack discipline on value ids
-    std::vector<Node> nodes;
-    nodes.reserve(len);
-    std::vector<int> stack[N_STACKS];
-    std::vector<int> instr_node;  // node id per kept instruction
+    std::vector<Node> &nodes = tls.nodes;
+    nodes.clear();
+    // the reference's stacks hold at most kRefStackSlots values each
+    int stack[N_STACKS][kRefStackSlots];
+    int sp[N_STACKS] = {0, 0, 0, 0, 0};
+    std::vector<int> &instr_node = tls.instr_node;  // node id per kept instruction
+    instr_node.clear();
     int last[N_STACKS][kRefStackSlots];
     for (auto &row : last) std::fill(row, row + kRefStackSlots, -1);
     for (uint32_t pc = 0; pc < len; ++pc) {
@@ -542,7 +578,7 @@ int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uin
                 if (a >= n_consts) { set_err(err, "pc " + std::to_string(pc) + ": constant index out of range"); return RSR_EPROGRAM; }
                 if (kinds[a] != const_kind_for_load(op)) {
                     n.stale = true;
-                    int p = (int)stack[t].size();
+                    int p = sp[t];
                     n.alias = p < kRefStackSlots ? last[t][p] : -1;
                 } else {
                     n.arg = flat[a];
@@ -553,19 +589,19 @@ int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uin
             for (int i = 0; i < g.n_in; ++i) cnt[g.in[i]]++;
             int base[N_STACKS];
             for (int t = 0; t < N_STACKS; ++t) {
-                if ((int)stack[t].size() < cnt[t]) {
+                if (sp[t] < cnt[t]) {
                     set_err(err, "pc " + std::to_string(pc) + ": stack underflow");
                     return RSR_EPROGRAM;
                 }
-                base[t] = (int)stack[t].size() - cnt[t];
+                base[t] = sp[t] - cnt[t];
             }
             n.n_in = g.n_in;
             for (int i = 0; i < g.n_in; ++i) n.in[i] = stack[g.in[i]][base[g.in[i]]++];
-            for (int t = 0; t < N_STACKS; ++t) stack[t].resize(stack[t].size() - cnt[t]);
+            for (int t = 0; t < N_STACKS; ++t) sp[t] -= cnt[t];
             n.out = g.out;
         }
         int t = n.out;
-        n.pos = (int)stack[t].size();
+        n.pos = sp[t];
         if (n.pos >= kRefStackSlots) {
             set_err(err, "pc " + std::to_string(pc) + ": more than 32 values on a stack");
             return RSR_EPROGRAM;
@@ -573,17 +609,19 @@ int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uin
         int id = (int)nodes.size();
         nodes.push_back(n);
         instr_node.push_back(id);
-        stack[t].push_back(id);
+        stack[t][sp[t]++] = id;
         if (!n.stale) last[t][n.pos] = id;
-        E.depth_ref[t] = std::max(E.depth_ref[t], (int)stack[t].size());
+        E.depth_ref[t] = std::max(E.depth_ref[t], sp[t]);
     }
     int root = last[SF][0];
     E.result_zero = root < 0;
 
     // live tree (DAG through stale aliases) behind stack_f[0]
-    std::vector<char> live(nodes.size(), 0);
+    std::vector<char> &live = tls.live;
+    live.assign(nodes.size(), 0);
     if (root >= 0) {
-        std::vector<int> work{root};
+        std::vector<int> &work = tls.work;
+        work.assign(1, root);
         while (!work.empty()) {
             int id = work.back();
             work.pop_back();
@@ -651,7 +689,7 @@ int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uin
             }
             for (int p = 0; fits && p < N_PROFILES; ++p)
                 if ((em.types_ & ~kProfileTypes[p]) == 0) { E.profile = p; break; }
-            if (E.profile >= 0) E.reg_code = std::move(em.code);
+            if (E.profile >= 0) E.reg_code.assign(em.code.begin(), em.code.end());
         }
     }
     return RSR_OK;

@@ -46,6 +46,16 @@ struct EncodedProgram {
     std::vector<uint32_t> tape_code;      // 2 header words + 5 words per live node
     uint32_t n_tape_val = 0, n_tape_adj = 0;  // scalar value / adjoint slots
     int tape_profile = P_ALL;             // smallest kernel profile covering the live values' types
+
+    // Back to the default state; the vectors keep their capacity, so an
+    // EncodedProgram reused across calls stops allocating.
+    void reset() {
+        std::vector<float> c = std::move(consts);
+        std::vector<uint32_t> sc = std::move(slot_code), rc = std::move(reg_code), tc = std::move(tape_code);
+        *this = EncodedProgram();
+        c.clear(); sc.clear(); rc.clear(); tc.clear();
+        consts = std::move(c); slot_code = std::move(sc); reg_code = std::move(rc); tape_code = std::move(tc);
+    }
 };
 
 // Validates and encodes.  num_features == 0 skips feature-range checks.

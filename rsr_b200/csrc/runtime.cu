@@ -152,13 +152,11 @@ static TuneChoice choice_for(rsr_ctx *ctx, int profile, uint64_t n_eval) {
     return c;
 }
 
-static uint32_t align4h(uint32_t v) { return (v + 3u) & ~3u; }
-
 int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_prog, uint64_t ds_all, int kernel,
                bool gradient, int mode, Plan *plan) {
     NvtxRange nvtx_range("rsr: encode + plan");
     Plan &P = *plan;
-    P = Plan();
+    P.reset();
     P.gradient = gradient;
     P.mode = mode;
     const uint32_t n = pop.n_programs;
@@ -188,9 +186,14 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             return fail(RSR_EINVAL, "population offsets decrease at " + std::to_string(i));
     const bool fuse = (ctx->opts.flags & RSR_OPT_NO_LOAD_FUSION) == 0;
     const unsigned forms = gradient ? FORM_TAPE : kernel == RSR_KERNEL_PLAIN ? FORM_SLOT : FORM_ACC;
-    std::vector<EncodedProgram> enc(n);
-    std::vector<int> erc(n, RSR_OK);
-    std::vector<std::string> emsg(n);
+    if (ctx->enc_cache.size() < n) {
+        ctx->enc_cache.resize(n);
+        ctx->enc_rc.resize(n);
+        ctx->enc_msg.resize(n);
+    }
+    std::vector<EncodedProgram> &enc = ctx->enc_cache;
+    std::vector<int> &erc = ctx->enc_rc;
+    std::vector<std::string> &emsg = ctx->enc_msg;
     auto encode_one = [&](uint32_t i, unsigned f) {
         const uint64_t c0 = pop.code_off[i], k0 = pop.kind_off[i], p0 = pop.param_off[i];
         erc[i] = encode_program(pop.code + c0, (uint32_t)(pop.code_off[i + 1] - c0), pop.const_kinds + k0,
@@ -257,6 +260,16 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
     });
     P.progs.resize(n);
     P.orig = order;
+    {
+        size_t cw = 0, cf = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            const EncodedProgram &E = enc[i];
+            cw += path[i] <= -2 ? E.tape_code.size() : path[i] == -1 ? E.slot_code.size() : E.reg_code.size();
+            cf += E.consts.size();
+        }
+        P.code.reserve(cw);
+        P.consts.reserve(cf);
+    }
     uint32_t part = 0;
     for (uint32_t li = 0; li < n; ++li) {
         const uint32_t i = order[li];
@@ -283,7 +296,10 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         P.program_points += n_eval;
     }
     P.n_partials = part * (gradient ? kGradSlotDoubles : 1);
-    // work items, one group per (path) run
+    // work items, one group per (path) run; an item has at most as many
+    // chunks as its first program has partial sums
+    P.items.reserve(part);
+    static thread_local std::vector<std::pair<uint64_t, WorkItem>> items, full, tail;
     uint32_t li = 0;
     while (li < n) {
         const int pth = path[order[li]];
@@ -310,7 +326,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         }
         // tile size and per-warp staging requirements
         uint32_t j = li;
-        std::vector<std::pair<uint64_t, WorkItem>> items;
+        items.clear();
         while (j < end) {
             uint32_t k = j + 1;
             const uint32_t ds = P.progs[j].dataset;
@@ -351,26 +367,35 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             }
             g.P = Pp;
         }
-        // expand chunks
-        std::vector<std::pair<uint64_t, WorkItem>> chunks;
+        // Expand each item into chunks of kChunkPoints and order them longest
+        // first (persistent kernels pull items in this order; any order
+        // gives the same sums).  A chunk's work is its programs' code length
+        // times its tiles: every chunk but an item's last has the same tile
+        // count whatever the dataset, so the items sorted by code length give
+        // the full chunks in order, and the short last chunks are merged in.
         const uint64_t tile_pts = 32ull * g.P;
+        const uint64_t tpc = kChunkPoints / tile_pts;
+        std::stable_sort(items.begin(), items.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+        full.clear();
+        tail.clear();
         for (auto &pr : items) {
             const WorkItem &w = pr.second;
             const uint64_t n_eval = P.datasets[P.progs[w.prog_begin].dataset].n_eval;
             const uint64_t n_tiles = (n_eval + tile_pts - 1) / tile_pts;
-            const uint64_t tpc = kChunkPoints / tile_pts;
             for (uint64_t c = 0, t = 0; t < n_tiles; ++c, t += tpc) {
                 WorkItem it = w;
                 it.tile_begin = (uint32_t)t;
                 it.tile_end = (uint32_t)std::min(n_tiles, t + tpc);
                 it.chunk = (uint32_t)c;
-                chunks.emplace_back(pr.first * (it.tile_end - it.tile_begin), it);
+                const uint64_t tiles = it.tile_end - it.tile_begin;
+                (tiles == tpc ? full : tail).emplace_back(pr.first * tiles, it);
             }
         }
-        // longest first (persistent kernels pull items in this order)
-        std::stable_sort(chunks.begin(), chunks.end(),
-                         [](const auto &a, const auto &b) { return a.first > b.first; });
-        for (auto &c : chunks) P.items.push_back(c.second);
+        std::stable_sort(tail.begin(), tail.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+        size_t a = 0, b = 0;
+        while (a < full.size() || b < tail.size())
+            P.items.push_back(b == tail.size() || (a < full.size() && full[a].first >= tail[b].first) ? full[a++].second
+                                                                                                   : tail[b++].second);
         g.n_items = (uint32_t)P.items.size() - g.item_begin;
         for (uint32_t q = li; q < end; ++q) {
             const EncodedProgram &E = enc[order[q]];
@@ -409,6 +434,16 @@ int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st
         if ((e = cudaEventSynchronize(dev->staged)) != cudaSuccess) return cuda_fail(e, "staging wait");
     } else if ((e = cudaEventCreateWithFlags(&dev->staged, cudaEventDisableTiming)) != cudaSuccess) {
         return cuda_fail(e, "cudaEventCreate");
+    }
+    if (!dev->fork) {
+        if ((e = cudaEventCreateWithFlags(&dev->fork, cudaEventDisableTiming)) != cudaSuccess)
+            return cuda_fail(e, "cudaEventCreate");
+        for (int i = 0; i < 2; ++i) {
+            if ((e = cudaEventCreateWithFlags(&dev->join[i], cudaEventDisableTiming)) != cudaSuccess)
+                return cuda_fail(e, "cudaEventCreate");
+            if ((e = cudaStreamCreateWithFlags(&dev->side[i], cudaStreamNonBlocking)) != cudaSuccess)
+                return cuda_fail(e, "cudaStreamCreate");
+        }
     }
     if ((e = dev->staging.reserve(total)) != cudaSuccess) return cuda_fail(e, "cudaHostAlloc");
     char *h = (char *)dev->staging.p;
@@ -450,9 +485,25 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
     uint32_t *counters = (uint32_t *)dev->counters.p;
     if ((e = cudaMemsetAsync(counters, 0, plan.groups.size() * sizeof(uint32_t), st)) != cudaSuccess)
         return cuda_fail(e, "counter reset");
+    // Launch j > 0 goes to side stream (j - 1) % 2 unless per-launch timing is
+    // asked for (events around each launch then time it alone).  Launches
+    // share nothing but the partials, which each item writes at its own index.
+    const bool concurrent = !group_events && dev->side[0];
+    unsigned forked = 0;
+    int j = -1;
     for (size_t gi = 0; gi < plan.groups.size(); ++gi) {
         const Group &g = plan.groups[gi];
         if (g.n_items == 0) continue;
+        cudaStream_t gs = st;
+        if (concurrent && ++j > 0) {
+            const int sd = (j - 1) & 1;
+            if (!(forked & (1u << sd))) {
+                if (!forked && (e = cudaEventRecord(dev->fork, st)) != cudaSuccess) return cuda_fail(e, "fork");
+                if ((e = cudaStreamWaitEvent(dev->side[sd], dev->fork, 0)) != cudaSuccess) return cuda_fail(e, "fork");
+                forked |= 1u << sd;
+            }
+            gs = dev->side[sd];
+        }
         LaunchArgs a = dev->base;
         a.items = dev->base.items + g.item_begin;
         a.n_items = g.n_items;
@@ -461,14 +512,14 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
         a.smem_const_floats = g.const_floats;
         a.smem_slots = g.slots;
         a.progs_per_warp = g.G;
-        if (group_events) cudaEventRecord(group_events[2 * gi], st);
+        if (group_events) cudaEventRecord(group_events[2 * gi], gs);
         if (g.kind == 0) {
             const size_t per = plain_smem_per_warp(g.code_words, g.const_floats, g.slots, g.P);
             uint32_t wpb = (uint32_t)std::max<size_t>(1, std::min<size_t>(kPlainThreads / 32, (200 * 1024) / per));
             g.grid = (g.n_items + wpb - 1) / wpb;
             g.smem = per * wpb;
             g.warps_per_block = wpb;
-            e = launch_plain(a, g.P, wpb, per * wpb, st);
+            e = launch_plain(a, g.P, wpb, per * wpb, gs);
         } else if (g.kind == 1) {
             reg_layout(g.code_words, g.const_floats, g.stack_depth, g.P, g.G, a.stack_off, &a.acc_off, &a.region_floats,
                        &a.block_hdr_floats);
@@ -478,7 +529,7 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             g.grid = std::max(1u, grid);
             g.smem = smem;
             g.warps_per_block = kRegThreads / 32;
-            e = launch_reg(a, g.profile, g.P, g.grid, st);
+            e = launch_reg(a, g.profile, g.P, g.grid, gs);
         } else {
             const size_t per = grad_smem_per_warp(g.code_words, g.const_floats, g.slots, g.adj_slots, g.P);
             a.smem_adj_slots = g.adj_slots;
@@ -489,12 +540,17 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             g.grid = (g.n_items + wpb - 1) / wpb;
             g.smem = per * wpb;
             g.warps_per_block = wpb;
-            e = launch_grad(a, g.profile, wpb, per * wpb, st);
+            e = launch_grad(a, g.profile, wpb, per * wpb, gs);
         }
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
-        if (group_events) cudaEventRecord(group_events[2 * gi + 1], st);
+        if (group_events) cudaEventRecord(group_events[2 * gi + 1], gs);
         ctx->launches++;
     }
+    for (int sd = 0; sd < 2; ++sd)
+        if (forked & (1u << sd)) {
+            if ((e = cudaEventRecord(dev->join[sd], dev->side[sd])) != cudaSuccess) return cuda_fail(e, "join");
+            if ((e = cudaStreamWaitEvent(st, dev->join[sd], 0)) != cudaSuccess) return cuda_fail(e, "join");
+        }
     if (ev_mid) cudaEventRecord(ev_mid, st);
     if (plan.mode == MODE_MSE && plan.raw_sums) {
         e = launch_finalize_sums(dev->base.progs, dev->base.partials, n, plan.gradient ? 33u : 1u,
@@ -558,19 +614,25 @@ static rsr_population single_pop(const rsr_program *p, uint64_t offs[6]) {
 
 // A large MSE (or MSE + gradient) call in chunks of programs: the host
 // encodes chunk k+1 while the device runs chunk k.  Chunks alternate between
-// two device plans; every launch and copy is on the context's stream, so a
-// plan's buffers are rewritten only after the device is done with them.
+// two device plans, each with its own stream, so chunk k+1's first launch
+// fills the SMs that chunk k's last blocks leave; a plan's buffers are
+// rewritten by a later chunk on the same stream, after the device is done
+// with them.
 static int run_chunked(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *dsp, uint64_t ds, int kernel,
-                       bool gradient, float *mse, float *grad, uint32_t n_chunks) {
+                       bool gradient, float *mse, float *grad, const std::vector<uint32_t> &start) {
+    const uint32_t n_chunks = (uint32_t)start.size() - 1;
     NvtxRange nvtx_range("rsr: chunked call");
     const uint32_t n = pop.n_programs, stride = gradient ? 33u : 1u;
     cudaError_t e;
     if ((e = ctx->results.reserve((size_t)n * stride * sizeof(float))) != cudaSuccess)
         return cuda_fail(e, "cudaHostAlloc");
     float *res = (float *)ctx->results.p;
-    std::vector<Plan> plans(n_chunks);
-    std::vector<uint32_t> start(n_chunks + 1);
-    for (uint32_t k = 0; k <= n_chunks; ++k) start[k] = (uint32_t)((uint64_t)n * k / n_chunks);
+    if (ctx->call_plans.size() < n_chunks) ctx->call_plans.resize(n_chunks);
+    std::vector<Plan> &plans = ctx->call_plans;
+    auto sync_both = [&] {
+        cudaStreamSynchronize(ctx->stream2);
+        cudaStreamSynchronize(ctx->stream);
+    };
     uint64_t h2d = 0;
     for (uint32_t k = 0; k < n_chunks; ++k) {
         const uint32_t s0 = start[k], cnt = start[k + 1] - s0;
@@ -588,17 +650,21 @@ static int run_chunked(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *
                 size_t end = m.find(':', at);
                 m = "program " + std::to_string(s0 + std::stoul(m.substr(at, end - at))) + m.substr(end);
             }
-            cudaStreamSynchronize(ctx->stream);
+            sync_both();
             return fail(rc, m);
         }
         DevicePlan *dev = &ctx->pipe[k & 1];
-        if ((rc = upload_plan(ctx, plans[k], dev, ctx->stream))) return rc;
+        cudaStream_t st = (k & 1) ? ctx->stream2 : ctx->stream;
+        if ((rc = upload_plan(ctx, plans[k], dev, st))) { sync_both(); return rc; }
         h2d += ctx->last_h2d;
-        if ((rc = enqueue_plan(ctx, plans[k], dev, ctx->stream, nullptr))) return rc;
+        if ((rc = enqueue_plan(ctx, plans[k], dev, st, nullptr))) { sync_both(); return rc; }
         if ((e = cudaMemcpyAsync(res + (size_t)s0 * stride, dev->out.p, (size_t)cnt * stride * sizeof(float),
-                                 cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess)
+                                 cudaMemcpyDeviceToHost, st)) != cudaSuccess) {
+            sync_both();
             return cuda_fail(e, "result download");
+        }
     }
+    if ((e = cudaStreamSynchronize(ctx->stream2)) != cudaSuccess) return cuda_fail(e, "evaluation");
     if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(e, "evaluation");
     for (uint32_t k = 0; k < n_chunks; ++k) {
         const uint32_t s0 = start[k], cnt = start[k + 1] - s0;
@@ -614,14 +680,30 @@ static int run_chunked(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *
     return RSR_OK;
 }
 
-static constexpr uint32_t kChunkPrograms = 1024;  // programs per chunk of a chunked call
+// Chunks of a chunked call double in size from kFirstChunk programs up to
+// kMaxChunk, and the last one takes the rest (up to one and a half chunks):
+// the device starts on a small first chunk soon, and since the host plans a
+// program several times faster than the device runs it, each later chunk is
+// planned while the device still runs the chunks before it.
+static constexpr uint32_t kFirstChunk = 256, kMaxChunk = 8192;
+
+static std::vector<uint32_t> chunk_starts(uint32_t n) {
+    std::vector<uint32_t> start{0};
+    uint32_t size = kFirstChunk;
+    while (n - start.back() > size + size / 2) {
+        start.push_back(start.back() + size);
+        if (size < kMaxChunk) size *= 2;
+    }
+    start.push_back(n);
+    return start;
+}
 
 static int run_oneshot(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *dsp, uint64_t ds, int kernel,
                        bool gradient, int mode, float *mse, float *grad, float *points) {
-    if (mode == MODE_MSE && pop.n_programs >= 2 * kChunkPrograms)
-        return run_chunked(ctx, pop, dsp, ds, kernel, gradient, mse, grad,
-                           std::min<uint32_t>(8, pop.n_programs / kChunkPrograms));
-    Plan plan;
+    if (mode == MODE_MSE && pop.n_programs >= 4 * kFirstChunk)
+        return run_chunked(ctx, pop, dsp, ds, kernel, gradient, mse, grad, chunk_starts(pop.n_programs));
+    if (ctx->call_plans.empty()) ctx->call_plans.resize(1);
+    Plan &plan = ctx->call_plans[0];
     int rc = build_plan(ctx, pop, dsp, ds, kernel, gradient, mode, &plan);
     if (rc) return rc;
     if (mode == MODE_POINTS) {
@@ -698,7 +780,9 @@ int rsr_ctx_create(int device, const rsr_options *opts, rsr_ctx **out) {
     ctx->num_sms = prop.multiProcessorCount;
     rsr_options_default(&ctx->opts);
     if (opts) memcpy(&ctx->opts, opts, std::min<size_t>(sizeof(rsr_options), opts->struct_size ? opts->struct_size : sizeof(rsr_options)));
-    if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking)) != cudaSuccess) {
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
         delete ctx;
         return cuda_fail(e, "stream");
     }
@@ -716,6 +800,7 @@ int rsr_ctx_destroy(rsr_ctx *ctx) {
     if (!ctx) return RSR_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    cudaStreamSynchronize(ctx->stream2);
     for (auto &kv : ctx->datasets) {
         cudaFree(kv.second->x);
         cudaFree(kv.second->y);
@@ -732,6 +817,7 @@ int rsr_ctx_destroy(rsr_ctx *ctx) {
     if (ctx->l2buf) cudaFree(ctx->l2buf);
     for (auto &ev : ctx->ev) if (ev) cudaEventDestroy(ev);
     cudaStreamDestroy(ctx->stream);
+    cudaStreamDestroy(ctx->stream2);
     delete ctx;
     return RSR_OK;
 }

@@ -134,6 +134,20 @@ struct Plan {
     uint64_t flops = 0;                     // algorithmic lane-ops of one run
     uint64_t program_points = 0;
     uint32_t n_plain = 0, n_reg = 0;
+
+    // Empty, with the vectors' capacity kept for the next build.
+    void reset() {
+        Plan keep = std::move(*this);
+        *this = Plan();
+        progs = std::move(keep.progs); progs.clear();
+        orig = std::move(keep.orig); orig.clear();
+        datasets = std::move(keep.datasets); datasets.clear();
+        ds_handles = std::move(keep.ds_handles); ds_handles.clear();
+        items = std::move(keep.items); items.clear();
+        code = std::move(keep.code); code.clear();
+        consts = std::move(keep.consts); consts.clear();
+        groups = std::move(keep.groups); groups.clear();
+    }
 };
 
 // Device copy of a plan plus the buffers one run writes.
@@ -145,6 +159,11 @@ struct DevicePlan {
     DevBuf status;
     HostBuf staging;    // pinned image of the pool, uploaded with one copy
     cudaEvent_t staged = nullptr;  // recorded after the staging buffer's copy
+    // Every launch of a plan but the first goes to one of two side streams,
+    // forked from and joined back into the caller's stream, so that a
+    // launch's blocks take the SMs that the previous launch's last blocks free.
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
     LaunchArgs base{};
     float *mse = nullptr, *grad = nullptr;
     DevicePlan() = default;
@@ -152,6 +171,11 @@ struct DevicePlan {
     DevicePlan &operator=(const DevicePlan &) = delete;
     ~DevicePlan() {
         if (staged) cudaEventDestroy(staged);
+        if (fork) cudaEventDestroy(fork);
+        for (int i = 0; i < 2; ++i) {
+            if (join[i]) cudaEventDestroy(join[i]);
+            if (side[i]) cudaStreamDestroy(side[i]);
+        }
     }
 };
 
@@ -161,6 +185,7 @@ struct rsr_ctx {
     int device = 0;
     int num_sms = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;  // odd chunks of a chunked one-shot call
     rsr_options opts{};
     std::mutex mu;
     std::map<uint64_t, std::unique_ptr<rsr::DatasetRec>> datasets;
@@ -172,6 +197,13 @@ struct rsr_ctx {
     rsr::DevicePlan pipe[2];   // one-shot calls split into chunks, alternating
     rsr::HostBuf results;      // pinned results of a chunked one-shot call
     std::unique_ptr<rsr::TaskPool> encoders;  // host threads for program encoding
+    // Kept between calls so that encoding and planning a population of a
+    // size seen before allocates nothing new: one encoding per program of
+    // the largest population so far, and the plans of one-shot calls.
+    std::vector<rsr::EncodedProgram> enc_cache;
+    std::vector<int> enc_rc;
+    std::vector<std::string> enc_msg;
+    std::vector<rsr::Plan> call_plans;
     void *l2buf = nullptr;
     size_t l2bytes = 0;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
