@@ -283,6 +283,21 @@ RSR_API int rsr_fit_nelder_mead(rsr_ctx *ctx, const rsr_population *pop, rsr_dat
                                 const rsr_dataset *ds_per_program, uint32_t max_iterations, float *params_out,
                                 float *mse_out, rsr_fit_stats *stats);
 
+/* run_cma_es (src/engine/optimize/cmaes.rs:19-192) for a whole population,
+ * the fit for non-differentiable programs with vector or matrix constants:
+ * max_iterations generations of 16 candidates per program (best 8
+ * recombined, diagonal covariance, sigma 0.5 shrinking by exp(-0.01), stop
+ * when the best MSE < 1e-8), objective mse + 0.01 * sum |x| over the
+ * reference's search vector (the flat parameters and a copy of them).  One
+ * launch scores the 16 candidates of every program.  The reference draws from
+ * an unseeded thread-local generator; here program i draws from a splitmix64
+ * stream seeded from (seed, i), so a population's result does not depend on
+ * its batching.  params_out receives the best point's parameters, mse_out[i]
+ * its MSE (the starting MSE for programs without parameters). */
+RSR_API int rsr_fit_cma_es(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const rsr_dataset *ds_per_program,
+                           uint32_t max_iterations, uint64_t seed, float *params_out, float *mse_out,
+                           rsr_fit_stats *stats);
+
 /* -------------------------------------------------- prepared batches */
 /* A population encoded and uploaded once, then run many times with inputs
  * resident on the device (the timed unit of the benchmark).  run() enqueues

@@ -124,6 +124,8 @@ _SIGS = {
                                       C.c_void_p, C.c_void_p, C.POINTER(FitStats)]),
     "rsr_fit_lbfgs": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p,
                                 C.c_void_p, C.POINTER(FitStats)]),
+    "rsr_fit_cma_es": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_uint32, C.c_uint64,
+                                 C.c_void_p, C.c_void_p, C.POINTER(FitStats)]),
     "rsr_batch_prepare": (C.c_int, [C.c_void_p, C.POINTER(Population), C.c_uint64, C.c_void_p, C.c_int, C.c_int,
                                     C.POINTER(C.c_void_p)]),
     "rsr_batch_run": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -20,7 +20,7 @@ BUILD = PKG / "_build"
 LIB = PKG / "librsrgpu.so"
 
 SOURCES = ["runtime.cu", "kernels_plain.cu", "kernels_reg.cu", "kernels_grad.cu", "encoder.cpp",
-           "serving.cu", "lbfgs.cu", "nelder_mead.cu", "ingest.cu", "noalloc.cu"]
+           "serving.cu", "lbfgs.cu", "nelder_mead.cu", "cma_es.cu", "ingest.cu", "noalloc.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-lineinfo", "-fmad=false",
               "-prec-div=true", "-prec-sqrt=true", "-Xcompiler", "-fPIC,-fvisibility=hidden,-ffp-contract=off",
               "-I", str(ROOT / "include"), "-I", str(HERE)]

@@ -221,6 +221,24 @@ class Engine:
                                               "gradient_evaluations": st.gradient_evaluations,
                                               "mse_evaluations": st.mse_evaluations}
 
+    def fit_cma_es(self, programs: PopulationLike, dataset=None, max_iterations: int = 6, datasets=None,
+                   seed: int = 0, rng: np.random.Generator = None):
+        """run_cma_es (src/engine/optimize/cmaes.rs:19-192) for every program
+        at once, program i drawing from a stream seeded from (seed, i); with
+        `rng` the seed is drawn from it.  Returns (fitted flat params, best
+        mse, stats)."""
+        pk = _packed(programs)
+        s, keep = _as_population(pk)
+        h, dsp = self._handles(pk.n, dataset, datasets)
+        if rng is not None:
+            seed = int(rng.integers(0, 2 ** 63))
+        params = np.zeros(max(1, len(pk.params)), np.float32)
+        mse = np.zeros(pk.n, np.float32)
+        st = N.FitStats()
+        N.check(N.lib().rsr_fit_cma_es(self.ctx, C.byref(s), h, dsp.ctypes.data if dsp is not None else None,
+                                       max_iterations, seed, params.ctypes.data, mse.ctypes.data, C.byref(st)))
+        return params[:len(pk.params)], mse, {"iterations": st.iterations, "mse_evaluations": st.mse_evaluations}
+
     def eval_points_batch(self, programs: PopulationLike, dataset, kernel: int = N.KERNEL_AUTO) -> np.ndarray:
         pk = _packed(programs)
         s, keep = _as_population(pk)
