@@ -250,6 +250,31 @@ def serving_bench(eng, jobs: int, rate: float, threads: int = 16, seed: int = 7,
                     "(program_points counts one evaluation per program)"}
 
 
+def search_bench(eng):
+    """Config C1 end to end: MSE of 1024 random scalar programs on 400
+    points, then the island search (24 islands x 25, the reference's
+    defaults, operators {+, -, *, /, sin, cos, exp}) to MSE < 1e-7 with
+    every score and constant fit on the engine."""
+    from rsr_b200 import isa as I
+    from rsr_b200 import workloads as W
+    from rsr_b200.search import engine as S
+    ds = W.scalar_dataset(400, seed=1)
+    d = eng.upload(ds)
+    pk = I.pack(W.scalar_population(1024, seed=11))
+    eng.compute_mse_batch(pk, d)
+    t0 = time.perf_counter()
+    eng.compute_mse_batch(pk, d)
+    t_pop = time.perf_counter() - t0
+    cfg = S.Config(excluded_ops=["SqrF", "SqrtF", "LnF"])
+    t0 = time.perf_counter()
+    res = S.SymbolicRegressor(cfg).fit(eng, d, [I.FLOAT])
+    t_fit = time.perf_counter() - t0
+    d.release()
+    return {"workload": "scalar: y=2.5x^2-1.2, 400 points; 1024 programs scored, then GP search to MSE<1e-7",
+            "population_mse_ms": t_pop * 1e3, "generations": res.generations, "seconds": t_fit,
+            "mse": res.mse, "reached_target": bool(res.mse <= 1e-7), "equation": res.equation}
+
+
 def run_engine(args):
     rank, world, local = rank_info()
     dist = None
@@ -364,6 +389,9 @@ def run_engine(args):
     serving = None
     if not args.no_serving:
         serving = serving_bench(eng, args.serving_jobs, args.serving_rate, slots=8)
+    search = None
+    if world == 1 and not args.no_search:
+        search = search_bench(eng)
 
     line = None
     if rank == 0:
@@ -406,6 +434,7 @@ def run_engine(args):
             "programs_on_register_kernel": desc["register_kernel_programs"],
             "programs_on_slot_kernel": desc["slot_kernel_programs"],
             "serving": serving,
+            "search": search,
         }
         print(json.dumps(line), flush=True)
     eng2.close()
@@ -424,6 +453,7 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-mix leg")
+    ap.add_argument("--no-search", action="store_true", help="skip the GP-search leg (config C1)")
     ap.add_argument("--serving-jobs", type=int, default=400)
     ap.add_argument("--serving-rate", type=float, default=2000.0)
     args = ap.parse_args()

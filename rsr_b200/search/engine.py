@@ -511,7 +511,12 @@ class SymbolicRegressor:
         cfg = self.config
         train = engine.subset(dataset, cfg.subset_size) if cfg.subset_size else dataset
         mini = engine.subset(train, cfg.mini_batch_size)
-        search = SearchEngine(cfg, variable_registry(feature_types), EngineBackend(engine, train, mini))
-        best = search.run()
-        full = float(engine.compute_mse_batch(I.pack([best.compile()]), dataset)[0])
+        try:
+            search = SearchEngine(cfg, variable_registry(feature_types), EngineBackend(engine, train, mini))
+            best = search.run()
+            full = float(engine.compute_mse_batch(I.pack([best.compile()]), dataset)[0])
+        finally:
+            mini.release()
+            if train is not dataset:
+                train.release()
         return FitResult(str(best), full, best.complexity(), search.generations)
