@@ -355,9 +355,13 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                 g.P >>= 1;
         // points per thread of slot-file kernels: largest that fits the smem budget
         if (g.kind != 1) {
-            // adjoint: two points per lane while eight warps' tapes still fit
-            // an SM; the tape's shared memory bounds the adjoint's occupancy
-            const size_t budget = g.kind == 2 ? 27 * 1024 : 110 * 1024;
+            // adjoint: the most points per lane (4, 2, 1) whose tape stays
+            // within 40 KB per warp.  More points per lane amortise the
+            // dispatch over more work at the cost of fewer resident tapes per
+            // SM; 40 KB measured best (gradient of 256 programs x 1M points,
+            // matrix workload: 28.9 ms against 33.2 ms at 27 KB and 43 ms at
+            // 14 KB; 4096 x 100k vector workload: 48.4 ms against 50.6 ms)
+            const size_t budget = g.kind == 2 ? 40 * 1024 : 110 * 1024;
             int Pp = 4;
             while (Pp > 1) {
                 size_t per = g.kind == 2 ? grad_smem_per_warp(g.code_words, g.const_floats, g.slots, g.adj_slots, Pp)
