@@ -115,7 +115,13 @@ void TaskPool::run(uint32_t n, const std::function<void(uint32_t)> &f) {
     done_cv_.wait(lk, [&] { return finished_ == threads_.size(); });
 }
 
-static constexpr int kRegPathStride = 8;          // register path = profile + 8 * spill-depth class
+static constexpr int kRegPathStride = 8;
+// Tape shared memory per warp that the adjoint's points per lane aim for.
+// More points per lane amortise the dispatch over more work at the cost of
+// fewer resident tapes per SM.  Gradient of 256 programs x 1M points (matrix
+// workload): 28.8 ms at 40 KB against 33.2 ms at 27 KB and 43 ms at 14 KB;
+// 4096 x 100k (vector workload): 51.4 ms.
+static constexpr size_t kGradTapeBudget = 40 * 1024;          // register path = profile + 8 * spill-depth class
 static constexpr uint64_t kChunkPoints = 4096;   // points per work-item chunk (all P)
 static constexpr uint64_t kStrideAlign = 1024;   // dataset column padding
 static constexpr int kGradSlotDoubles = 33;      // sse + 32 gradient sums
@@ -222,8 +228,15 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             // follows its own programs' tapes: <= 32, 64, 128, 256, more slots
             const uint32_t nt = enc[i].n_tape_val + enc[i].n_tape_adj;
             const int bucket = nt <= 32 ? 0 : nt <= 64 ? 1 : nt <= 128 ? 2 : nt <= 256 ? 3 : 4;
-            // one launch per (tape-size bucket, kernel profile)
-            path[i] = -2 - (bucket * N_PROFILES + enc[i].tape_profile);
+            // Points per lane: the most (4, 2, 1) whose tape fits
+            // kGradTapeBudget, decided from the program alone, so that its
+            // sums do not depend on the other programs of the call.
+            int lp = 2;
+            while (lp > 0 && grad_smem_per_warp((uint32_t)enc[i].tape_code.size() + 1, (uint32_t)enc[i].consts.size(),
+                                                enc[i].n_tape_val, enc[i].n_tape_adj, 1 << lp) > kGradTapeBudget)
+                --lp;
+            // one launch per (tape-size bucket, points per lane, kernel profile)
+            path[i] = -2 - ((bucket * 3 + lp) * N_PROFILES + enc[i].tape_profile);
         }
         else if (kernel == RSR_KERNEL_PLAIN || enc[i].profile < 0) path[i] = -1;
         else {
@@ -323,6 +336,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             P.n_plain += end - li;
         } else {
             g.G = 1;
+            g.P = 1 << (((-2 - pth) / N_PROFILES) % 3);
         }
         // tile size and per-warp staging requirements
         uint32_t j = li;
@@ -353,22 +367,10 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         if (g.kind == 1)
             while (g.P > 2 && reg_smem_bytes(g.code_words, g.const_floats, g.stack_depth, g.P, g.G) > kRegSmemBudget)
                 g.P >>= 1;
-        // points per thread of slot-file kernels: largest that fits the smem budget
-        if (g.kind != 1) {
-            // adjoint: the most points per lane (4, 2, 1) whose tape stays
-            // within 40 KB per warp.  More points per lane amortise the
-            // dispatch over more work at the cost of fewer resident tapes per
-            // SM; 40 KB measured best (gradient of 256 programs x 1M points,
-            // matrix workload: 28.9 ms against 33.2 ms at 27 KB and 43 ms at
-            // 14 KB; 4096 x 100k vector workload: 48.4 ms against 50.6 ms)
-            const size_t budget = g.kind == 2 ? 40 * 1024 : 110 * 1024;
+        // points per thread of the slot-file kernel: largest that fits the smem budget
+        if (g.kind == 0) {
             int Pp = 4;
-            while (Pp > 1) {
-                size_t per = g.kind == 2 ? grad_smem_per_warp(g.code_words, g.const_floats, g.slots, g.adj_slots, Pp)
-                                         : plain_smem_per_warp(g.code_words, g.const_floats, g.slots, Pp);
-                if (per <= budget) break;
-                Pp >>= 1;
-            }
+            while (Pp > 1 && plain_smem_per_warp(g.code_words, g.const_floats, g.slots, Pp) > 110 * 1024) Pp >>= 1;
             g.P = Pp;
         }
         // Expand each item into chunks of kChunkPoints and order them longest
