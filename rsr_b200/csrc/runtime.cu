@@ -115,13 +115,14 @@ void TaskPool::run(uint32_t n, const std::function<void(uint32_t)> &f) {
     done_cv_.wait(lk, [&] { return finished_ == threads_.size(); });
 }
 
+// register path = profile + 8 * (spill-depth class + 3 * no-unary flag)
 static constexpr int kRegPathStride = 8;
 // Tape shared memory per warp that the adjoint's points per lane aim for.
 // More points per lane amortise the dispatch over more work at the cost of
 // fewer resident tapes per SM.  Gradient of 256 programs x 1M points (matrix
 // workload): 28.8 ms at 40 KB against 33.2 ms at 27 KB and 43 ms at 14 KB;
 // 4096 x 100k (vector workload): 51.4 ms.
-static constexpr size_t kGradTapeBudget = 40 * 1024;          // register path = profile + 8 * spill-depth class
+static constexpr size_t kGradTapeBudget = 40 * 1024;
 static constexpr uint64_t kChunkPoints = 4096;   // points per work-item chunk (all P)
 static constexpr uint64_t kStrideAlign = 1024;   // dataset column padding
 static constexpr int kGradSlotDoubles = 33;      // sse + 32 gradient sums
@@ -254,7 +255,15 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                 uint32_t dmax = 0;
                 for (int t = 0; t < N_STACKS; ++t) dmax = std::max(dmax, depth[t]);
                 const int cls = dmax <= 1 ? 0 : dmax <= 2 ? 1 : 2;
-                path[i] = enc[i].profile + kRegPathStride * cls;
+                // and apart, programs without a unary Float op, whose kernel
+                // is built without those handlers (a smaller kernel: fewer
+                // instruction-cache misses)
+                bool nu = reg_has_no_unary(enc[i].profile);
+                for (uint32_t w : enc[i].reg_code) {
+                    const uint32_t kind = w & 0xFFu;
+                    if (kind >= (uint32_t)K_F_UN && kind < (uint32_t)K_F_END) nu = false;
+                }
+                path[i] = enc[i].profile + kRegPathStride * (cls + 3 * (nu ? 1 : 0));
             }
         }
         // programs the register kernel cannot take run on the slot-file kernel
@@ -321,6 +330,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         Group g;
         g.kind = pth <= -2 ? 2 : pth == -1 ? 0 : 1;
         g.profile = pth >= 0 ? pth % kRegPathStride : pth <= -2 ? (-2 - pth) % N_PROFILES : -1;
+        g.no_unary = pth >= 3 * kRegPathStride;
         g.item_begin = (uint32_t)P.items.size();
         if (g.kind == 1) {
             // P and G are per profile and dataset size; one launch uses one P,
@@ -530,12 +540,12 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             reg_layout(g.code_words, g.const_floats, g.stack_depth, g.P, g.G, a.stack_off, &a.acc_off, &a.region_floats,
                        &a.block_hdr_floats);
             const size_t smem = ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (kRegThreads / 32)) * 4u;
-            int bps = std::max(1, reg_max_blocks_per_sm(g.profile, g.P, smem));
+            int bps = std::max(1, reg_max_blocks_per_sm(g.profile, g.P, g.no_unary, smem));
             uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)bps * ctx->num_sms, g.n_items);
             g.grid = std::max(1u, grid);
             g.smem = smem;
             g.warps_per_block = kRegThreads / 32;
-            e = launch_reg(a, g.profile, g.P, g.grid, gs);
+            e = launch_reg(a, g.profile, g.P, g.no_unary, g.grid, gs);
         } else {
             const size_t per = grad_smem_per_warp(g.code_words, g.const_floats, g.slots, g.adj_slots, g.P);
             a.smem_adj_slots = g.adj_slots;

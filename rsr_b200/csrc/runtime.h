@@ -101,6 +101,7 @@ struct TuneChoice {
 struct Group {
     int kind = 0;        // 0 plain, 1 register, 2 adjoint
     int profile = -1;
+    bool no_unary = false;  // register kernel: no unary Float op in the launch's programs
     int P = 4;
     int G = 1;
     uint32_t item_begin = 0, n_items = 0;  // into the plan's item array
