@@ -233,6 +233,28 @@ def test_cma_es_matches_sequential_restatement():
 
 
 @pytest.mark.gpu
+def test_cma_es_per_program_datasets_match_restatement():
+    """Programs fitted against different resident datasets in one call take
+    the steps of the restatement run on each program's own dataset."""
+    from rsr_b200.evaluator import Engine
+    progs, _ = _cma_population()
+    sets = [W.inverse_dataset(n, seed=90 + k) for k, n in enumerate((300, 1700, 5000))]
+    with Engine() as eng:
+        dev = [eng.upload(ds) for ds in sets]
+        which = [0, 2, 1, 2]
+        params, mse, _ = eng.fit_cma_es(progs, datasets=[dev[k] for k in which], max_iterations=4, seed=77)
+        pk = I.pack(progs)
+        for i, p in enumerate(progs):
+            q = I.Program(list(p.code), [I.Scalar(c.kind, c.values) for c in p.constants])
+            d = dev[which[i]]
+            x, m, _ = OC.run_cma_es(q, sets[which[i]], 4, seed=77, index=i,
+                                    mse_fn=lambda pr: eng.compute_mse(pr, d))
+            got = params[pk.param_off[i]:pk.param_off[i + 1]]
+            np.testing.assert_array_equal(got, x[:len(got)], err_msg=f"program {i}")
+            assert f32(mse[i]) == f32(m), i
+
+
+@pytest.mark.gpu
 def test_cma_es_quadratic(engine):
     prog, ds = _quadratic()
     m0 = B.mse_ref32(prog, ds)
