@@ -34,7 +34,9 @@ constexpr size_t kRegSmemBudget = 200 * 1024;  // at least one block per SM, bel
 int reg_max_blocks_per_sm(int profile, int P, bool no_unary, size_t smem);
 
 // adjoint kernel (kernels_grad.cu)
-cudaError_t launch_grad(const LaunchArgs &a, int profile, uint32_t warps_per_block, size_t smem, cudaStream_t st);
+cudaError_t launch_grad(const LaunchArgs &a, int profile, bool no_unary, uint32_t warps_per_block, size_t smem,
+                        cudaStream_t st);
+bool grad_has_no_unary(int profile);
 size_t grad_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t val_slots, uint32_t adj_slots,
                           int P);
 cudaError_t launch_finalize_grad(const ProgDesc *progs, const DatasetDesc *ds, const double *partials, uint32_t n,

@@ -72,9 +72,10 @@ __device__ __forceinline__ void fwd_scale(const TapeCtx<P> &t, uint32_t o, uint3
 }
 
 // Forward value of one tape instruction (same semantics as the slot kernel).
-template <int PROF, int P>
+template <int PROF, int P, bool NU>
 __device__ __forceinline__ void tape_forward(const TapeCtx<P> &t, const uint32_t *w) {
     RSR_PROFILE_TYPES(PROF)
+    constexpr bool HU = !NU;  // the launch has unary Float ops
     const uint32_t op = w[0] & 0xFFu, aux = (w[0] >> 8) & 0xFFFFFu;
     const uint32_t o = w[1] & 0xFFFFu, i0 = w[2] & 0xFFFFu, i1 = w[3] & 0xFFFFu, i2 = w[4] & 0xFFFFu;
     Vf<P> A[9], B[9], R[9];
@@ -100,12 +101,12 @@ __device__ __forceinline__ void tape_forward(const TapeCtx<P> &t, const uint32_t
         case SUB_F: t.SV(o, t.V(i0) - t.V(i1)); break;
         case MUL_F: t.SV(o, t.V(i0) * t.V(i1)); break;
         case DIV_F: t.SV(o, t.V(i0) / t.V(i1)); break;
-        case SIN_F: t.SV(o, vsin(t.V(i0))); break;
-        case COS_F: t.SV(o, vcos(t.V(i0))); break;
-        case EXP_F: t.SV(o, vexp(t.V(i0))); break;
-        case SQR_F: { Vf<P> a = t.V(i0); t.SV(o, a * a); break; }
-        case SQRT_F: t.SV(o, vsqrt(t.V(i0))); break;
-        case LN_F: t.SV(o, vlog(t.V(i0))); break;
+        case RSR_GATE(SIN_F, HU): t.SV(o, vsin(t.V(i0))); break;
+        case RSR_GATE(COS_F, HU): t.SV(o, vcos(t.V(i0))); break;
+        case RSR_GATE(EXP_F, HU): t.SV(o, vexp(t.V(i0))); break;
+        case RSR_GATE(SQR_F, HU): { Vf<P> a = t.V(i0); t.SV(o, a * a); break; }
+        case RSR_GATE(SQRT_F, HU): t.SV(o, vsqrt(t.V(i0))); break;
+        case RSR_GATE(LN_F, HU): t.SV(o, vlog(t.V(i0))); break;
         case MAKE_VEC2: A[0] = t.V(i0); A[1] = t.V(i1); Sn(o, A, 2); break;
         case MAKE_VEC3: A[0] = t.V(i0); A[1] = t.V(i1); A[2] = t.V(i2); Sn(o, A, 3); break;
         case RSR_GATE(GET_X_V2, HV2): case RSR_GATE(GET_X_V3, HV3): t.SV(o, t.V(i0)); break;
@@ -214,9 +215,10 @@ __device__ __forceinline__ void rev_mulmv(const TapeCtx<P> &t, uint32_t vo, uint
 
 // Reverse sweep of one tape instruction.  gacc: this lane's f32 gradient
 // contributions of the tile (summed over its P points).
-template <int PROF, int P>
+template <int PROF, int P, bool NU>
 __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t *w, float *gacc_lane) {
     RSR_PROFILE_TYPES(PROF)
+    constexpr bool HU = !NU;
     const uint32_t op = w[0] & 0xFFu, aux = (w[0] >> 8) & 0xFFFFFu, width = w[0] >> 28;
     const uint32_t vo = w[1] & 0xFFFFu, ao = w[1] >> 16;
     const uint32_t v0 = w[2] & 0xFFFFu, a0 = w[2] >> 16, v1 = w[3] & 0xFFFFu, a1 = w[3] >> 16;
@@ -249,12 +251,12 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t
             t.AddA(a1, -(q * t.V(vo)));
             break;
         }
-        case SIN_F: t.AddA(a0, t.A(ao) * vcos(t.V(v0))); break;
-        case COS_F: t.AddA(a0, t.A(ao) * (-vsin(t.V(v0)))); break;
-        case EXP_F: t.AddA(a0, t.A(ao) * t.V(vo)); break;
-        case SQR_F: t.AddA(a0, t.A(ao) * (splat<P>(2.0f) * t.V(v0))); break;
-        case SQRT_F: t.AddA(a0, t.A(ao) / (splat<P>(2.0f) * t.V(vo))); break;
-        case LN_F: t.AddA(a0, t.A(ao) / t.V(v0)); break;
+        case RSR_GATE(SIN_F, HU): t.AddA(a0, t.A(ao) * vcos(t.V(v0))); break;
+        case RSR_GATE(COS_F, HU): t.AddA(a0, t.A(ao) * (-vsin(t.V(v0)))); break;
+        case RSR_GATE(EXP_F, HU): t.AddA(a0, t.A(ao) * t.V(vo)); break;
+        case RSR_GATE(SQR_F, HU): t.AddA(a0, t.A(ao) * (splat<P>(2.0f) * t.V(v0))); break;
+        case RSR_GATE(SQRT_F, HU): t.AddA(a0, t.A(ao) / (splat<P>(2.0f) * t.V(vo))); break;
+        case RSR_GATE(LN_F, HU): t.AddA(a0, t.A(ao) / t.V(v0)); break;
         case MAKE_VEC2: t.AddA(a0, t.A(ao)); t.AddA(a1, t.A(ao + 1)); break;
         case MAKE_VEC3: t.AddA(a0, t.A(ao)); t.AddA(a1, t.A(ao + 1)); t.AddA(a2, t.A(ao + 2)); break;
         case RSR_GATE(GET_X_V2, HV2): case RSR_GATE(GET_X_V3, HV3): t.AddA(a0, t.A(ao)); break;
@@ -354,7 +356,9 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t
     for (uint32_t i = 0; i < width; ++i) t.adj[(ao + i) * 32 + t.lane] = splat<P>(0.0f);
 }
 
-template <int PROF, int P>
+// NU: no program of the launch has a unary Float op (sin, cos, exp, sqr,
+// sqrt, ln), so their forward and reverse handlers are left out.
+template <int PROF, int P, bool NU>
 __global__ void __launch_bounds__(kGradThreads, 16) grad_kernel(const LaunchArgs a) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -389,7 +393,7 @@ __global__ void __launch_bounds__(kGradThreads, 16) grad_kernel(const LaunchArgs
     Kahan sse;
     for (uint32_t tile = it.tile_begin; tile < it.tile_end; ++tile) {
         t.p0 = (uint64_t)tile * (32u * P) + (uint64_t)lane * P;
-        for (uint32_t i = 0; i < n_nodes; ++i) tape_forward<PROF, P>(t, code + 5 * i);
+        for (uint32_t i = 0; i < n_nodes; ++i) tape_forward<PROF, P, NU>(t, code + 5 * i);
         const Vf<P> pred = result == 0xFFFFFFFFu ? splat<P>(0.0f) : t.V(result);
         const Vf<P> y = load_pts<P>(ds.y + t.p0);
         Vf<P> seed;
@@ -403,7 +407,7 @@ __global__ void __launch_bounds__(kGradThreads, 16) grad_kernel(const LaunchArgs
         if (result == 0xFFFFFFFFu) continue;
         t.AddA(result_adj, seed);
         // reverse sweep; constant loads add their adjoints to gacc
-        for (uint32_t i = n_nodes; i-- > 0;) tape_reverse<PROF, P>(t, code + 5 * i, gacc + lane);
+        for (uint32_t i = n_nodes; i-- > 0;) tape_reverse<PROF, P, NU>(t, code + 5 * i, gacc + lane);
     }
     double *out = a.partials + (size_t)(pd.part_off + it.chunk) * (1 + kGradParams);
     const double s = warp_sum(sse.value());
@@ -435,28 +439,34 @@ __global__ void finalize_grad_kernel(const ProgDesc *progs, const DatasetDesc *d
     for (uint32_t k = 0; k < kGradParams; ++k) grad_out[(size_t)p * kGradParams + k] = (bad || k >= np) ? 0.0f : (float)(g[k] / n);
 }
 
-template <int PROF, int P>
+template <int PROF, int P, bool NU>
 static cudaError_t launch_grad_p(const LaunchArgs &a, uint32_t wpb, size_t smem, cudaStream_t st) {
-    auto k = grad_kernel<PROF, P>;
+    auto k = grad_kernel<PROF, P, NU>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin);
     if (e != cudaSuccess) return e;
     k<<<(a.n_items + wpb - 1) / wpb, wpb * 32, smem, st>>>(a);
     return cudaGetLastError();
 }
 
-template <int PROF>
+template <int PROF, bool NU>
 static cudaError_t launch_grad_prof(const LaunchArgs &a, uint32_t wpb, size_t smem, cudaStream_t st) {
-    return a.progs_per_warp >= 4 ? launch_grad_p<PROF, 4>(a, wpb, smem, st)
-         : a.progs_per_warp >= 2 ? launch_grad_p<PROF, 2>(a, wpb, smem, st) : launch_grad_p<PROF, 1>(a, wpb, smem, st);
+    return a.progs_per_warp >= 4 ? launch_grad_p<PROF, 4, NU>(a, wpb, smem, st)
+         : a.progs_per_warp >= 2 ? launch_grad_p<PROF, 2, NU>(a, wpb, smem, st)
+                                 : launch_grad_p<PROF, 1, NU>(a, wpb, smem, st);
 }
 
-cudaError_t launch_grad(const LaunchArgs &a, int profile, uint32_t wpb, size_t smem, cudaStream_t st) {
+// Kernels without the unary Float handlers exist for the F and F+V3 profiles.
+bool grad_has_no_unary(int profile) { return profile == P_F || profile == P_FV3; }
+
+cudaError_t launch_grad(const LaunchArgs &a, int profile, bool no_unary, uint32_t wpb, size_t smem, cudaStream_t st) {
     switch (profile) {
-        case P_F: return launch_grad_prof<P_F>(a, wpb, smem, st);
-        case P_FV3: return launch_grad_prof<P_FV3>(a, wpb, smem, st);
-        case P_FV2M2: return launch_grad_prof<P_FV2M2>(a, wpb, smem, st);
-        case P_FV3M3: return launch_grad_prof<P_FV3M3>(a, wpb, smem, st);
-        default: return launch_grad_prof<P_ALL>(a, wpb, smem, st);
+        case P_F: return no_unary ? launch_grad_prof<P_F, true>(a, wpb, smem, st)
+                                  : launch_grad_prof<P_F, false>(a, wpb, smem, st);
+        case P_FV3: return no_unary ? launch_grad_prof<P_FV3, true>(a, wpb, smem, st)
+                                    : launch_grad_prof<P_FV3, false>(a, wpb, smem, st);
+        case P_FV2M2: return launch_grad_prof<P_FV2M2, false>(a, wpb, smem, st);
+        case P_FV3M3: return launch_grad_prof<P_FV3M3, false>(a, wpb, smem, st);
+        default: return launch_grad_prof<P_ALL, false>(a, wpb, smem, st);
     }
 }
 

@@ -120,8 +120,7 @@ static constexpr int kRegPathStride = 8;
 // Tape shared memory per warp that the adjoint's points per lane aim for.
 // More points per lane amortise the dispatch over more work at the cost of
 // fewer resident tapes per SM.  Gradient of 256 programs x 1M points (matrix
-// workload): 28.8 ms at 40 KB against 33.2 ms at 27 KB and 43 ms at 14 KB;
-// 4096 x 100k (vector workload): 51.4 ms.
+// workload): 28.8 ms at 40 KB against 33.2 ms at 27 KB and 43 ms at 14 KB.
 static constexpr size_t kGradTapeBudget = 40 * 1024;
 static constexpr uint64_t kChunkPoints = 4096;   // points per work-item chunk (all P)
 static constexpr uint64_t kStrideAlign = 1024;   // dataset column padding
@@ -236,8 +235,17 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             while (lp > 0 && grad_smem_per_warp((uint32_t)enc[i].tape_code.size() + 1, (uint32_t)enc[i].consts.size(),
                                                 enc[i].n_tape_val, enc[i].n_tape_adj, 1 << lp) > kGradTapeBudget)
                 --lp;
-            // one launch per (tape-size bucket, points per lane, kernel profile)
-            path[i] = -2 - ((bucket * 3 + lp) * N_PROFILES + enc[i].tape_profile);
+            // programs without a unary Float op run on a kernel built without
+            // those handlers (F and F+V3 profiles)
+            bool nu = grad_has_no_unary(enc[i].tape_profile);
+            const std::vector<uint32_t> &tc = enc[i].tape_code;
+            for (size_t w = 2; w + 5 <= tc.size(); w += 5) {
+                const uint32_t op = tc[w] & 0xFFu;
+                if (op >= (uint32_t)SIN_F && op <= (uint32_t)LN_F) nu = false;
+            }
+            // one launch per (tape-size bucket, points per lane, no-unary
+            // flag, kernel profile)
+            path[i] = -2 - (((bucket * 3 + lp) * 2 + (nu ? 1 : 0)) * N_PROFILES + enc[i].tape_profile);
         }
         else if (kernel == RSR_KERNEL_PLAIN || enc[i].profile < 0) path[i] = -1;
         else {
@@ -330,7 +338,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         Group g;
         g.kind = pth <= -2 ? 2 : pth == -1 ? 0 : 1;
         g.profile = pth >= 0 ? pth % kRegPathStride : pth <= -2 ? (-2 - pth) % N_PROFILES : -1;
-        g.no_unary = pth >= 3 * kRegPathStride;
+        g.no_unary = pth >= 3 * kRegPathStride;  // register kernel; the adjoint's flag is set below
         g.item_begin = (uint32_t)P.items.size();
         if (g.kind == 1) {
             // P and G are per profile and dataset size; one launch uses one P,
@@ -346,7 +354,8 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             P.n_plain += end - li;
         } else {
             g.G = 1;
-            g.P = 1 << (((-2 - pth) / N_PROFILES) % 3);
+            g.no_unary = ((-2 - pth) / N_PROFILES) % 2 != 0;
+            g.P = 1 << (((-2 - pth) / (2 * N_PROFILES)) % 3);
         }
         // tile size and per-warp staging requirements
         uint32_t j = li;
@@ -556,7 +565,7 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             g.grid = (g.n_items + wpb - 1) / wpb;
             g.smem = per * wpb;
             g.warps_per_block = wpb;
-            e = launch_grad(a, g.profile, wpb, per * wpb, gs);
+            e = launch_grad(a, g.profile, g.no_unary, wpb, per * wpb, gs);
         }
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
         if (group_events) cudaEventRecord(group_events[2 * gi + 1], gs);
