@@ -288,6 +288,8 @@ __device__ __forceinline__ void run_program(Acc<PROF, P> &a, const AccIO<P> &io,
             switch (kind) { RSR_BLOCK_F_NU RSR_BLOCK_V3 default: break; }
         } else if constexpr (PROF == P_FV3) {
             switch (kind) { RSR_BLOCK_F RSR_BLOCK_V3 default: break; }
+        } else if constexpr (PROF == P_FV2M2 && NU) {
+            switch (kind) { RSR_BLOCK_F_NU RSR_BLOCK_V2 RSR_BLOCK_M2 default: break; }
         } else if constexpr (PROF == P_FV2M2) {
             switch (kind) { RSR_BLOCK_F RSR_BLOCK_V2 RSR_BLOCK_M2 default: break; }
         } else if constexpr (PROF == P_FV3M3) {
@@ -493,8 +495,9 @@ static cudaError_t launch_reg_pp(const LaunchArgs &a, uint32_t grid, cudaStream_
 // F+V2+M2 profiles, {2, 4} for the others.
 int reg_max_p(int profile) { return profile == P_F || profile == P_FV3 || profile == P_FV2M2 ? 8 : 4; }
 
-// Kernels without the unary Float handlers exist for the F and F+V3 profiles.
-bool reg_has_no_unary(int profile) { return profile == P_F || profile == P_FV3; }
+// Kernels without the unary Float handlers exist for the F, F+V3 and F+V2+M2
+// profiles.
+bool reg_has_no_unary(int profile) { return profile == P_F || profile == P_FV3 || profile == P_FV2M2; }
 
 template <int PROF, bool NU>
 static cudaError_t launch_reg_p3(const LaunchArgs &a, int P, uint32_t grid, cudaStream_t st) {
@@ -507,7 +510,8 @@ cudaError_t launch_reg(const LaunchArgs &a, int profile, int P, bool no_unary, u
         case P_F: return no_unary ? launch_reg_p3<P_F, true>(a, P, grid, st) : launch_reg_p3<P_F, false>(a, P, grid, st);
         case P_FV3: return no_unary ? launch_reg_p3<P_FV3, true>(a, P, grid, st)
                                     : launch_reg_p3<P_FV3, false>(a, P, grid, st);
-        case P_FV2M2: return launch_reg_p3<P_FV2M2, false>(a, P, grid, st);
+        case P_FV2M2: return no_unary ? launch_reg_p3<P_FV2M2, true>(a, P, grid, st)
+                                      : launch_reg_p3<P_FV2M2, false>(a, P, grid, st);
         case P_FV3M3: return P >= 4 ? launch_reg_pp<P_FV3M3, 4, false>(a, grid, st)
                                     : launch_reg_pp<P_FV3M3, 2, false>(a, grid, st);
         default: return P >= 4 ? launch_reg_pp<P_ALL, 4, false>(a, grid, st) : launch_reg_pp<P_ALL, 2, false>(a, grid, st);
@@ -534,7 +538,7 @@ int reg_max_blocks_per_sm(int profile, int P, bool no_unary, size_t smem) {
     switch (profile) {
         case P_F: return no_unary ? occ3<P_F, true>(P, smem) : occ3<P_F, false>(P, smem);
         case P_FV3: return no_unary ? occ3<P_FV3, true>(P, smem) : occ3<P_FV3, false>(P, smem);
-        case P_FV2M2: return occ3<P_FV2M2, false>(P, smem);
+        case P_FV2M2: return no_unary ? occ3<P_FV2M2, true>(P, smem) : occ3<P_FV2M2, false>(P, smem);
         case P_FV3M3: return P >= 4 ? occ<P_FV3M3, 4, false>(smem) : occ<P_FV3M3, 2, false>(smem);
         default: return P >= 4 ? occ<P_ALL, 4, false>(smem) : occ<P_ALL, 2, false>(smem);
     }
