@@ -1125,6 +1125,7 @@ int rsr_batch_describe(rsr_ctx *ctx, rsr_batch *b, char *buf, size_t len) {
         const Group &g = b->plan.groups[i];
         const char *kn = g.kind == 0 ? "slot" : g.kind == 1 ? "register" : "adjoint";
         s += (i ? ", " : "") + std::string("{\"kernel\": \"") + kn + "\", \"profile\": " + std::to_string(g.profile) +
+             ", \"no_unary\": " + (g.no_unary ? "true" : "false") +
              ", \"points_per_thread\": " + std::to_string(g.P) + ", \"programs_per_warp\": " + std::to_string(g.G) +
              ", \"items\": " + std::to_string(g.n_items) + ", \"flops\": " + std::to_string(g.flops) +
              ", \"program_points\": " + std::to_string(g.program_points) + ", \"grid\": " + std::to_string(g.grid) +

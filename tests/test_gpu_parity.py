@@ -238,8 +238,35 @@ def test_prepared_batch_graph_replay(engine):
         assert t_ms > 0
         d = b.describe()
         assert d["programs"] == len(pop) and d["register_kernel_programs"] + d["slot_kernel_programs"] == len(pop)
+        # the vector workload uses no unary Float op: its register launches
+        # run on the instances built without those handlers
+        assert all(g["no_unary"] for g in d["groups"] if g["kernel"] == "register")
     finally:
         b.close()
+
+
+def test_unary_and_plain_programs_split_and_agree(engine):
+    """A scalar population mixes programs with and without sin/cos/exp:
+    they launch on different kernel instances, and every result matches the
+    FP64 oracle as in the single-kind calls."""
+    ds, pop = W.scalar_dataset(1000, seed=21), W.scalar_population(600, seed=22)
+    uses = [any(I.OP_NAMES[w & 0xFF] in ("SinF", "CosF", "ExpF") for w in p.code) for p in pop]
+    assert 0 < sum(uses) < len(pop)
+    b = engine.prepare(pop, ds)
+    try:
+        b.run()
+        got = b.results()
+        flags = {g["no_unary"] for g in b.describe()["groups"] if g["kernel"] == "register"}
+        assert flags == {True, False}
+    finally:
+        b.close()
+    m64, _ = O.mse_batch(I.pack(pop), ds)
+    fin = np.isfinite(m64) & (m64 < 1e30)
+    np.testing.assert_allclose(got[fin], m64[fin], rtol=1e-6)
+    alone = np.concatenate([engine.compute_mse_batch([p for p, u in zip(pop, uses) if u], ds),
+                            engine.compute_mse_batch([p for p, u in zip(pop, uses) if not u], ds)])
+    order = [i for i, u in enumerate(uses) if u] + [i for i, u in enumerate(uses) if not u]
+    np.testing.assert_array_equal(alone, got[order])
 
 
 def test_dataset_handles(engine):
