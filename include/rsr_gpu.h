@@ -225,7 +225,13 @@ typedef struct rsr_server_options {
 typedef enum rsr_job_kind {
     RSR_JOB_MSE = 0,       /* mse_out[n] */
     RSR_JOB_MSE_GRAD = 1,  /* mse_out[n], grad_out[n*32] */
-    RSR_JOB_FIT = 2        /* rsr_fit_lbfgs: params_out (pop->params layout), mse_out[n] */
+    RSR_JOB_FIT = 2,       /* rsr_fit_lbfgs: params_out (pop->params layout), mse_out[n] */
+    /* optimize_individual_constants (src/engine/optimize/mod.rs:10-59) per
+     * program: L-BFGS (15 iterations) for differentiable programs, CMA-ES
+     * (max(fit_iterations / 16, 2) generations, streams from `seed`) for the
+     * others with a vector or matrix constant, Nelder-Mead (fit_iterations)
+     * otherwise; params_out and mse_out as RSR_JOB_FIT */
+    RSR_JOB_FIT_AUTO = 3
 } rsr_job_kind;
 
 typedef struct rsr_job {
@@ -237,6 +243,7 @@ typedef struct rsr_job {
     float *mse_out;                      /* written when the job completes; */
     float *grad_out;                     /* the caller keeps these valid until */
     float *params_out;                   /* rsr_wait returns or the job is cancelled */
+    uint64_t seed;                       /* RSR_JOB_FIT_AUTO: CMA-ES random streams */
 } rsr_job;
 
 typedef enum rsr_job_state { RSR_JOB_QUEUED = 0, RSR_JOB_RUNNING = 1, RSR_JOB_DONE = 2 } rsr_job_state;

@@ -47,7 +47,7 @@ class FitStats(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("gradient_evaluations", C.c_uint32), ("mse_evaluations", C.c_uint32)]
 
 
-JOB_MSE, JOB_MSE_GRAD, JOB_FIT = 0, 1, 2
+JOB_MSE, JOB_MSE_GRAD, JOB_FIT, JOB_FIT_AUTO = 0, 1, 2, 3
 JOB_QUEUED, JOB_RUNNING, JOB_DONE = 0, 1, 2
 
 
@@ -59,7 +59,7 @@ class ServerOptions(C.Structure):
 class Job(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("fit_iterations", C.c_uint32), ("pop", C.POINTER(Population)),
                 ("ds", C.c_uint64), ("ds_per_program", C.POINTER(C.c_uint64)), ("mse_out", C.POINTER(C.c_float)),
-                ("grad_out", C.POINTER(C.c_float)), ("params_out", C.POINTER(C.c_float))]
+                ("grad_out", C.POINTER(C.c_float)), ("params_out", C.POINTER(C.c_float)), ("seed", C.c_uint64)]
 
 
 class JobInfo(C.Structure):

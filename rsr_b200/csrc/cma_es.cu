@@ -72,7 +72,8 @@ struct CmState {
 }  // namespace
 
 int fit_cma_es(rsr_ctx *ctx, const rsr_population *pop, const uint64_t *dsp, uint64_t ds, uint32_t max_iterations,
-               uint64_t seed, cudaStream_t stream, float *params_out, float *mse_out, rsr_fit_stats *stats) {
+               uint64_t seed, cudaStream_t stream, std::mutex *plan_mu, const std::atomic<bool> *cancel,
+               float *params_out, float *mse_out, rsr_fit_stats *stats) {
     NvtxRange nvtx_range("rsr: CMA-ES fit");
     const uint32_t N = pop->n_programs;
     rsr_fit_stats local{};
@@ -102,7 +103,7 @@ int fit_cma_es(rsr_ctx *ctx, const rsr_population *pop, const uint64_t *dsp, uin
     fit::Evaluator ev;
     ev.dev = &ws.mse;
     ev.active = &ws.mse_active;
-    int rc = fit::prepare(ctx, rep, dsp ? rdsp.data() : nullptr, ds, false, stream, nullptr, &ev);
+    int rc = fit::prepare(ctx, rep, dsp ? rdsp.data() : nullptr, ds, false, stream, plan_mu, &ev);
     if (rc) return rc;
 
     // weights and effective selection mass (cmaes.rs:80-94); the two
@@ -165,6 +166,7 @@ int fit_cma_es(rsr_ctx *ctx, const rsr_population *pop, const uint64_t *dsp, uin
 
     std::vector<std::pair<float, int>> order(kLambda);
     for (uint32_t it = 0; it < max_iterations; ++it) {
+        if (cancel && cancel->load()) return fail(RSR_ECANCELED, "fit cancelled");
         // sample (cmaes.rs:119-135)
         bool any = false;
         for (uint32_t i = 0; i < N; ++i) {
@@ -255,5 +257,6 @@ extern "C" int rsr_fit_cma_es(rsr_ctx *ctx, const rsr_population *pop, rsr_datas
     if (!ctx || !pop || !params_out || !mse_out) return fail(RSR_EINVAL, "null argument");
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaSetDevice(ctx->device);
-    return fit_cma_es(ctx, pop, dsp, ds, max_iterations, seed, ctx->stream, params_out, mse_out, stats);
+    return fit_cma_es(ctx, pop, dsp, ds, max_iterations, seed, ctx->stream, nullptr, nullptr, params_out, mse_out,
+                      stats);
 }

@@ -67,8 +67,8 @@ void sort_simplex(NmState &s) {
 }  // namespace
 
 int fit_nelder_mead(rsr_ctx *ctx, const rsr_population *pop, const uint64_t *dsp, uint64_t ds,
-                    uint32_t max_iterations, cudaStream_t stream, float *params_out, float *mse_out,
-                    rsr_fit_stats *stats) {
+                    uint32_t max_iterations, cudaStream_t stream, std::mutex *plan_mu,
+                    const std::atomic<bool> *cancel, float *params_out, float *mse_out, rsr_fit_stats *stats) {
     NvtxRange nvtx_range("rsr: Nelder-Mead fit");
     const uint32_t N = pop->n_programs;
     rsr_fit_stats local{};
@@ -80,7 +80,7 @@ int fit_nelder_mead(rsr_ctx *ctx, const rsr_population *pop, const uint64_t *dsp
     fit::Evaluator ev;
     ev.dev = &ws.mse;
     ev.active = &ws.mse_active;
-    int rc = fit::prepare(ctx, *pop, dsp, ds, false, stream, nullptr, &ev);
+    int rc = fit::prepare(ctx, *pop, dsp, ds, false, stream, plan_mu, &ev);
     if (rc) return rc;
 
     // Float constants of each program and their flat offsets (nelder_mead.rs:22-31)
@@ -149,6 +149,7 @@ int fit_nelder_mead(rsr_ctx *ctx, const rsr_population *pop, const uint64_t *dsp
     }
 
     for (uint32_t iter = 0; iter < max_iterations; ++iter) {
+        if (cancel && cancel->load()) return fail(RSR_ECANCELED, "fit cancelled");
         // sort, stop test, centroid, reflection (nelder_mead.rs:69-97)
         bool any = false;
         for (uint32_t i = 0; i < N; ++i) {
@@ -278,5 +279,6 @@ extern "C" int rsr_fit_nelder_mead(rsr_ctx *ctx, const rsr_population *pop, rsr_
     if (!ctx || !pop || !params_out || !mse_out) return fail(RSR_EINVAL, "null argument");
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaSetDevice(ctx->device);
-    return fit_nelder_mead(ctx, pop, dsp, ds, max_iterations, ctx->stream, params_out, mse_out, stats);
+    return fit_nelder_mead(ctx, pop, dsp, ds, max_iterations, ctx->stream, nullptr, nullptr, params_out, mse_out,
+                           stats);
 }

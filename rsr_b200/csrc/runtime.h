@@ -245,6 +245,14 @@ int fit_population(rsr_ctx *ctx, const rsr_population *pop, const uint64_t *dsp,
                    uint32_t max_iterations, cudaStream_t stream, std::mutex *plan_mu,
                    const std::atomic<bool> *cancel, FitWorkspace *ws, float *params_out, float *mse_out,
                    rsr_fit_stats *stats);
+// Batched Nelder-Mead and CMA-ES (nelder_mead.cu, cma_es.cu); plan_mu and
+// cancel as for fit_population.
+int fit_nelder_mead(rsr_ctx *ctx, const rsr_population *pop, const uint64_t *dsp, uint64_t ds,
+                    uint32_t max_iterations, cudaStream_t stream, std::mutex *plan_mu,
+                    const std::atomic<bool> *cancel, float *params_out, float *mse_out, rsr_fit_stats *stats);
+int fit_cma_es(rsr_ctx *ctx, const rsr_population *pop, const uint64_t *dsp, uint64_t ds, uint32_t max_iterations,
+               uint64_t seed, cudaStream_t stream, std::mutex *plan_mu, const std::atomic<bool> *cancel,
+               float *params_out, float *mse_out, rsr_fit_stats *stats);
 // group_events: optional, 2 per group (before/after its kernel); not used
 // while capturing a graph.
 int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st, cudaEvent_t ev_mid,

@@ -52,6 +52,7 @@ struct Job {
     std::vector<uint64_t> dsp;      // dataset per program
     std::vector<uint64_t> handles;  // distinct datasets, referenced while the job lives
     float *mse_out = nullptr, *grad_out = nullptr, *params_out = nullptr;
+    uint64_t seed = 0;  // RSR_JOB_FIT_AUTO: CMA-ES streams
     uint64_t est_bytes = 0, program_points = 0;
     std::atomic<bool> cancel{false};
     uint32_t state = RSR_JOB_QUEUED;
@@ -94,6 +95,24 @@ struct Slot {
     }
 };
 
+// The optimiser optimize_individual_constants (src/engine/optimize/mod.rs:
+// 24-58) picks for a program: L-BFGS when every opcode is differentiable
+// (all but the inverses), else CMA-ES when a constant is a vector or matrix,
+// else Nelder-Mead.
+enum FitMethod { FIT_LBFGS = 0, FIT_CMAES = 1, FIT_NM = 2 };
+
+int fit_method(const Job &j, uint32_t i) {
+    for (uint64_t k = j.code_off[i]; k < j.code_off[i + 1]; ++k) {
+        const uint32_t op = j.code[k] & 0xFFu;
+        if (op == INVERSE_M2 || op == INVERSE_M3) {
+            for (uint64_t c = j.kind_off[i]; c < j.kind_off[i + 1]; ++c)
+                if (j.kinds[c] >= 3) return FIT_CMAES;  // Vec2, Vec3, Mat2, Mat3
+            return FIT_NM;
+        }
+    }
+    return FIT_LBFGS;
+}
+
 // Device bytes one job's launch(es) hold: plan pool, partial sums, outputs.
 uint64_t estimate_bytes(const Job &j, const std::vector<uint64_t> &n_eval_per_prog) {
     const bool grad = j.kind != RSR_JOB_MSE;
@@ -103,7 +122,10 @@ uint64_t estimate_bytes(const Job &j, const std::vector<uint64_t> &n_eval_per_pr
         const uint64_t np = j.param_off[i + 1] - j.param_off[i];
         const uint64_t parts = std::max<uint64_t>(1, (n_eval_per_prog[i] + 4095) / 4096);
         uint64_t per = 64 + 16 * (len + 1) + 4 * (np + 1) + 24 * parts + 8 * parts * (grad ? 33 : 1) + 4 * 33;
-        if (j.kind == RSR_JOB_FIT) per += 64 + 16 * (len + 1) + 4 * (np + 1) + 24 * parts + 8 * parts + 8;
+        if (j.kind == RSR_JOB_FIT || j.kind == RSR_JOB_FIT_AUTO)
+            per += 64 + 16 * (len + 1) + 4 * (np + 1) + 24 * parts + 8 * parts + 8;
+        // CMA-ES plans 16 copies of the program
+        if (j.kind == RSR_JOB_FIT_AUTO && fit_method(j, i) == FIT_CMAES) per *= 16;
         b += per;
     }
     return b;
@@ -207,6 +229,57 @@ int run_eval(rsr_server *S, Slot &slot, const std::vector<JobPtr> &batch) {
     return RSR_OK;
 }
 
+// An RSR_JOB_FIT_AUTO job: the programs split by the optimiser the reference
+// would pick for them (fit_method), each group fitted by its batched driver
+// on this slot's stream, results scattered back in the job's order.
+int fit_auto(rsr_server *S, Slot &slot, Job &j) {
+    NvtxRange nvtx_range("rsr: serving fit (auto)");
+    const uint32_t n = j.n();
+    struct Sub {
+        std::vector<uint32_t> idx, code;
+        std::vector<uint8_t> kinds;
+        std::vector<float> params, out_params, out_mse;
+        std::vector<uint64_t> code_off{0}, kind_off{0}, param_off{0}, dsp;
+    } sub[3];
+    for (uint32_t i = 0; i < n; ++i) {
+        Sub &g = sub[fit_method(j, i)];
+        g.idx.push_back(i);
+        g.code.insert(g.code.end(), j.code.begin() + j.code_off[i], j.code.begin() + j.code_off[i + 1]);
+        g.kinds.insert(g.kinds.end(), j.kinds.begin() + j.kind_off[i], j.kinds.begin() + j.kind_off[i + 1]);
+        g.params.insert(g.params.end(), j.params.begin() + j.param_off[i], j.params.begin() + j.param_off[i + 1]);
+        g.code_off.push_back(g.code.size());
+        g.kind_off.push_back(g.kinds.size());
+        g.param_off.push_back(g.params.size());
+        g.dsp.push_back(j.dsp[i]);
+    }
+    for (int m = 0; m < 3; ++m) {
+        Sub &g = sub[m];
+        if (g.idx.empty()) continue;
+        const rsr_population pop{(uint32_t)g.idx.size(), g.code.data(), g.code_off.data(), g.kinds.data(),
+                                 g.kind_off.data(), g.params.data(), g.param_off.data()};
+        g.out_params.assign(std::max<size_t>(g.params.size(), 1), 0.0f);
+        g.out_mse.assign(g.idx.size(), 0.0f);
+        int rc;
+        if (m == FIT_LBFGS)  // optimize/mod.rs:50-52: 15 iterations whatever the budget
+            rc = fit_population(S->ctx, &pop, g.dsp.data(), 0, 15, slot.st, &S->ctx->mu, &j.cancel, &slot.fit,
+                                g.out_params.data(), g.out_mse.data(), nullptr);
+        else if (m == FIT_CMAES)  // optimize/mod.rs:53-55
+            rc = fit_cma_es(S->ctx, &pop, g.dsp.data(), 0, std::max(j.fit_iterations / 16, 2u), j.seed, slot.st,
+                            &S->ctx->mu, &j.cancel, g.out_params.data(), g.out_mse.data(), nullptr);
+        else  // optimize/mod.rs:56-57
+            rc = fit_nelder_mead(S->ctx, &pop, g.dsp.data(), 0, j.fit_iterations, slot.st, &S->ctx->mu, &j.cancel,
+                                 g.out_params.data(), g.out_mse.data(), nullptr);
+        if (rc) return rc;
+        for (size_t k = 0; k < g.idx.size(); ++k) {
+            const uint32_t i = g.idx[k];
+            j.mse_out[i] = g.out_mse[k];
+            std::copy(g.out_params.begin() + g.param_off[k], g.out_params.begin() + g.param_off[k + 1],
+                      j.params_out + j.param_off[i]);
+        }
+    }
+    return RSR_OK;
+}
+
 void finish(rsr_server *S, const std::vector<JobPtr> &batch, const std::vector<int> &status,
             const std::vector<std::string> &msgs, uint64_t need) {
     const auto now = Clock::now();
@@ -249,7 +322,7 @@ void worker_main(rsr_server *S, Slot *slot) {
             S->queue.pop_front();
             batch.push_back(head);
             need = head->est_bytes;
-            if (head->kind != RSR_JOB_FIT) {
+            if (head->kind != RSR_JOB_FIT && head->kind != RSR_JOB_FIT_AUTO) {
                 uint64_t progs = head->n();
                 while (!S->queue.empty()) {
                     const JobPtr &j = S->queue.front();
@@ -276,7 +349,16 @@ void worker_main(rsr_server *S, Slot *slot) {
         }
         std::vector<int> status(batch.size(), RSR_OK);
         std::vector<std::string> msgs(batch.size());
-        if (batch[0]->kind == RSR_JOB_FIT) {
+        if (batch[0]->kind == RSR_JOB_FIT_AUTO) {
+            Job &j = *batch[0];
+            if (j.cancel.load()) {
+                status[0] = RSR_ECANCELED;
+                msgs[0] = "cancelled";
+            } else {
+                status[0] = fit_auto(S, *slot, j);
+                if (status[0]) msgs[0] = thread_error();
+            }
+        } else if (batch[0]->kind == RSR_JOB_FIT) {
             Job &j = *batch[0];
             if (j.cancel.load()) {
                 status[0] = RSR_ECANCELED;
@@ -394,11 +476,12 @@ int rsr_server_destroy(rsr_server *S) {
 int rsr_submit(rsr_server *S, const rsr_job *job, uint64_t *ticket) {
     if (!S || !job || !ticket || !job->pop) return fail(RSR_EINVAL, "null argument");
     const rsr_population &p = *job->pop;
-    if (job->kind > RSR_JOB_FIT) return fail(RSR_EINVAL, "unknown job kind");
+    if (job->kind > RSR_JOB_FIT_AUTO) return fail(RSR_EINVAL, "unknown job kind");
     if (p.n_programs && (!p.code_off || !p.kind_off || !p.param_off)) return fail(RSR_EINVAL, "null population array");
     if (p.n_programs && !job->mse_out) return fail(RSR_EINVAL, "mse_out is null");
     if (job->kind == RSR_JOB_MSE_GRAD && p.n_programs && !job->grad_out) return fail(RSR_EINVAL, "grad_out is null");
-    if (job->kind == RSR_JOB_FIT && p.n_programs && !job->params_out) return fail(RSR_EINVAL, "params_out is null");
+    if ((job->kind == RSR_JOB_FIT || job->kind == RSR_JOB_FIT_AUTO) && p.n_programs && !job->params_out)
+        return fail(RSR_EINVAL, "params_out is null");
     auto j = std::make_shared<Job>();
     j->kind = job->kind;
     j->fit_iterations = job->fit_iterations;
@@ -424,6 +507,7 @@ int rsr_submit(rsr_server *S, const rsr_job *job, uint64_t *ticket) {
     j->mse_out = job->mse_out;
     j->grad_out = job->grad_out;
     j->params_out = job->params_out;
+    j->seed = job->seed;
     // datasets: resolve, size the job, and hold a reference until it is done
     std::vector<uint64_t> n_eval(n, 0);
     {

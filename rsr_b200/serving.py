@@ -18,7 +18,7 @@ import numpy as np
 from . import _native as N
 from .evaluator import Engine, PopulationLike, _as_population, _packed
 
-KINDS = {"mse": N.JOB_MSE, "grad": N.JOB_MSE_GRAD, "fit": N.JOB_FIT}
+KINDS = {"mse": N.JOB_MSE, "grad": N.JOB_MSE_GRAD, "fit": N.JOB_FIT, "fit_auto": N.JOB_FIT_AUTO}
 STATES = {N.JOB_QUEUED: "queued", N.JOB_RUNNING: "running", N.JOB_DONE: "done"}
 
 
@@ -39,18 +39,23 @@ class Server:
         self._lock = threading.Lock()
 
     def submit(self, programs: PopulationLike, dataset=None, datasets: Optional[Sequence] = None,
-               kind: str = "mse", fit_iterations: int = 10) -> int:
+               kind: str = "mse", fit_iterations: int = 10, seed: int = 0) -> int:
+        """Queues a job and returns its ticket.  kind: "mse", "grad" (MSE and
+        d(MSE)/d(constants)), "fit" (L-BFGS, `fit_iterations` steps) or
+        "fit_auto" (the reference's choice per program: L-BFGS, CMA-ES with
+        streams from `seed`, or Nelder-Mead)."""
         pk = _packed(programs)
         pop, keep = _as_population(pk)
         n = pk.n
         mse = np.zeros(max(n, 1), np.float32)
         grad = np.zeros(max(n, 1) * 32, np.float32) if kind == "grad" else None
-        params = np.array(pk.params, np.float32, copy=True) if kind == "fit" else None
+        params = np.array(pk.params, np.float32, copy=True) if kind in ("fit", "fit_auto") else None
         if params is not None and len(params) == 0:
             params = np.zeros(1, np.float32)
         j = N.Job()
         j.kind = KINDS[kind]
         j.fit_iterations = fit_iterations
+        j.seed = seed
         j.pop = C.pointer(pop)
         dsp = None
         if datasets is not None:

@@ -202,3 +202,49 @@ def test_dataset_pinned_by_job_and_dead_submitter(setup):
         assert srv.poll(t) == "done"
         srv.wait(t)
     d.release()
+
+
+def _method(p):
+    """optimize_individual_constants' choice (src/engine/optimize/mod.rs:24-58)."""
+    ops = {w & 0xFF for w in p.code}
+    if not ops & {I.OP["InverseM2"], I.OP["InverseM3"]}:
+        return "lbfgs"
+    return "cmaes" if any(c.kind in (I.VEC2, I.VEC3, I.MAT2, I.MAT3) for c in p.constants) else "nelder_mead"
+
+
+def test_fit_auto_picks_the_reference_optimiser(setup):
+    """A "fit_auto" job fits each program with the optimiser the reference
+    would pick, and each group's results are exactly those of the batched
+    driver called on that group alone."""
+    eng, data, pops, dev = setup
+    M = lambda i: I.load_var(I.MAT2, i)
+    extra = [
+        Program([M(0), I.op("InverseM2"), I.load_const(I.MAT2, 0), I.op("AddM2"), I.op("TraceM2")],
+                [I.Scalar(I.MAT2, (0.5, -0.2, 0.1, 0.4))]),
+        Program([M(4), I.load_const(I.VEC2, 0), I.op("MulM2V2"), I.op("NormV2"), M(0), I.op("InverseM2"),
+                 I.op("DetM2"), I.op("AddF")], [I.Scalar(I.VEC2, (1.0, -1.0))]),
+    ]
+    progs = [p for p in pops["inverse"][:60] if p.param_count() > 0] + extra
+    kinds = [_method(p) for p in progs]
+    assert {"lbfgs", "nelder_mead", "cmaes"} <= set(kinds)
+    iters, seed = 40, 4242
+    srv = Server(eng, slots=2)
+    try:
+        out = srv.wait(srv.submit(progs, dev["inverse"], kind="fit_auto", fit_iterations=iters, seed=seed))
+    finally:
+        srv.close()
+    pk = I.pack(progs)
+    for method in ("lbfgs", "nelder_mead", "cmaes"):
+        idx = [i for i, k in enumerate(kinds) if k == method]
+        sub = [progs[i] for i in idx]
+        if method == "lbfgs":
+            p, m, _ = eng.fit_lbfgs(sub, dev["inverse"], 15)
+        elif method == "nelder_mead":
+            p, m, _ = eng.fit_nelder_mead(sub, dev["inverse"], iters)
+        else:
+            p, m, _ = eng.fit_cma_es(sub, dev["inverse"], max(iters // 16, 2), seed=seed)
+        spk = I.pack(sub)
+        for k, i in enumerate(idx):
+            got = out["params"][pk.param_off[i]:pk.param_off[i + 1]]
+            np.testing.assert_array_equal(got, p[spk.param_off[k]:spk.param_off[k + 1]], err_msg=f"{method} {i}")
+            assert np.float32(out["mse"][i]) == np.float32(m[k]), (method, i)
