@@ -23,15 +23,18 @@ cudaError_t launch_finalize_mse(const ProgDesc *progs, const DatasetDesc *ds, co
                                 float *out, cudaStream_t st);
 
 // register-stack kernel (kernels_reg.cu)
-cudaError_t launch_reg(const LaunchArgs &a, int profile, int P, bool no_unary, uint32_t grid, cudaStream_t st);
-bool reg_has_no_unary(int profile);
+// omit: handler sets the launch's programs do not need (bit 0: unary Float
+// ops; bit 1: mat-vec with a feature, constant or spilled matrix), within
+// reg_omittable(profile)
+cudaError_t launch_reg(const LaunchArgs &a, int profile, int P, unsigned omit, uint32_t grid, cudaStream_t st);
+unsigned reg_omittable(int profile);
 void reg_layout(uint32_t code_words, uint32_t const_floats, const uint32_t *stack_depth, int P, int G,
                 uint32_t *stack_off, uint32_t *acc_off, uint32_t *region_floats, uint32_t *block_hdr_floats);
 int reg_max_p(int profile);
 // Dynamic shared memory of one register-kernel block (bytes).
 size_t reg_smem_bytes(uint32_t code_words, uint32_t const_floats, const uint32_t *stack_depth, int P, int G);
 constexpr size_t kRegSmemBudget = 200 * 1024;  // at least one block per SM, below the 227 KB cap
-int reg_max_blocks_per_sm(int profile, int P, bool no_unary, size_t smem);
+int reg_max_blocks_per_sm(int profile, int P, unsigned omit, size_t smem);
 
 // adjoint kernel (kernels_grad.cu)
 cudaError_t launch_grad(const LaunchArgs &a, int profile, bool no_unary, uint32_t warps_per_block, size_t smem,

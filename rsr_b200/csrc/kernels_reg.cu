@@ -262,15 +262,21 @@ __device__ __forceinline__ void acc_op(Acc<PROF, P> &a, const AccIO<P> &io, uint
 #define RSR_BLOCK_F RSR_C27(K_F)     // 0..26
 #define RSR_BLOCK_F_NU RSR_C9(K_F) RSR_C9(K_F + 9) RSR_C(K_F + 18) RSR_C(K_F + 19) RSR_C(K_F + 20)  // 0..20
 static_assert(K_F_UN == K_F + 21 && K_F_END == K_F + 27, "Float block: 21 kinds, then the 6 unary ones");
+// Vec3 block without the mat-vec kinds whose matrix is a feature, a constant
+// or a spilled value (64 + 30..32)
+#define RSR_BLOCK_V3_NM RSR_C27(K_V3) RSR_C(K_V3 + 27) RSR_C(K_V3 + 28) RSR_C(K_V3 + 29) RSR_C(K_V3 + 33)
+static_assert(kv_mulm(5, 3) == 29 && kv_make(5, 3) == 33, "Vec3 block: mat-vec kinds at 29..32");
 #define RSR_BLOCK_V2 RSR_C27(K_V2)   // 32..58
 #define RSR_BLOCK_V3 RSR_C27(K_V3) RSR_C4(K_V3 + 27) RSR_C(K_V3 + 31) RSR_C(K_V3 + 32) RSR_C(K_V3 + 33)  // 64..97
 #define RSR_BLOCK_M2 RSR_C27(K_M2)   // 104..130
 #define RSR_BLOCK_M3 RSR_C27(K_M3)   // 136..162
 
 // Runs one program (accumulator form) on this lane's P points; the result
-// is left in A_F.  NU: the launch's programs use no unary Float op (sin, cos,
-// exp, sqr, sqrt, ln), so their handlers are left out of the kernel.
-template <int PROF, int P, bool NU>
+// is left in A_F.  OMIT: handlers left out of the kernel because no program
+// of the launch needs them -- bit 0: the unary Float ops (sin, cos, exp,
+// sqr, sqrt, ln); bit 1 (F+V3 profile): mat-vec products whose matrix is a
+// feature, a constant or a spilled value.
+template <int PROF, int P, int OMIT>
 __device__ __forceinline__ void run_program(Acc<PROF, P> &a, const AccIO<P> &io, const uint32_t *code,
                                             uint32_t len) {
     // Each profile's switch lists only its own types' kinds, so the branch
@@ -280,12 +286,17 @@ __device__ __forceinline__ void run_program(Acc<PROF, P> &a, const AccIO<P> &io,
         const uint32_t wn = code[pc + 1];
         const uint32_t arg = w >> 8;
         const uint32_t kind = w & 0xFFu;
+        constexpr bool NU = (OMIT & 1) != 0, NM = (OMIT & 2) != 0;
         if constexpr (PROF == P_F && NU) {
             switch (kind) { RSR_BLOCK_F_NU default: break; }
         } else if constexpr (PROF == P_F) {
             switch (kind) { RSR_BLOCK_F default: break; }
+        } else if constexpr (PROF == P_FV3 && NU && NM) {
+            switch (kind) { RSR_BLOCK_F_NU RSR_BLOCK_V3_NM default: break; }
         } else if constexpr (PROF == P_FV3 && NU) {
             switch (kind) { RSR_BLOCK_F_NU RSR_BLOCK_V3 default: break; }
+        } else if constexpr (PROF == P_FV3 && NM) {
+            switch (kind) { RSR_BLOCK_F RSR_BLOCK_V3_NM default: break; }
         } else if constexpr (PROF == P_FV3) {
             switch (kind) { RSR_BLOCK_F RSR_BLOCK_V3 default: break; }
         } else if constexpr (PROF == P_FV2M2 && NU) {
@@ -303,6 +314,7 @@ __device__ __forceinline__ void run_program(Acc<PROF, P> &a, const AccIO<P> &io,
 
 #undef RSR_BLOCK_F
 #undef RSR_BLOCK_F_NU
+#undef RSR_BLOCK_V3_NM
 #undef RSR_BLOCK_V2
 #undef RSR_BLOCK_V3
 #undef RSR_BLOCK_M2
@@ -336,7 +348,7 @@ constexpr int reg_min_blocks() {
     else return P >= 8 ? 2 : 4;
 }
 
-template <int PROF, int P, bool NU>
+template <int PROF, int P, int OMIT>
 __global__ void __launch_bounds__(kRegThreads, reg_min_blocks<PROF, P>()) reg_eval_kernel(const LaunchArgs a) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -402,7 +414,7 @@ __global__ void __launch_bounds__(kRegThreads, reg_min_blocks<PROF, P>()) reg_ev
             for (uint32_t g = 0; g < G; ++g) {
                 if (a.active && !a.active[it.prog_begin + g]) continue;
                 io.consts = sconst + meta[3 * g + 2];
-                run_program<PROF, P, NU>(acc, io, scode + meta[3 * g], meta[3 * g + 1]);
+                run_program<PROF, P, OMIT>(acc, io, scode + meta[3 * g], meta[3 * g + 1]);
                 const Vf<P> pred = acc.F[0];
                 if (a.mode == MODE_POINTS) {
                     store_pts<P>(a.points_out + (uint64_t)(it.prog_begin + g) * a.points_stride + p0, pred, p0,
@@ -481,9 +493,9 @@ size_t reg_smem_bytes(uint32_t code_words, uint32_t const_floats, const uint32_t
     return ((size_t)hf + (size_t)rf * (kRegThreads / 32)) * 4u;
 }
 
-template <int PROF, int P, bool NU>
+template <int PROF, int P, int OMIT>
 static cudaError_t launch_reg_pp(const LaunchArgs &a, uint32_t grid, cudaStream_t st) {
-    auto k = reg_eval_kernel<PROF, P, NU>;
+    auto k = reg_eval_kernel<PROF, P, OMIT>;
     const size_t smem = ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (kRegThreads / 32)) * 4u;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin);
     if (e != cudaSuccess) return e;
@@ -495,52 +507,64 @@ static cudaError_t launch_reg_pp(const LaunchArgs &a, uint32_t grid, cudaStream_
 // F+V2+M2 profiles, {2, 4} for the others.
 int reg_max_p(int profile) { return profile == P_F || profile == P_FV3 || profile == P_FV2M2 ? 8 : 4; }
 
-// Kernels without the unary Float handlers exist for the F, F+V3 and F+V2+M2
-// profiles.
-bool reg_has_no_unary(int profile) { return profile == P_F || profile == P_FV3 || profile == P_FV2M2; }
-
-template <int PROF, bool NU>
-static cudaError_t launch_reg_p3(const LaunchArgs &a, int P, uint32_t grid, cudaStream_t st) {
-    return P >= 8 ? launch_reg_pp<PROF, 8, NU>(a, grid, st)
-         : P >= 4 ? launch_reg_pp<PROF, 4, NU>(a, grid, st) : launch_reg_pp<PROF, 2, NU>(a, grid, st);
+// Handler sets a profile has kernels without (the OMIT mask of run_program).
+unsigned reg_omittable(int profile) {
+    return profile == P_FV3 ? 3u : profile == P_F || profile == P_FV2M2 ? 1u : 0u;
 }
 
-cudaError_t launch_reg(const LaunchArgs &a, int profile, int P, bool no_unary, uint32_t grid, cudaStream_t st) {
+template <int PROF, int OMIT>
+static cudaError_t launch_reg_p3(const LaunchArgs &a, int P, uint32_t grid, cudaStream_t st) {
+    return P >= 8 ? launch_reg_pp<PROF, 8, OMIT>(a, grid, st)
+         : P >= 4 ? launch_reg_pp<PROF, 4, OMIT>(a, grid, st) : launch_reg_pp<PROF, 2, OMIT>(a, grid, st);
+}
+
+cudaError_t launch_reg(const LaunchArgs &a, int profile, int P, unsigned omit, uint32_t grid, cudaStream_t st) {
     switch (profile) {
-        case P_F: return no_unary ? launch_reg_p3<P_F, true>(a, P, grid, st) : launch_reg_p3<P_F, false>(a, P, grid, st);
-        case P_FV3: return no_unary ? launch_reg_p3<P_FV3, true>(a, P, grid, st)
-                                    : launch_reg_p3<P_FV3, false>(a, P, grid, st);
-        case P_FV2M2: return no_unary ? launch_reg_p3<P_FV2M2, true>(a, P, grid, st)
-                                      : launch_reg_p3<P_FV2M2, false>(a, P, grid, st);
-        case P_FV3M3: return P >= 4 ? launch_reg_pp<P_FV3M3, 4, false>(a, grid, st)
-                                    : launch_reg_pp<P_FV3M3, 2, false>(a, grid, st);
-        default: return P >= 4 ? launch_reg_pp<P_ALL, 4, false>(a, grid, st) : launch_reg_pp<P_ALL, 2, false>(a, grid, st);
+        case P_F: return omit & 1u ? launch_reg_p3<P_F, 1>(a, P, grid, st) : launch_reg_p3<P_F, 0>(a, P, grid, st);
+        case P_FV3:
+            switch (omit & 3u) {
+                case 3: return launch_reg_p3<P_FV3, 3>(a, P, grid, st);
+                case 2: return launch_reg_p3<P_FV3, 2>(a, P, grid, st);
+                case 1: return launch_reg_p3<P_FV3, 1>(a, P, grid, st);
+                default: return launch_reg_p3<P_FV3, 0>(a, P, grid, st);
+            }
+        case P_FV2M2: return omit & 1u ? launch_reg_p3<P_FV2M2, 1>(a, P, grid, st)
+                                       : launch_reg_p3<P_FV2M2, 0>(a, P, grid, st);
+        case P_FV3M3: return P >= 4 ? launch_reg_pp<P_FV3M3, 4, 0>(a, grid, st)
+                                    : launch_reg_pp<P_FV3M3, 2, 0>(a, grid, st);
+        default: return P >= 4 ? launch_reg_pp<P_ALL, 4, 0>(a, grid, st) : launch_reg_pp<P_ALL, 2, 0>(a, grid, st);
     }
 }
 
-template <int PROF, int P, bool NU>
+template <int PROF, int P, int OMIT>
 static int occ(size_t smem) {
     // the occupancy query counts a block above 48 KB of dynamic shared memory
     // as unlaunchable until the kernel's limit has been raised
-    auto k = reg_eval_kernel<PROF, P, NU>;
+    auto k = reg_eval_kernel<PROF, P, OMIT>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin) != cudaSuccess) return 0;
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kRegThreads, smem) != cudaSuccess) return 0;
     return n;
 }
 
-template <int PROF, bool NU>
+template <int PROF, int OMIT>
 static int occ3(int P, size_t smem) {
-    return P >= 8 ? occ<PROF, 8, NU>(smem) : P >= 4 ? occ<PROF, 4, NU>(smem) : occ<PROF, 2, NU>(smem);
+    return P >= 8 ? occ<PROF, 8, OMIT>(smem) : P >= 4 ? occ<PROF, 4, OMIT>(smem) : occ<PROF, 2, OMIT>(smem);
 }
 
-int reg_max_blocks_per_sm(int profile, int P, bool no_unary, size_t smem) {
+int reg_max_blocks_per_sm(int profile, int P, unsigned omit, size_t smem) {
     switch (profile) {
-        case P_F: return no_unary ? occ3<P_F, true>(P, smem) : occ3<P_F, false>(P, smem);
-        case P_FV3: return no_unary ? occ3<P_FV3, true>(P, smem) : occ3<P_FV3, false>(P, smem);
-        case P_FV2M2: return no_unary ? occ3<P_FV2M2, true>(P, smem) : occ3<P_FV2M2, false>(P, smem);
-        case P_FV3M3: return P >= 4 ? occ<P_FV3M3, 4, false>(smem) : occ<P_FV3M3, 2, false>(smem);
-        default: return P >= 4 ? occ<P_ALL, 4, false>(smem) : occ<P_ALL, 2, false>(smem);
+        case P_F: return omit & 1u ? occ3<P_F, 1>(P, smem) : occ3<P_F, 0>(P, smem);
+        case P_FV3:
+            switch (omit & 3u) {
+                case 3: return occ3<P_FV3, 3>(P, smem);
+                case 2: return occ3<P_FV3, 2>(P, smem);
+                case 1: return occ3<P_FV3, 1>(P, smem);
+                default: return occ3<P_FV3, 0>(P, smem);
+            }
+        case P_FV2M2: return omit & 1u ? occ3<P_FV2M2, 1>(P, smem) : occ3<P_FV2M2, 0>(P, smem);
+        case P_FV3M3: return P >= 4 ? occ<P_FV3M3, 4, 0>(smem) : occ<P_FV3M3, 2, 0>(smem);
+        default: return P >= 4 ? occ<P_ALL, 4, 0>(smem) : occ<P_ALL, 2, 0>(smem);
     }
 }
 

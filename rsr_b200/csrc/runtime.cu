@@ -115,7 +115,7 @@ void TaskPool::run(uint32_t n, const std::function<void(uint32_t)> &f) {
     done_cv_.wait(lk, [&] { return finished_ == threads_.size(); });
 }
 
-// register path = profile + 8 * (spill-depth class + 3 * no-unary flag)
+// register path = profile + 8 * (spill-depth class + 3 * omitted-handler mask)
 static constexpr int kRegPathStride = 8;
 // Tape shared memory per warp that the adjoint's points per lane aim for.
 // More points per lane amortise the dispatch over more work at the cost of
@@ -263,15 +263,18 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                 uint32_t dmax = 0;
                 for (int t = 0; t < N_STACKS; ++t) dmax = std::max(dmax, depth[t]);
                 const int cls = dmax <= 1 ? 0 : dmax <= 2 ? 1 : 2;
-                // and apart, programs without a unary Float op, whose kernel
-                // is built without those handlers (a smaller kernel: fewer
-                // instruction-cache misses)
-                bool nu = reg_has_no_unary(enc[i].profile);
+                // and apart by the handler sets the program does not use
+                // (unary Float ops; mat-vec with a leaf or spilled matrix),
+                // whose kernels are built without them: smaller kernels,
+                // fewer instruction-cache misses
+                const uint32_t mv = (uint32_t)(K_V3 + kv_mulm(kBinOps[SV3], 3));
+                unsigned omit = reg_omittable(enc[i].profile);
                 for (uint32_t w : enc[i].reg_code) {
                     const uint32_t kind = w & 0xFFu;
-                    if (kind >= (uint32_t)K_F_UN && kind < (uint32_t)K_F_END) nu = false;
+                    if (kind >= (uint32_t)K_F_UN && kind < (uint32_t)K_F_END) omit &= ~1u;
+                    if (kind >= mv + 1 && kind <= mv + 3) omit &= ~2u;
                 }
-                path[i] = enc[i].profile + kRegPathStride * (cls + 3 * (nu ? 1 : 0));
+                path[i] = enc[i].profile + kRegPathStride * (cls + 3 * (int)omit);
             }
         }
         // programs the register kernel cannot take run on the slot-file kernel
@@ -338,7 +341,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         Group g;
         g.kind = pth <= -2 ? 2 : pth == -1 ? 0 : 1;
         g.profile = pth >= 0 ? pth % kRegPathStride : pth <= -2 ? (-2 - pth) % N_PROFILES : -1;
-        g.no_unary = pth >= 3 * kRegPathStride;  // register kernel; the adjoint's flag is set below
+        g.omit = pth >= 0 ? (unsigned)(pth / kRegPathStride / 3) : 0u;
         g.item_begin = (uint32_t)P.items.size();
         if (g.kind == 1) {
             // P and G are per profile and dataset size; one launch uses one P,
@@ -549,12 +552,12 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             reg_layout(g.code_words, g.const_floats, g.stack_depth, g.P, g.G, a.stack_off, &a.acc_off, &a.region_floats,
                        &a.block_hdr_floats);
             const size_t smem = ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (kRegThreads / 32)) * 4u;
-            int bps = std::max(1, reg_max_blocks_per_sm(g.profile, g.P, g.no_unary, smem));
+            int bps = std::max(1, reg_max_blocks_per_sm(g.profile, g.P, g.omit, smem));
             uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)bps * ctx->num_sms, g.n_items);
             g.grid = std::max(1u, grid);
             g.smem = smem;
             g.warps_per_block = kRegThreads / 32;
-            e = launch_reg(a, g.profile, g.P, g.no_unary, g.grid, gs);
+            e = launch_reg(a, g.profile, g.P, g.omit, g.grid, gs);
         } else {
             const size_t per = grad_smem_per_warp(g.code_words, g.const_floats, g.slots, g.adj_slots, g.P);
             a.smem_adj_slots = g.adj_slots;
@@ -1125,7 +1128,8 @@ int rsr_batch_describe(rsr_ctx *ctx, rsr_batch *b, char *buf, size_t len) {
         const Group &g = b->plan.groups[i];
         const char *kn = g.kind == 0 ? "slot" : g.kind == 1 ? "register" : "adjoint";
         s += (i ? ", " : "") + std::string("{\"kernel\": \"") + kn + "\", \"profile\": " + std::to_string(g.profile) +
-             ", \"no_unary\": " + (g.no_unary ? "true" : "false") +
+             ", \"no_unary\": " + ((g.kind == 1 ? (g.omit & 1u) != 0 : g.no_unary) ? "true" : "false") +
+             ", \"no_matrix_operand\": " + ((g.kind == 1 && (g.omit & 2u)) ? "true" : "false") +
              ", \"points_per_thread\": " + std::to_string(g.P) + ", \"programs_per_warp\": " + std::to_string(g.G) +
              ", \"items\": " + std::to_string(g.n_items) + ", \"flops\": " + std::to_string(g.flops) +
              ", \"program_points\": " + std::to_string(g.program_points) + ", \"grid\": " + std::to_string(g.grid) +

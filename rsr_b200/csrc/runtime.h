@@ -101,7 +101,8 @@ struct TuneChoice {
 struct Group {
     int kind = 0;        // 0 plain, 1 register, 2 adjoint
     int profile = -1;
-    bool no_unary = false;  // register kernel: no unary Float op in the launch's programs
+    unsigned omit = 0;      // register kernel: handler sets its programs do not need (launch_reg)
+    bool no_unary = false;  // adjoint kernel: no unary Float op in the launch's programs
     int P = 4;
     int G = 1;
     uint32_t item_begin = 0, n_items = 0;  // into the plan's item array
