@@ -37,12 +37,12 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 # DRAM bytes (read + write) of the dominant kernel's launches in one step of
-# this workload (three spill-depth classes), from one ncu capture
+# this workload (three spill-depth classes, P=8 G=4), from one ncu capture
 # (profiles/reg_eval_kernel_vector_1024x100k.md, "Full bench size"):
-# 5,120,512 + 4,896,512 + 4,131,584 read, 0 written.  ncu replays each launch
+# 4,856,832 + 4,630,016 + 4,114,944 read, 0 written.  ncu replays each launch
 # with cold caches, so each re-reads the 4 MB dataset; in a step the second
 # and third launches find it in L2.
-DOMINANT_KERNEL_DRAM_BYTES = 14_148_608
+DOMINANT_KERNEL_DRAM_BYTES = 13_601_792
 METRIC = "program_points_per_sec"
 UNIT = "program*points/s"
 N_PROGRAMS = 4096

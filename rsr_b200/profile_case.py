@@ -27,8 +27,10 @@ def main(argv=None) -> int:
     ap.add_argument("--points", type=int, default=0, help="override the workload's point count")
     ap.add_argument("--kernel", default="register", choices=["register", "plain", "adjoint"])
     ap.add_argument("--runs", type=int, default=3)
+    ap.add_argument("--points-per-thread", type=int, default=0, help="register kernel P (default: the engine's)")
+    ap.add_argument("--programs-per-warp", type=int, default=0, help="register kernel G (default: the engine's)")
     a = ap.parse_args(argv)
-    eng = Engine(use_graphs=False)
+    eng = Engine(use_graphs=False, points_per_thread=a.points_per_thread, programs_per_warp=a.programs_per_warp)
     if a.workload == "scalar":
         ds, pop = W.scalar_dataset(a.points or 400, seed=1), W.scalar_population(a.programs, seed=11)
     elif a.workload == "vector":
