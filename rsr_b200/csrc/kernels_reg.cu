@@ -339,17 +339,22 @@ constexpr uint32_t kMaxProgsPerWarp = 8;
 // as many as its accumulators allow without spilling.
 // At four points per lane a fourth block (64 registers, a few bytes of
 // spill) pays for the F and F+V3 profiles (vector workload: 4.75 ms against
-// 5.14 ms at three blocks); F+V2+M2 spills more there and keeps three.
-template <int PROF, int P>
+// 5.14 ms at three blocks); F+V2+M2 spills more there and keeps three.  At
+// eight points, the F+V3 instances without the leaf-matrix mat-vec handlers
+// fit a third block (80 registers, 52 bytes of spill; vector workload 4.29
+// ms against 4.50 ms at two blocks); with those handlers they spill twice as
+// much and keep two.
+template <int PROF, int P, int OMIT>
 constexpr int reg_min_blocks() {
     if constexpr (PROF == P_ALL) return P >= 4 ? 1 : 2;
     else if constexpr (PROF == P_FV3M3) return P >= 4 ? 2 : 3;
     else if constexpr (PROF == P_FV2M2) return P >= 8 ? 2 : P >= 4 ? 3 : 4;
+    else if constexpr (PROF == P_FV3 && (OMIT & 2) != 0) return P >= 8 ? 3 : 4;
     else return P >= 8 ? 2 : 4;
 }
 
 template <int PROF, int P, int OMIT>
-__global__ void __launch_bounds__(kRegThreads, reg_min_blocks<PROF, P>()) reg_eval_kernel(const LaunchArgs a) {
+__global__ void __launch_bounds__(kRegThreads, reg_min_blocks<PROF, P, OMIT>()) reg_eval_kernel(const LaunchArgs a) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nw = blockDim.x >> 5;
