@@ -266,6 +266,9 @@ static_assert(K_F_UN == K_F + 21 && K_F_END == K_F + 27, "Float block: 21 kinds,
 // or a spilled value (64 + 30..32)
 #define RSR_BLOCK_V3_NM RSR_C27(K_V3) RSR_C(K_V3 + 27) RSR_C(K_V3 + 28) RSR_C(K_V3 + 29) RSR_C(K_V3 + 33)
 static_assert(kv_mulm(5, 3) == 29 && kv_make(5, 3) == 33, "Vec3 block: mat-vec kinds at 29..32");
+// Vec3 block as the F+V3 profile can meet it: a mat-vec with a spilled matrix
+// (64 + 32) needs a Mat3 accumulator, which that profile does not have
+#define RSR_BLOCK_V3_F RSR_C27(K_V3) RSR_C4(K_V3 + 27) RSR_C(K_V3 + 31) RSR_C(K_V3 + 33)
 #define RSR_BLOCK_V2 RSR_C27(K_V2)   // 32..58
 #define RSR_BLOCK_V3 RSR_C27(K_V3) RSR_C4(K_V3 + 27) RSR_C(K_V3 + 31) RSR_C(K_V3 + 32) RSR_C(K_V3 + 33)  // 64..97
 #define RSR_BLOCK_M2 RSR_C27(K_M2)   // 104..130
@@ -294,11 +297,11 @@ __device__ __forceinline__ void run_program(Acc<PROF, P> &a, const AccIO<P> &io,
         } else if constexpr (PROF == P_FV3 && NU && NM) {
             switch (kind) { RSR_BLOCK_F_NU RSR_BLOCK_V3_NM default: break; }
         } else if constexpr (PROF == P_FV3 && NU) {
-            switch (kind) { RSR_BLOCK_F_NU RSR_BLOCK_V3 default: break; }
+            switch (kind) { RSR_BLOCK_F_NU RSR_BLOCK_V3_F default: break; }
         } else if constexpr (PROF == P_FV3 && NM) {
             switch (kind) { RSR_BLOCK_F RSR_BLOCK_V3_NM default: break; }
         } else if constexpr (PROF == P_FV3) {
-            switch (kind) { RSR_BLOCK_F RSR_BLOCK_V3 default: break; }
+            switch (kind) { RSR_BLOCK_F RSR_BLOCK_V3_F default: break; }
         } else if constexpr (PROF == P_FV2M2 && NU) {
             switch (kind) { RSR_BLOCK_F_NU RSR_BLOCK_V2 RSR_BLOCK_M2 default: break; }
         } else if constexpr (PROF == P_FV2M2) {
@@ -315,6 +318,7 @@ __device__ __forceinline__ void run_program(Acc<PROF, P> &a, const AccIO<P> &io,
 #undef RSR_BLOCK_F
 #undef RSR_BLOCK_F_NU
 #undef RSR_BLOCK_V3_NM
+#undef RSR_BLOCK_V3_F
 #undef RSR_BLOCK_V2
 #undef RSR_BLOCK_V3
 #undef RSR_BLOCK_M2
