@@ -374,6 +374,35 @@ def run_engine(args):
     plain_value = pp_rank * world * len(pms) / (max_over_ranks(sum(pms)) * 1e-3)
     bp.close()
 
+    # ------------------------------------------ adjoint: MSE and gradient
+    bg = eng.prepare(pk, dd, gradient=True)
+    ams = []
+    for i in range(3 + max(3, min(args.steps, 10))):
+        eng.flush_l2()
+        bg.run()
+        bg.results()
+        t = bg.timing()[1]
+        if i >= 3:
+            ams.append(t)
+    adj_value = pp_rank * world * len(ams) / (max_over_ranks(sum(ams)) * 1e-3)
+    bg.close()
+
+    # ------------------- register interpreter without the batching extras
+    # one program per work item, 4 points per lane, no autotuning, no graph:
+    # the register kernel as a one-program-per-warp interpreter
+    eng3 = Engine(points_per_thread=4, programs_per_warp=1, use_graphs=False)
+    b3 = eng3.prepare(pk, eng3.upload(ds))
+    rms = []
+    for i in range(3 + max(3, min(args.steps, 10))):
+        eng3.flush_l2()
+        b3.run()
+        t = b3.timing()[1]
+        if i >= 3:
+            rms.append(t)
+    reg1_value = pp_rank * world * len(rms) / (max_over_ranks(sum(rms)) * 1e-3)
+    b3.close()
+    eng3.close()
+
     # ------------------------------------------- end to end through the API
     e2e_ms, h2d, d2h = [], 0, 0
     for i in range(2 + max(3, min(args.steps, 20))):
@@ -411,6 +440,13 @@ def run_engine(args):
                        "l2": "flushed between steps (256 MiB memset outside the timed events)"},
             "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                            "max": float(max(step_ms))},
+            "adjoint": {"value": adj_value, "unit": UNIT, "ms_per_step": float(np.median(ams)),
+                        "what": "MSE and d(MSE)/d(constants) of the same batch, reverse-mode adjoint kernel, "
+                                "graph replay"},
+            "register_one_program_per_item": {
+                "value": reg1_value, "unit": UNIT, "speedup_of_batched": value / reg1_value,
+                "ms_per_step": float(np.median(rms)),
+                "what": "register kernel, G=1, P=4, no autotuning, no CUDA graph"},
             "plain": {"value": plain_value, "unit": UNIT, "speedup_of_batched": value / plain_value,
                       "ms_per_step": float(np.median(pms))},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
