@@ -122,21 +122,28 @@ struct Scratch {
     // tape form
     std::vector<int> idx, pos, vend, astart;
     std::vector<uint32_t> vs, as;
-    SlotPool vals, adjs;
+    SlotPool vals;
 };
 thread_local Scratch tls;
 
 // Tape form for the adjoint kernel.  Live nodes in program order; node t runs
-// forward at time t and in reverse at time 2N-1-t.  A value slot lives from
-// its definition to its last forward read, or to the reverse step of the
-// last node whose reverse rule reads it; an adjoint slot lives from the
-// reverse step of its latest consumer (its first contribution) to its own
-// reverse step, after which the kernel zeroes it.  Feature loads have no
-// tape entry: their value slot is kTapeFeature | feature offset, read from
-// the dataset where it is used, and their adjoint contributions go to a sink
-// run of 9 slots at 0 that is never read.  Words: header (result value slot, result adjoint slot), then
-// 5 per node: op | aux << 8 | out_width << 28, vo | ao << 16, and
-// vi | ai << 16 for inputs 0..2.
+// forward at time t and in reverse at time 2N-1-t.  A value lives from its
+// definition to its last forward read, or to the reverse step of the last
+// node whose reverse rule reads it; an adjoint lives from the reverse step of
+// its latest consumer (its first contribution) to its own reverse step.
+// Values and adjoints share one slot file, allocated first-fit by lifetime
+// in order of start time; the input through which an adjoint receives its
+// first contribution carries kTapeZeroFirst, so the reverse step clears those
+// slots before adding to them (the root's adjoint is written by the seed).
+// Feature loads have no tape entry: their value slot is kTapeFeature |
+// feature offset, read from the dataset where it is used, and their adjoint
+// field is a sink past the slot file, which takes contributions and is never
+// read; the reverse rules of matrix products and inverses skip a feature
+// matrix's contributions outright, so the sink is as wide as the widest
+// feature that other rules send contributions from.  Words: header (result value slot, result adjoint
+// slot), then 5 per node: op | aux << 8 | out_width << 28 (aux: the load's
+// operand, a copy's has_alias | width << 1, else the input widths in three
+// nibbles), vo | ao << 16, and vi | ai << 16 for inputs 0..2.
 void emit_tape(const std::vector<Node> &nodes, const std::vector<char> &live, int root, EncodedProgram *E) {
     std::vector<int> &idx = tls.idx;  // tape order -> node id
     std::vector<int> &pos = tls.pos;
@@ -152,6 +159,13 @@ void emit_tape(const std::vector<Node> &nodes, const std::vector<char> &live, in
     std::vector<int> &vend = tls.vend, &astart = tls.astart;
     vend.assign(N, -1);
     astart.assign(N, 1 << 30);
+    // first[u]: (consumer, input) of u's first adjoint contribution -- the
+    // latest consumer in program order, its lowest input that reads u
+    std::vector<int> &first = tls.work;
+    first.assign(2 * (size_t)N, -1);
+    // sink_width: the widest feature whose adjoint contributions are made
+    // (the matrix input of a matrix product or inverse skips them)
+    uint32_t sink_width = 0;
     for (int t = 0; t < N; ++t) {
         const Node &n = nodes[idx[t]];
         const int rr = n.stale ? 0 : reverse_reads(n.opcode);
@@ -161,6 +175,17 @@ void emit_tape(const std::vector<Node> &nodes, const std::vector<char> &live, in
             vend[u] = std::max(vend[u], t);                                // forward read
             if (k >= 0 && ((rr >> k) & 1)) vend[u] = std::max(vend[u], rev - t);
             astart[u] = std::min(astart[u], rev - t);                      // adjoint contribution
+            if (first[2 * u] != t) {
+                first[2 * u] = t;
+                first[2 * u + 1] = k < 0 ? 0 : k;
+            }
+            const Node &un = nodes[in_node];
+            if (!un.stale && is_load(un.opcode) && !is_const_load(un.opcode)) {
+                const int op = n.stale ? -1 : n.opcode;
+                const bool skipped = ((op == MUL_M2V2 || op == MUL_M3V3) && k == 0) || op == MUL_M2 ||
+                                     op == MUL_M3 || op == INVERSE_M2 || op == INVERSE_M3;
+                if (!skipped) sink_width = std::max(sink_width, (uint32_t)kStackWidth[un.out]);
+            }
         };
         if (n.stale) {
             if (n.alias >= 0) use(n.alias, -1);
@@ -173,30 +198,48 @@ void emit_tape(const std::vector<Node> &nodes, const std::vector<char> &live, in
         vend[rt] = std::max(vend[rt], N);          // read for the prediction
         astart[rt] = std::min(astart[rt], N - 1);  // seeded before the reverse sweep
     }
-    SlotPool &vals = tls.vals, &adjs = tls.adjs;
-    vals.busy_until.clear();
-    adjs.busy_until.clear();
-    adjs.take(9, -1, 1 << 30);  // the sink
-    std::vector<uint32_t> &vs = tls.vs, &as = tls.as;
-    vs.assign(N, 0);
-    as.assign(N, 0);
     auto is_feature = [&](int t) {
         const Node &n = nodes[idx[t]];
         return !n.stale && is_load(n.opcode) && !is_const_load(n.opcode) && n.arg < kTapeFeature;
     };
-    for (int t = 0; t < N; ++t)
-        vs[t] = is_feature(t) ? (kTapeFeature | nodes[idx[t]].arg)  // read from the dataset where used
-                              : vals.take(kStackWidth[nodes[idx[t]].out], t, std::max(vend[t], t));
-    for (int t = N - 1; t >= 0; --t) {  // adjoint intervals start in reverse node order
-        const Node &n = nodes[idx[t]];
-        if (is_feature(t) || astart[t] > rev - t) continue;  // sink
-        as[t] = adjs.take(kStackWidth[n.out], astart[t], rev - t);
+    // one slot file: every value and adjoint interval, first-fit in order of
+    // start time (the order that packs intervals of one width optimally)
+    struct Interval { int t0, t1, w, node; bool adj; };
+    std::vector<Interval> iv;
+    iv.reserve(2 * (size_t)N);
+    for (int t = 0; t < N; ++t) {
+        if (is_feature(t)) continue;
+        const int w = kStackWidth[nodes[idx[t]].out];
+        iv.push_back({t, std::max(vend[t], t), w, t, false});
+        if (astart[t] <= rev - t) iv.push_back({astart[t], rev - t, w, t, true});
     }
-    E->n_tape_val = (uint32_t)vals.busy_until.size();
-    E->n_tape_adj = (uint32_t)adjs.busy_until.size();
+    std::stable_sort(iv.begin(), iv.end(), [](const Interval &a, const Interval &b) { return a.t0 < b.t0; });
+    SlotPool &slots = tls.vals;
+    slots.busy_until.clear();
+    std::vector<uint32_t> &vs = tls.vs, &as = tls.as;
+    vs.assign(N, 0);
+    as.assign(N, 0);
+    for (const Interval &x : iv) (x.adj ? as : vs)[x.node] = slots.take(x.w, x.t0, x.t1);
+    const uint32_t sink = (uint32_t)slots.busy_until.size();
+    for (int t = 0; t < N; ++t)
+        if (is_feature(t)) {
+            vs[t] = kTapeFeature | nodes[idx[t]].arg;  // read from the dataset where used
+            as[t] = sink;
+        }
+    if (rt >= 0 && is_feature(rt)) sink_width = std::max(sink_width, (uint32_t)kStackWidth[nodes[idx[rt]].out]);  // the seed
+    E->n_tape_val = sink + sink_width;
+    E->n_tape_adj = 0;
     E->tape_code.clear();
     E->tape_code.push_back(rt >= 0 ? vs[rt] : 0xFFFFFFFFu);
     E->tape_code.push_back(rt >= 0 ? as[rt] : 0u);
+    // input k of node t carries the clear flag when it is the first
+    // contribution to that value's adjoint (never the root's: the seed is)
+    auto in_word = [&](int t, int k, int in_node) {
+        const int u = pos[in_node];
+        uint32_t a = as[u];
+        if (!is_feature(u) && u != rt && first[2 * u] == t && first[2 * u + 1] == k) a |= kTapeZeroFirst;
+        return vs[u] | (a << 16);
+    };
     for (int t = 0; t < N; ++t) {
         const Node &n = nodes[idx[t]];
         if (is_feature(t)) continue;  // no tape entry: consumers read the dataset
@@ -204,10 +247,16 @@ void emit_tape(const std::vector<Node> &nodes, const std::vector<char> &live, in
         if (n.stale) {
             // copy of the value left in that slot, or zero; aux = has_alias | width << 1
             w0 = (uint32_t)SLOT_NOP | (((n.alias >= 0 ? 1u : 0u) | ((uint32_t)kStackWidth[n.out] << 1)) << 8);
-            if (n.alias >= 0) in[0] = vs[pos[n.alias]] | (as[pos[n.alias]] << 16);
-        } else {
+            if (n.alias >= 0) in[0] = in_word(t, 0, n.alias);
+        } else if (is_load(n.opcode)) {
             w0 = (uint32_t)n.opcode | (n.arg << 8);
-            for (int k = 0; k < n.n_in; ++k) in[k] = vs[pos[n.in[k]]] | (as[pos[n.in[k]]] << 16);
+        } else {
+            uint32_t widths = 0;
+            for (int k = 0; k < n.n_in; ++k) {
+                in[k] = in_word(t, k, n.in[k]);
+                widths |= (uint32_t)kStackWidth[nodes[n.in[k]].out] << (4 * k);
+            }
+            w0 = (uint32_t)n.opcode | (widths << 8);
         }
         w0 |= (uint32_t)kStackWidth[n.out] << 28;
         E->tape_code.push_back(w0);

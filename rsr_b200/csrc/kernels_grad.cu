@@ -50,9 +50,13 @@ struct TapeCtx {
     }
     __device__ __forceinline__ void SV(uint32_t s, const Vf<P> &v) const { val[s * 32 + lane] = v; }
     __device__ __forceinline__ Vf<P> A(uint32_t s) const { return adj[s * 32 + lane]; }
+    // adds a contribution to adjoint slot s (a feature's goes to the sink)
     __device__ __forceinline__ void AddA(uint32_t s, const Vf<P> &v) const {
         Vf<P> &r = adj[s * 32 + lane];
         r = r + v;
+    }
+    __device__ __forceinline__ void ClearA(uint32_t s, uint32_t width) const {
+        for (uint32_t i = 0; i < width; ++i) adj[(s + i) * 32 + lane] = splat<P>(0.0f);
     }
     __device__ __forceinline__ Vf<P> X(uint32_t f) const { return load_pts<P>(x + f * stride + p0); }
 };
@@ -150,6 +154,7 @@ __device__ __forceinline__ void tape_forward(const TapeCtx<P> &t, const uint32_t
 // dA = -O^T G O^T for O = A^-1 (N x N, column-major), zero where singular.
 template <int P, int N>
 __device__ __forceinline__ void inverse_adjoint(const TapeCtx<P> &t, uint32_t vo, uint32_t ao, uint32_t v0, uint32_t a0) {
+    if (v0 & kTapeFeature) return;  // a feature matrix keeps no adjoint
     Vf<P> O[N * N], G[N * N], H[N * N], M[N * N];
     for (int i = 0; i < N * N; ++i) { O[i] = t.V(vo + i); G[i] = t.A(ao + i); M[i] = t.V(v0 + i); }
     Vf<P> det;
@@ -177,6 +182,8 @@ __device__ __forceinline__ void inverse_adjoint(const TapeCtx<P> &t, uint32_t vo
 template <int P, int N>
 __device__ __forceinline__ void rev_mulm(const TapeCtx<P> &t, uint32_t vo, uint32_t ao, uint32_t v0, uint32_t a0, uint32_t v1,
                                          uint32_t a1) {
+    // a feature matrix keeps no adjoint
+    const bool keep_a = !(v0 & kTapeFeature), keep_b = !(v1 & kTapeFeature);
     Vf<P> Am[N * N], Bm[N * N], G[N * N];
 #pragma unroll
     for (int i = 0; i < N * N; ++i) { Am[i] = t.V(v0 + i); Bm[i] = t.V(v1 + i); G[i] = t.A(ao + i); }
@@ -190,8 +197,8 @@ __device__ __forceinline__ void rev_mulm(const TapeCtx<P> &t, uint32_t vo, uint3
                 da = da + G[N * j + r] * Bm[N * j + c];   // G(r,j) B(c,j)
                 db = db + Am[N * r + j] * G[N * c + j];   // A(j,r) G(j,c)
             }
-            t.AddA(a0 + N * c + r, da);
-            t.AddA(a1 + N * c + r, db);
+            if (keep_a) t.AddA(a0 + N * c + r, da);
+            if (keep_b) t.AddA(a1 + N * c + r, db);
         }
 }
 // o = M v: dM(r,c) += g_r v_c, dv_c += sum_r M(r,c) g_r.
@@ -201,14 +208,17 @@ __device__ __forceinline__ void rev_mulmv(const TapeCtx<P> &t, uint32_t vo, uint
     Vf<P> g[N], v[N];
 #pragma unroll
     for (int i = 0; i < N; ++i) { g[i] = t.A(ao + i); v[i] = t.V(v1 + i); }
+    if (!(v0 & kTapeFeature)) {  // a feature matrix keeps no adjoint
+#pragma unroll
+        for (int c = 0; c < N; ++c)
+#pragma unroll
+            for (int r = 0; r < N; ++r) t.AddA(a0 + N * c + r, g[r] * v[c]);
+    }
 #pragma unroll
     for (int c = 0; c < N; ++c) {
         Vf<P> dv = splat<P>(0.0f);
 #pragma unroll
-        for (int r = 0; r < N; ++r) {
-            t.AddA(a0 + N * c + r, g[r] * v[c]);
-            dv = dv + t.V(v0 + N * c + r) * g[r];
-        }
+        for (int r = 0; r < N; ++r) dv = dv + t.V(v0 + N * c + r) * g[r];
         t.AddA(a1 + c, dv);
     }
 }
@@ -219,10 +229,23 @@ template <int PROF, int P, bool NU>
 __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t *w, float *gacc_lane) {
     RSR_PROFILE_TYPES(PROF)
     constexpr bool HU = !NU;
-    const uint32_t op = w[0] & 0xFFu, aux = (w[0] >> 8) & 0xFFFFFu, width = w[0] >> 28;
+    const uint32_t op = w[0] & 0xFFu, aux = (w[0] >> 8) & 0xFFFFFu;
     const uint32_t vo = w[1] & 0xFFFFu, ao = w[1] >> 16;
-    const uint32_t v0 = w[2] & 0xFFFFu, a0 = w[2] >> 16, v1 = w[3] & 0xFFFFu, a1 = w[3] >> 16;
-    const uint32_t a2 = w[4] >> 16;
+    const uint32_t v0 = w[2] & 0xFFFFu, v1 = w[3] & 0xFFFFu;
+    const uint32_t a0 = (w[2] >> 16) & ~kTapeZeroFirst, a1 = (w[3] >> 16) & ~kTapeZeroFirst,
+                   a2 = (w[4] >> 16) & ~kTapeZeroFirst;
+    // inputs whose adjoint gets its first contribution here: clear their
+    // slots, which may still hold an earlier value (widths: a copy's own
+    // width, else one nibble per input)
+    if ((w[2] | w[3] | w[4]) & (kTapeZeroFirst << 16)) {
+        if (op == SLOT_NOP) {
+            if (w[2] & (kTapeZeroFirst << 16)) t.ClearA(a0, aux >> 1);
+        } else {
+            if (w[2] & (kTapeZeroFirst << 16)) t.ClearA(a0, aux & 0xFu);
+            if (w[3] & (kTapeZeroFirst << 16)) t.ClearA(a1, (aux >> 4) & 0xFu);
+            if (w[4] & (kTapeZeroFirst << 16)) t.ClearA(a2, (aux >> 8) & 0xFu);
+        }
+    }
     switch (op) {
         case SLOT_NOP:
             if (aux & 1u) for (uint32_t i = 0; i < (aux >> 1); ++i) t.AddA(a0 + i, t.A(ao + i));
@@ -351,9 +374,6 @@ __device__ __forceinline__ void tape_reverse(const TapeCtx<P> &t, const uint32_t
         case RSR_GATE(INVERSE_M3, HM3): inverse_adjoint<P, 3>(t, vo, ao, v0, a0); break;
         default: break;
     }
-    // this node's adjoint has been consumed: clear it for the slot's next
-    // holder and for the next tile
-    for (uint32_t i = 0; i < width; ++i) t.adj[(ao + i) * 32 + t.lane] = splat<P>(0.0f);
 }
 
 // NU: no program of the launch has a unary Float op (sin, cos, exp, sqr,
@@ -372,7 +392,7 @@ __global__ void __launch_bounds__(kGradThreads, 16) grad_kernel(const LaunchArgs
     float *sconst = base + cw;
     float *gacc = sconst + cf;  // [param][lane] f32 gradient sums of this item's tiles
     Vf<P> *val = reinterpret_cast<Vf<P> *>(gacc + gp * 32u);
-    Vf<P> *adj = val + (size_t)a.smem_slots * 32u;
+    Vf<P> *adj = val;  // values and adjoints share the slot file
 
     const WorkItem it = a.items[item_id];
     if (a.active && !a.active[it.prog_begin]) return;
@@ -382,9 +402,6 @@ __global__ void __launch_bounds__(kGradThreads, 16) grad_kernel(const LaunchArgs
     for (uint32_t i = lane; i < pd.n_consts; i += 32) sconst[i] = __ldg(a.consts + pd.const_off + i);
     const uint32_t np = min(pd.n_consts, kGradParams);
     for (uint32_t k = 0; k < np; ++k) gacc[k * 32 + lane] = 0.0f;
-    // adjoint slots start at zero; each node's reverse step clears its own
-    const uint32_t n_adj = pd.n_tape >> 16;
-    for (uint32_t s = 0; s < n_adj; ++s) adj[s * 32 + lane] = splat<P>(0.0f);
     __syncwarp();
     const uint32_t result = scode[0], result_adj = scode[1];
     const uint32_t *code = scode + 2;
@@ -405,7 +422,7 @@ __global__ void __launch_bounds__(kGradThreads, 16) grad_kernel(const LaunchArgs
             seed.v[k] = valid ? 2.0f * d : 0.0f;  // d(diff^2)/d pred, as in evaluator.rs:207
         }
         if (result == 0xFFFFFFFFu) continue;
-        t.AddA(result_adj, seed);
+        adj[result_adj * 32 + lane] = seed;  // the first contribution
         // reverse sweep; constant loads add their adjoints to gacc
         for (uint32_t i = n_nodes; i-- > 0;) tape_reverse<PROF, P, NU>(t, code + 5 * i, gacc + lane);
     }

@@ -105,10 +105,16 @@ RSR_HD static inline constexpr uint32_t push_load_arg(uint32_t slot, uint32_t ty
     return slot | (type1 << 4) | (is_const << 7) | (off << 8);
 }
 
-// Register-kernel profiles: the accumulator types a kernel instance holds.
 // Tape value slot that stands for a feature column (adjoint kernel): the
 // low 15 bits are the feature offset.
 constexpr uint32_t kTapeFeature = 0x8000u;
+// Tape adjoint slot fields (16 bits).  Value and adjoint slots share one slot
+// file, so on an input field kTapeZeroFirst asks the reverse step to clear
+// that input's adjoint slots before adding to them: the step holds the first
+// contribution to that adjoint, and its slots may still hold an earlier value.
+constexpr uint32_t kTapeZeroFirst = 0x8000u;
+
+// Register-kernel profiles: the accumulator types a kernel instance holds.
 
 enum Profile : int { P_F = 0, P_FV3 = 1, P_FV2M2 = 2, P_FV3M3 = 3, P_ALL = 4, N_PROFILES = 5 };
 static constexpr uint32_t kProfileTypes[N_PROFILES] = {
