@@ -250,6 +250,53 @@ def serving_bench(eng, jobs: int, rate: float, threads: int = 16, seed: int = 7,
                     "(program_points counts one evaluation per program)"}
 
 
+def serving_light_bench(eng, jobs: int = 300, rate: float = 150.0, threads: int = 8, seed: int = 9):
+    """Evaluation latency below saturation: `threads` island threads submit
+    MSE-only jobs of 64-1024 vector-workload programs (100k points) with
+    Poisson arrivals at `rate` jobs/s in total, a load the device keeps up
+    with, so latency is the jobs' own service time rather than queueing."""
+    from rsr_b200 import isa as I
+    from rsr_b200 import workloads as W
+    from rsr_b200.serving import Server
+    rng = np.random.default_rng(seed)
+    progs = W.lorentz_population(1024, seed=35)
+    d = eng.upload(W.lorentz_dataset(100_000, seed=2))
+    plan = []
+    for _ in range(jobs):
+        n = int(rng.integers(64, 1025))
+        lo = int(rng.integers(0, 1024 - n + 1))
+        plan.append(I.pack(progs[lo:lo + n]))
+    gaps = rng.exponential(threads / rate, jobs)
+    srv = Server(eng, slots=4)
+    tickets = [None] * jobs
+
+    def island(idx):
+        t_next = time.perf_counter()
+        for i in idx:
+            t_next += gaps[i]
+            dt = t_next - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            tickets[i] = srv.submit(plan[i], d, kind="mse")
+
+    th = [threading.Thread(target=island, args=(list(range(t, jobs, threads)),)) for t in range(threads)]
+    t0 = time.perf_counter()
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for t in tickets:
+        srv.wait(t)
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    d.release()
+    return {"jobs": jobs, "arrival_rate_jobs_per_s": rate, "drain_s": wall, "completed": st["completed"],
+            "latency_ms": {"p50": st["p50_ms"], "p95": st["p95_ms"], "p99": st["p99_ms"], "max": st["max_ms"]},
+            "what": "rsr_server, MSE jobs of 64-1024 programs x 100k points (vector workload) below saturation; "
+                    "latency = submit -> results written"}
+
+
 def search_bench(eng):
     """Config C1 end to end: MSE of 1024 random scalar programs on 400
     points, then the island search (24 islands x 25, the reference's
@@ -418,6 +465,9 @@ def run_engine(args):
     serving = None
     if not args.no_serving:
         serving = serving_bench(eng, args.serving_jobs, args.serving_rate, slots=8)
+    serving_light = None
+    if not args.no_serving:
+        serving_light = serving_light_bench(eng)
     search = None
     if world == 1 and not args.no_search:
         search = search_bench(eng)
@@ -470,6 +520,7 @@ def run_engine(args):
             "programs_on_register_kernel": desc["register_kernel_programs"],
             "programs_on_slot_kernel": desc["slot_kernel_programs"],
             "serving": serving,
+            "serving_below_saturation": serving_light,
             "search": search,
         }
         print(json.dumps(line), flush=True)
