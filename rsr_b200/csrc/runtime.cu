@@ -121,7 +121,11 @@ static constexpr int kRegPathStride = 8;
 // More points per lane amortise the dispatch over more work at the cost of
 // fewer resident tapes per SM.  Gradient of 256 programs x 1M points (matrix
 // workload): 28.8 ms at 40 KB against 33.2 ms at 27 KB and 43 ms at 14 KB.
-static constexpr size_t kGradTapeBudget = 40 * 1024;
+// Uneven workload (2048 programs, 16 datasets), whose longest tapes need
+// more than 40 KB at 4 points per lane: 49.7 ms at 80 KB against 52.6 ms at
+// 40 KB and 81.6 ms at 20 KB; the vector and matrix workloads' tapes fit
+// 40 KB at 4 points and do not change.
+static constexpr size_t kGradTapeBudget = 80 * 1024;
 static constexpr uint64_t kChunkPoints = 4096;   // points per work-item chunk (all P)
 static constexpr uint64_t kStrideAlign = 1024;   // dataset column padding
 static constexpr int kGradSlotDoubles = 33;      // sse + 32 gradient sums
