@@ -10,7 +10,7 @@ from __future__ import annotations
 
 import ctypes as C
 import json
-from typing import Dict, List, Optional, Sequence, Tuple, Union
+from typing import Dict, Optional, Sequence, Tuple, Union
 
 import numpy as np
 

@@ -13,7 +13,7 @@ operation order as the tests compute them.
 """
 from __future__ import annotations
 
-from typing import List, Tuple
+from typing import List
 
 import numpy as np
 

@@ -10,7 +10,7 @@ target bit for bit, so the program's MSE is exactly 0; for the others
 """
 from __future__ import annotations
 
-from typing import Callable, Dict, List, Tuple
+from typing import Dict, Tuple
 
 import numpy as np
 

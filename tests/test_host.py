@@ -15,7 +15,7 @@ from rsr_b200 import evaluator as E
 from rsr_b200 import isa as I
 from rsr_b200 import workloads as W
 from rsr_b200.dataset import Dataset
-from rsr_b200.isa import FLOAT, MAT2, MAT3, VEC2, VEC3, Program, Scalar
+from rsr_b200.isa import FLOAT, VEC2, VEC3, Program, Scalar
 
 ROOT = Path(__file__).resolve().parent.parent
 f32 = np.float32

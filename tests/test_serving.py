@@ -13,7 +13,7 @@ from rsr_b200 import _native as N
 from rsr_b200 import isa as I
 from rsr_b200 import workloads as W
 from rsr_b200.evaluator import Engine
-from rsr_b200.isa import FLOAT, Program
+from rsr_b200.isa import Program
 from rsr_b200.serving import Server
 
 pytestmark = pytest.mark.gpu
