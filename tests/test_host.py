@@ -34,6 +34,15 @@ def test_library_exports_every_declared_symbol():
     assert set(N.exported_symbols()) <= declared
 
 
+def test_rust_bindings_cover_the_header():
+    """The Rust binding a maintainer adds declares every entry point of the
+    header, under the same name, and nothing the header lacks."""
+    header = (ROOT / "include" / "rsr_gpu.h").read_text()
+    declared = set(re.findall(r"RSR_API [^;]*?\b(rsr_\w+)\(", header))
+    rust = set(re.findall(r"pub fn (rsr_\w+)\(", (ROOT / "INTEGRATION.md").read_text()))
+    assert rust == declared, (sorted(declared - rust), sorted(rust - declared))
+
+
 def test_opcode_numbering_matches_device_header():
     text = (ROOT / "rsr_b200" / "csrc" / "uops.h").read_text()
     body = text[text.index("enum Opcode"):text.index("N_OPCODES,")]
