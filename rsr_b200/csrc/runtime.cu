@@ -126,7 +126,10 @@ static constexpr int kRegPathStride = 8;
 // 40 KB and 81.6 ms at 20 KB; the vector and matrix workloads' tapes fit
 // 40 KB at 4 points and do not change.
 static constexpr size_t kGradTapeBudget = 80 * 1024;
-static constexpr uint64_t kChunkPoints = 4096;   // points per work-item chunk (all P)
+// Points per work-item chunk (all P).  8192 measured slower on every kernel
+// (vector register 4.32 ms against 4.30, matrix register 4.84 against 4.69,
+// vector adjoint 6.68 against 5.90): coarser items balance worse.
+static constexpr uint64_t kChunkPoints = 4096;
 static constexpr uint64_t kStrideAlign = 1024;   // dataset column padding
 static constexpr int kGradSlotDoubles = 33;      // sse + 32 gradient sums
 
