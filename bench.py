@@ -15,9 +15,20 @@ CUDA events on the launching stream; multi-GPU runs shard programs across
 ranks (weak scaling, no collective on the data path) and take the max over
 ranks.
 
+The line also carries the other workloads as legs: `matrix` (256 programs
+x 1M points: MSE, MSE + gradient with the adjoint kernel's roofline, a
+20-iteration L-BFGS fit) and `uneven` (8192 programs over 16 datasets of
+400-262,144 points, graph replay), besides the plain-kernel, adjoint,
+end-to-end, serving and search legs.
+
 `--impl reference` times the reference's CPU evaluator in its restated form
 (oracle/simd_baseline.c: the reference Rust crate cannot be built in this
 image) on all host cores, on bounded samples of the same workload.
+
+`--case` runs one fixed evaluation case for profilers instead (`--workload`,
+`--programs`, `--points`, `--kernel register|plain|adjoint`, `--runs`,
+`--points-per-thread`, `--programs-per-warp`): the commands under profiles/
+use it.
 """
 from __future__ import annotations
 
@@ -47,6 +58,22 @@ METRIC = "program_points_per_sec"
 UNIT = "program*points/s"
 N_PROGRAMS = 4096
 N_POINTS = 100_000
+# The workload both arms report (the engine and the reference CPU arm print
+# the same config).
+CONFIG = {"workload": "vector: 4096 programs len 4-48 x 100000 points, y=|E+v x B|",
+          "programs": N_PROGRAMS, "points": N_POINTS,
+          "l2": "engine arm: flushed between steps (256 MiB memset outside the timed events); "
+                "CPU reference arm: no flush"}
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def rank_info():
@@ -165,9 +192,9 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded)",
-            "config": {"workload": "vector: 4096 programs len 4-48 x 100000 points, y=|E+v x B|",
-                       "programs": N_PROGRAMS, "points": N_POINTS, "l2": "n/a (CPU)"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+            "config": dict(CONFIG),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "cpu_model": cpu_model(),
+                             "kind": "port", "sample": sample,
                              "what": "AVX2 8-lane restatement of the reference's compute_mse "
                                      "(oracle/simd_baseline.c); the Rust reference cannot be built here"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -295,6 +322,112 @@ def serving_light_bench(eng, jobs: int = 300, rate: float = 150.0, threads: int 
             "latency_ms": {"p50": st["p50_ms"], "p95": st["p95_ms"], "p99": st["p99_ms"], "max": st["max_ms"]},
             "what": "rsr_server, MSE jobs of 64-1024 programs x 100k points (vector workload) below saturation; "
                     "latency = submit -> results written"}
+
+
+def _replay_ms(eng, b, reps: int, warm: int = 3, results: bool = False):
+    """Device ms per run of a prepared batch (graph replay when the engine
+    uses graphs), L2 flushed before each run."""
+    out = []
+    for i in range(warm + reps):
+        eng.flush_l2()
+        b.run()
+        if results:
+            b.results()
+        t = b.timing()[1]
+        if i >= warm:
+            out.append(t)
+    return out
+
+
+def _group_ms(eng, b, reps: int, warm: int = 3):
+    """Per-launch device ms of a prepared batch on an engine without graphs
+    (CUDA events around each launch): (per-run lists, group descriptions)."""
+    per = []
+    for i in range(warm + reps):
+        eng.flush_l2()
+        b.run()
+        b.timing()
+        if i >= warm:
+            per.append([g["last_ms"] for g in b.describe()["groups"]])
+    return per, b.describe()["groups"]
+
+
+def matrix_bench(eng, eng_nog, fp32_peak: float, reps: int):
+    """The matrix workload with constant fitting: M a Mat3 ~ U(-1, 1), v, u
+    ~ N(0, 1) Vec3, y = |M v - u| over 1,000,000 points; 256 programs of
+    length 8-40 with 1-8 constants.  MSE and MSE + gradient of the whole
+    population (graph replay), the adjoint kernel's lane-op rate against the
+    FP32 peak, and a 20-iteration L-BFGS fit of the differentiable programs."""
+    from rsr_b200 import isa as I
+    from rsr_b200 import workloads as W
+    ds = W.transform_dataset(1_000_000, seed=3)
+    pop = W.transform_population(256, seed=13)
+    pk = I.pack(pop)
+    d = eng.upload(ds)
+    b = eng.prepare(pk, d)
+    mse_ms = _replay_ms(eng, b, reps)
+    pp = b.describe()["program_points"]
+    b.close()
+    bg = eng.prepare(pk, d, gradient=True)
+    adj_ms = _replay_ms(eng, bg, reps, results=True)
+    bg.close()
+    d2 = eng_nog.upload(ds)
+    bg2 = eng_nog.prepare(pk, d2, gradient=True)
+    per, groups = _group_ms(eng_nog, bg2, reps)
+    bg2.close()
+    d2.release()
+    adj = [i for i, g in enumerate(groups) if g["kernel"] == "adjoint"]
+    k_ms = statistics.median([sum(r[i] for i in adj) for r in per])
+    k_flops = sum(groups[i]["flops"] for i in adj)
+    fit = [p for p in pop if p.is_differentiable()]
+    eng.fit_lbfgs(fit[:16], d, max_iterations=2)  # warm-up
+    eng.synchronize()
+    t0 = time.perf_counter()
+    _, fit_mse, stats = eng.fit_lbfgs(fit, d, max_iterations=20)
+    fit_s = time.perf_counter() - t0
+    d.release()
+    return {"workload": "matrix: 256 programs len 8-40, 1-8 constants x 1000000 points, y=|M v - u|",
+            "mse": {"ms_per_step": float(np.median(mse_ms)), "value": pp / (np.median(mse_ms) * 1e-3),
+                    "unit": UNIT},
+            "adjoint": {"ms_per_step": float(np.median(adj_ms)), "value": pp / (np.median(adj_ms) * 1e-3),
+                        "unit": UNIT, "over_mse": float(np.median(adj_ms) / np.median(mse_ms)),
+                        "what": "MSE and d(MSE)/d(constants) of all 256 programs, graph replay"},
+            "adjoint_roofline": {"bound": "fp32", "achieved": k_flops / (k_ms * 1e-3) / 1e12,
+                                 "peak": fp32_peak / 1e12, "unit": "TFLOP/s",
+                                 "frac": k_flops / (k_ms * 1e-3) / fp32_peak, "kernel_ms": k_ms,
+                                 "algorithmic_lane_ops": k_flops, "launches": len(adj),
+                                 "what": "forward + reverse-rule lane-ops of the live trees (encoder.cpp "
+                                         "reverse_flops) over the adjoint launches' CUDA-event time"},
+            "lbfgs_20": {"programs": len(fit), "seconds": fit_s, "iterations": stats["iterations"],
+                         "gradient_launches": stats["gradient_evaluations"],
+                         "mse_launches": stats["mse_evaluations"],
+                         "mean_final_mse": float(np.mean(fit_mse[fit_mse < np.finfo(np.float32).max]))}}
+
+
+def uneven_bench(eng, reps: int):
+    """The uneven batch: A, B Mat2 (A = 2I + U(-0.5, 0.5), B ~ N(0, 1)),
+    y = Tr(A^-1 B) + det(A); 8192 programs of length 4-64 against 16 datasets
+    of 400 to 262,144 points (log-uniform), one autotuned launch set replayed
+    through a CUDA graph."""
+    from rsr_b200 import isa as I
+    from rsr_b200 import workloads as W
+    sizes = W.uneven_sizes(16)
+    dd = [eng.upload(W.inverse_dataset(n, seed=100 + i)) for i, n in enumerate(sizes)]
+    pop = W.inverse_population(8192, seed=14)
+    which = np.random.default_rng(5).integers(0, 16, len(pop))
+    pk = I.pack(pop)
+    handles = [dd[k] for k in which]
+    tune = eng.autotune(pk, datasets=handles, reps=2)
+    b = eng.prepare(pk, datasets=handles)
+    ms = _replay_ms(eng, b, reps)
+    pp = b.describe()["program_points"]
+    b.close()
+    for x in dd:
+        x.release()
+    return {"workload": "uneven: 8192 programs len 4-64 over 16 datasets of 400-262144 points, "
+                        "y=Tr(A^-1 B)+det(A)",
+            "ms_per_step": float(np.median(ms)), "value": pp / (np.median(ms) * 1e-3), "unit": UNIT,
+            "program_points": pp, "autotune": tune["chosen"]}
 
 
 def search_bench(eng):
@@ -462,6 +595,11 @@ def run_engine(args):
     e2e_value = pp_rank * world * len(e2e_ms) / (max_over_ranks(sum(e2e_ms)) * 1e-3)
     assert np.array_equal(out, mse_ref)
 
+    matrix = uneven = None
+    if not args.no_configs:
+        matrix = matrix_bench(eng, eng2, fp32_peak, max(3, min(args.steps, 10)))
+        uneven = uneven_bench(eng, max(3, min(args.steps, 10)))
+
     serving = None
     if not args.no_serving:
         serving = serving_bench(eng, args.serving_jobs, args.serving_rate, slots=8)
@@ -477,17 +615,18 @@ def run_engine(args):
         cpu = None
         if world == 1 and not args.no_cpu:
             v, cores, sample = cpu_baseline(lambda n: I.pack(pop[:n]), ds)
-            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "cpu_model": cpu_model(), "kind": "port",
+                   "sample": sample,
+                   "what": "AVX2 8-lane restatement of the reference's compute_mse (oracle/simd_baseline.c) on "
+                           "all host threads; the Rust reference cannot be built here"}
         achieved = dom_flops / (dom_ms * 1e-3) / 1e12
         peak = fp32_peak / 1e12
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / len(step_ms), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": "vector: 4096 programs len 4-48 x 100000 points, y=|E+v x B|",
-                       "programs_per_gpu": N_PROGRAMS, "points": N_POINTS,
-                       "kernel": "register-stack persistent, CUDA graph replay",
-                       "l2": "flushed between steps (256 MiB memset outside the timed events)"},
+            "config": dict(CONFIG),
+            "kernel": "register-stack persistent, CUDA graph replay; programs per GPU = config.programs",
             "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                            "max": float(max(step_ms))},
             "adjoint": {"value": adj_value, "unit": UNIT, "ms_per_step": float(np.median(ams)),
@@ -519,6 +658,8 @@ def run_engine(args):
             "autotune": tune["chosen"],
             "programs_on_register_kernel": desc["register_kernel_programs"],
             "programs_on_slot_kernel": desc["slot_kernel_programs"],
+            "matrix": matrix,
+            "uneven": uneven,
             "serving": serving,
             "serving_below_saturation": serving_light,
             "search": search,
@@ -532,6 +673,49 @@ def run_engine(args):
     return 0
 
 
+def run_case(args):
+    """One fixed evaluation case for profilers (ncu), one kernel kind at a
+    time: a prepared batch of the chosen workload run `--runs` times without
+    a CUDA graph (every kernel its own launch); prints the per-launch CUDA
+    event times.  Workloads: scalar (400 points), vector (100k points),
+    matrix (1M points), uneven (16 datasets of 400-262,144 points)."""
+    from rsr_b200 import _native as N
+    from rsr_b200 import isa as I
+    from rsr_b200 import workloads as W
+    from rsr_b200.evaluator import Engine
+    eng = Engine(use_graphs=False, points_per_thread=args.points_per_thread,
+                 programs_per_warp=args.programs_per_warp)
+    if args.workload == "scalar":
+        ds, pop = W.scalar_dataset(args.points or 400, seed=1), W.scalar_population(args.programs, seed=11)
+    elif args.workload == "vector":
+        ds, pop = W.lorentz_dataset(args.points or N_POINTS, seed=2), W.lorentz_population(args.programs, seed=12)
+    elif args.workload == "matrix":
+        ds, pop = (W.transform_dataset(args.points or 1_000_000, seed=3),
+                   W.transform_population(args.programs, seed=13))
+    else:
+        ds, pop = None, W.inverse_population(args.programs, seed=14)
+    pk = I.pack(pop)
+    kernel = N.KERNEL_PLAIN if args.kernel == "plain" else N.KERNEL_AUTO
+    grad = args.kernel == "adjoint"
+    if ds is None:
+        dss = [eng.upload(W.inverse_dataset(n, seed=100 + i)) for i, n in enumerate(W.uneven_sizes(16))]
+        which = np.random.default_rng(5).integers(0, 16, pk.n)
+        b = eng.prepare(pk, datasets=[dss[int(k)] for k in which], kernel=kernel, gradient=grad)
+    else:
+        b = eng.prepare(pk, eng.upload(ds), kernel=kernel, gradient=grad)
+    for _ in range(args.runs):
+        b.run()
+        b.timing()
+    d = b.describe()
+    print(json.dumps({"workload": args.workload, "programs": pk.n, "kernel": args.kernel,
+                      "groups": [{k: g[k] for k in ("kernel", "profile", "points_per_thread", "programs_per_warp",
+                                                    "grid", "warps_per_block", "smem_bytes", "last_ms", "flops",
+                                                    "program_points")} for g in d["groups"]]}))
+    b.close()
+    eng.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -541,11 +725,23 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-mix leg")
     ap.add_argument("--no-search", action="store_true", help="skip the GP-search leg (config C1)")
+    ap.add_argument("--no-configs", action="store_true", help="skip the matrix and uneven workload legs")
     ap.add_argument("--serving-jobs", type=int, default=400)
+    ap.add_argument("--case", action="store_true",
+                    help="run one fixed evaluation case for profilers instead of the benchmark (below)")
+    ap.add_argument("--workload", default="vector", choices=["scalar", "vector", "matrix", "uneven"])
+    ap.add_argument("--programs", type=int, default=1024)
+    ap.add_argument("--points", type=int, default=0, help="--case: override the workload's point count")
+    ap.add_argument("--kernel", default="register", choices=["register", "plain", "adjoint"])
+    ap.add_argument("--runs", type=int, default=3)
+    ap.add_argument("--points-per-thread", type=int, default=0, help="--case: register kernel P (0: tuned)")
+    ap.add_argument("--programs-per-warp", type=int, default=0, help="--case: register kernel G (0: tuned)")
     ap.add_argument("--serving-rate", type=float, default=2000.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.case:
+        return run_case(args)
     return run_reference(args) if args.impl == "reference" else run_engine(args)
 
 

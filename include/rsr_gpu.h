@@ -168,8 +168,10 @@ RSR_API int rsr_eval_points_batch(rsr_ctx *ctx, const rsr_population *pop, rsr_d
  * so the program is limited to 512 instructions and 1024 constants /
  * parameter floats, and the dataset to 16,777,216 points; larger inputs
  * return RSR_EINVAL.  The first call on a device takes the array's address
- * (cudaGetSymbolAddress, with the device current) and should come before any
- * stream capture on that device.  Calls that overlap in time on one device
+ * (cudaGetSymbolAddress, with the device current) and loads every kernel the
+ * entry point launches (lazy module loading would otherwise allocate on a
+ * kernel's first launch); it should come before any stream capture on that
+ * device.  Calls after it allocate no device memory.  Calls that overlap in time on one device
  * through different contexts race on the array.  The dataset must already
  * be resident (rsr_dataset_upload). */
 RSR_API int rsr_compute_mse_noalloc(rsr_ctx *ctx, const rsr_program *prog, rsr_dataset ds, float *mse);

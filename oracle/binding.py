@@ -47,6 +47,8 @@ def lib() -> C.CDLL:
         L.orc_mse_f64.argtypes = PROG + DS
         L.orc_mse_grad_dual.restype = C.c_float
         L.orc_mse_grad_dual.argtypes = PROG + DS + [f32p]
+        L.orc_grad_dual_f64.restype = C.c_double
+        L.orc_grad_dual_f64.argtypes = PROG + DS + [f64p, f64p]
         L.orc_grad_fd.restype = None
         L.orc_grad_fd.argtypes = PROG + DS + [C.c_double, f64p]
         L.orc_mse_batch.restype = None
@@ -121,6 +123,17 @@ def mse_grad_dual(p, ds):
     g = np.zeros(32, np.float32)
     m = lib().orc_mse_grad_dual(*a, *d, ds.num_samples, _p(g, f32p))
     return float(m), g
+
+
+def grad_dual_f64(p, ds):
+    """(f64 MSE, gradient, per-component L1 scale): the reference's dual
+    rules per point, sums over points in f64 (orc_grad_dual_f64)."""
+    a, k = _prog(p)
+    d, k2 = _ds(ds)
+    g = np.zeros(32, np.float64)
+    l1 = np.zeros(32, np.float64)
+    m = lib().orc_grad_dual_f64(*a, *d, ds.num_samples, _p(g, f64p), _p(l1, f64p))
+    return float(m), g, l1
 
 
 def grad_fd(p, ds, h: float = 1e-3) -> np.ndarray:

@@ -590,6 +590,51 @@ ORC_API void orc_grad_fd(const uint32_t *code, uint32_t len, const uint8_t *kind
     free(q);
 }
 
+/* The dual-number gradient of orc_mse_grad_dual (the reference's per-point
+ * rules, evaluator.rs:228-388, in f32) with the sums over points taken in
+ * f64 instead of per-lane f32, for datasets of a million points where the
+ * reference's f32 accumulation would add noise of its own.  Also returns,
+ * per flat parameter k, the L1 scale of the sum: l1[k] = sum |2 diff_i
+ * dpred_i/dtheta_k| / num_samples.  A component whose value is small
+ * against its L1 scale is a cancellation of large per-point terms, and an
+ * f32 evaluation of it cannot be resolved below that scale times the
+ * per-point rounding.  Returns the f64 MSE. */
+ORC_API double orc_grad_dual_f64(const uint32_t *code, uint32_t len, const uint8_t *kinds, uint32_t nk,
+                                 const float *params, uint32_t np, const float *feature_flat, const float *target,
+                                 uint32_t nf, uint64_t nbatch, uint64_t nsamples, double *grad, double *l1) {
+    prog_t p = mkprog(code, len, kinds, nk, params, np);
+    uint32_t P = np < 32 ? np : 32;
+    for (int k = 0; k < 32; ++k) grad[k] = l1[k] = 0.0;
+    double sse = 0.0;
+    float feat[256];
+    for (uint64_t b = 0; b < nbatch; ++b)
+        for (int l = 0; l < 8; ++l) {
+            for (uint32_t f = 0; f < nf; ++f) feat[f] = feature_flat[(b * nf + f) * 8 + l];
+            if (P == 0) {
+                double d = (double)eval_point(&p, feat) - (double)target[b * 8 + l];
+                sse += d * d;
+                continue;
+            }
+            float diff = 0.0f;
+            for (uint32_t k = 0; k < P; ++k) {
+                dual r = eval_point_dual(&p, feat, k);
+                if (k == 0) {
+                    diff = r.v - target[b * 8 + l];
+                    sse += (double)diff * (double)diff;
+                }
+                const double t = (2.0 * (double)diff) * (double)r.g;
+                grad[k] += t;
+                l1[k] += fabs(t);
+            }
+        }
+    const double n = (double)nsamples;
+    for (uint32_t k = 0; k < P; ++k) {
+        grad[k] /= n;
+        l1[k] /= n;
+    }
+    return sse / n;
+}
+
 /* ---------------------------------------------- batched, multi-threaded */
 /* Packed population: code/kinds/params concatenated with offset arrays of
  * n+1 entries.  Used by tests at sizes where a Python loop would be slow. */

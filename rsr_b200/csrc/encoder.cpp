@@ -60,6 +60,58 @@ const SigTable &sigs() {
 
 constexpr int kKindWidth[7] = {1, 0, 0, 2, 3, 4, 9};
 constexpr int kMseEpilogueFlops = 3;
+// Reverse sweep of the MSE epilogue: the seed 2 (pred - y) (multiply; the
+// difference is the forward pass's).
+constexpr int kMseEpilogueRevFlops = 1;
+
+// Unfused FP32 lane-ops of each opcode's reverse rule (the adjoint kernel's
+// work beside the forward pass), counted from the rules: one multiply per
+// product term and one add per adjoint accumulation.  E.g. MulF: ga += g b,
+// gb += g a (4); DivF: q = g / b, ga += q, gb -= q * out (4 + the divide);
+// CrossV3: ga += b x g, gb += g x a (2 x (9 + 3)); MulM3V3: gM += g v^T
+// (9 + 9), gv += M^T g (15 + 3); InverseM3: gA -= X^T G X^T with X the
+// inverse (2 x 45 + 9).  A LoadConst adds its adjoint into the parameter
+// sums (one add per component); a LoadVar's adjoint is dropped (0).
+int reverse_flops(int op, int const_width) {
+    switch (op) {
+        case LOAD_CONST_F: case LOAD_CONST_V2: case LOAD_CONST_V3: case LOAD_CONST_M2: case LOAD_CONST_M3:
+            return const_width;
+        case ADD_F: case SUB_F: return 2;
+        case MUL_F: return 4;
+        case DIV_F: return 5;
+        case SIN_F: case COS_F: case SQR_F: case SQRT_F: return 3;
+        case EXP_F: case LN_F: return 2;
+        case MAKE_VEC2: return 2;
+        case MAKE_VEC3: return 3;
+        case GET_X_V2: case GET_Y_V2: case GET_X_V3: case GET_Y_V3: case GET_Z_V3: return 1;
+        case ADD_V2: case SUB_V2: return 4;
+        case ADD_V3: case SUB_V3: return 6;
+        case MAKE_MAT2: case TRANSPOSE_M2: return 4;
+        case ADD_M2: case SUB_M2: return 8;
+        case ADD_M3: case SUB_M3: return 18;
+        case MAKE_MAT3: case TRANSPOSE_M3: return 9;
+        case SCALE_V2: return 8;
+        case SCALE_V3: return 12;
+        case SCALE_M2: return 16;
+        case SCALE_M3: return 36;
+        case DOT_V2: return 8;
+        case DOT_V3: return 12;
+        case NORM_V2: return 5;
+        case NORM_V3: return 7;
+        case CROSS_V3: return 24;
+        case MUL_M2: return 32;
+        case MUL_M3: return 108;
+        case MUL_M2V2: return 16;
+        case MUL_M3V3: return 36;
+        case DET_M2: return 8;
+        case DET_M3: return 45;
+        case TRACE_M2: return 2;
+        case TRACE_M3: return 3;
+        case INVERSE_M2: return 28;
+        case INVERSE_M3: return 99;
+        default: return 0;
+    }
+}
 
 struct Node {
     int opcode = 0;
@@ -681,15 +733,18 @@ int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uin
             if (n.stale && n.alias >= 0) work.push_back(n.alias);
         }
     }
-    uint32_t flops = 0;
+    uint32_t flops = 0, rev_flops = 0;
     bool has_stale_live = false;
     for (size_t i = 0; i < nodes.size(); ++i) {
         if (!live[i]) continue;
         flops += op_sig(nodes[i].opcode).flops;
+        rev_flops += (uint32_t)reverse_flops(nodes[i].opcode, is_const_load(nodes[i].opcode) && !nodes[i].stale
+                                                                   ? kStackWidth[nodes[i].out] : 0);
         if (nodes[i].opcode == INVERSE_M2 || nodes[i].opcode == INVERSE_M3) E.differentiable = false;
         if (nodes[i].stale) has_stale_live = true;
     }
     E.flops_per_point = flops + kMseEpilogueFlops;
+    E.adj_flops_per_point = E.flops_per_point + rev_flops + kMseEpilogueRevFlops;
     {
         uint32_t types = 1u << SF;
         for (size_t i = 0; i < nodes.size(); ++i)

@@ -31,6 +31,7 @@ struct EncodedProgram {
     uint32_t n_params = 0;
     std::vector<float> consts;            // flat parameters (kernel constant pool)
     uint32_t flops_per_point = 0;         // incl. MSE epilogue
+    uint32_t adj_flops_per_point = 0;     // forward + reverse sweep (adjoint kernel), incl. epilogues
     bool differentiable = true;
     bool result_zero = false;             // stack_f[0] is never written
     int depth_ref[N_STACKS] = {0, 0, 0, 0, 0};

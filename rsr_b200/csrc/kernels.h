@@ -14,6 +14,9 @@ constexpr int kGradThreads = 32;  // one warp per block, one item per warp
 
 cudaError_t launch_plain(const LaunchArgs &a, int P, uint32_t warps_per_block, size_t smem, cudaStream_t st);
 size_t plain_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t slots, int P);
+// Loads the slot-file kernel's variants and the MSE epilogue ahead of their
+// first real launch (lazy module loading), with empty launches on st.
+cudaError_t preload_plain_mse(cudaStream_t st);
 cudaError_t launch_aosoa_to_soa(const float *ff, const float *tb, float *x, float *y, uint32_t nf, uint64_t nbatch,
                                 uint64_t stride, int num_sms, cudaStream_t st);
 cudaError_t measure_fp32_peak(int num_sms, cudaStream_t st, double *lane_ops_per_s);

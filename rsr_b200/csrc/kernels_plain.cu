@@ -214,6 +214,34 @@ size_t plain_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t 
     return ((size_t)align4u(code_words) + align4u(const_floats) + (size_t)slots * 32u * P) * 4u;
 }
 
+// With lazy module loading (the default since CUDA 12.2) a kernel's code is
+// loaded, and device memory taken for it and for its local memory, on its
+// first launch.  This loads every point-count variant of the slot-file
+// kernel and the MSE epilogue ahead of time: each is looked up
+// (cudaFuncGetAttributes) and launched once with no work (no items, no
+// programs), which returns at once.
+cudaError_t preload_plain_mse(cudaStream_t st) {
+    cudaFuncAttributes fa;
+    cudaError_t e;
+    if ((e = cudaFuncGetAttributes(&fa, plain_eval_kernel<1>)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&fa, plain_eval_kernel<2>)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&fa, plain_eval_kernel<4>)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&fa, finalize_mse_kernel)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(plain_eval_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kMaxDynSmemOptin)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(plain_eval_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kMaxDynSmemOptin)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(plain_eval_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kMaxDynSmemOptin)) != cudaSuccess)
+        return e;
+    LaunchArgs none{};  // n_items = 0: every warp returns before reading anything
+    plain_eval_kernel<1><<<1, 32, 0, st>>>(none);
+    plain_eval_kernel<2><<<1, 32, 0, st>>>(none);
+    plain_eval_kernel<4><<<1, 32, 0, st>>>(none);
+    finalize_mse_kernel<<<1, 32, 0, st>>>(nullptr, nullptr, nullptr, 0u, nullptr);  // n_progs = 0
+    return cudaGetLastError();
+}
+
 cudaError_t launch_aosoa_to_soa(const float *ff, const float *tb, float *x, float *y, uint32_t nf, uint64_t nbatch,
                                 uint64_t stride, int num_sms, cudaStream_t st) {
     const uint64_t n = nbatch * 8;

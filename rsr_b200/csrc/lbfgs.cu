@@ -1,4 +1,4 @@
-// lbfgs.cpp -- batched L-BFGS constant fitting on the engine's gradient.
+// lbfgs.cu -- batched L-BFGS constant fitting on the engine's gradient.
 //
 // Restates run_lbfgs (src/engine/optimize/lbfgs.rs:9-165) for a whole
 // population at once: every program keeps its own L-BFGS state (memory 6,

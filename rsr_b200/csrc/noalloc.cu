@@ -5,8 +5,10 @@
 // constants, work items, per-chunk partial sums and the result -- in one
 // file-scope __device__ array of kNoAllocScratchBytes.  Its address is taken
 // with cudaGetSymbolAddress once per device, with that device current, on the
-// first call for the device; that first call should come before any stream
-// capture on the device.  After it, a call performs no cudaMalloc/cudaFree,
+// first call for the device, which also loads every kernel the entry point
+// launches (lazy module loading would otherwise allocate on a kernel's first
+// launch); that first call should come before any stream capture on the
+// device.  After it, a call performs no cudaMalloc/cudaFree,
 // no pinned-host or managed allocation and no C++ heap allocation on its
 // success path: the program is encoded into fixed-size arrays on the host
 // stack, copied into the scratch array with one cudaMemcpyAsync, and the
@@ -169,14 +171,24 @@ int encode_slots_fixed(const rsr_program &p, uint32_t num_features, uint32_t *wo
     return RSR_OK;
 }
 
-// Scratch address of the current device, taken once.
-int scratch_for(int device, unsigned char **out) {
+// Set-up of the current device, once: the scratch array's address, and every
+// kernel this entry point launches loaded ahead of its first real use (with
+// lazy module loading a kernel's code and local memory are allocated on its
+// first launch), so that no later call allocates.
+int scratch_for(int device, cudaStream_t st, unsigned char **out) {
     if (device < 0 || device >= kMaxDevices) return fail(RSR_EINVAL, "device ordinal out of range");
     std::lock_guard<std::mutex> lk(g_setup_mu);
     if (!g_scratch[device]) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(noalloc scratch)");
+        cudaFuncAttributes fa;
+        if ((e = cudaFuncGetAttributes(&fa, noalloc_items_kernel)) != cudaSuccess)
+            return cuda_fail(e, "noalloc kernel load");
+        noalloc_items_kernel<<<1, 32, 0, st>>>(nullptr, 0u, 0u, 1u);  // no chunks: returns at once
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "noalloc kernel load");
+        if ((e = preload_plain_mse(st)) != cudaSuccess) return cuda_fail(e, "noalloc kernel load");
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "noalloc kernel load");
         g_scratch[device] = static_cast<unsigned char *>(p);
     }
     *out = g_scratch[device];
@@ -194,7 +206,7 @@ extern "C" int rsr_compute_mse_noalloc(rsr_ctx *ctx, const rsr_program *prog, rs
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
     unsigned char *scratch = nullptr;
-    int rc = scratch_for(ctx->device, &scratch);
+    int rc = scratch_for(ctx->device, ctx->stream, &scratch);
     if (rc) return rc;
     auto it = ctx->datasets.find(ds);
     if (it == ctx->datasets.end()) return fail(RSR_ENOTFOUND, "unknown dataset handle");

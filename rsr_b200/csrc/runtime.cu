@@ -334,7 +334,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         P.code.insert(P.code.end(), code.begin(), code.end());
         P.consts.insert(P.consts.end(), E.consts.begin(), E.consts.end());
         P.progs[li] = d;
-        P.flops += (uint64_t)E.flops_per_point * n_eval;
+        P.flops += (uint64_t)(gradient ? E.adj_flops_per_point : E.flops_per_point) * n_eval;
         P.program_points += n_eval;
     }
     P.n_partials = part * (gradient ? kGradSlotDoubles : 1);
@@ -437,7 +437,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         for (uint32_t q = li; q < end; ++q) {
             const EncodedProgram &E = enc[order[q]];
             const uint64_t ne = P.datasets[P.progs[q].dataset].n_eval;
-            g.flops += (uint64_t)E.flops_per_point * ne;
+            g.flops += (uint64_t)(gradient ? E.adj_flops_per_point : E.flops_per_point) * ne;
             g.program_points += ne;
         }
         P.groups.push_back(g);
@@ -881,7 +881,8 @@ static int upload_soa(rsr_ctx *ctx, const float *ff, const float *tb, bool aosoa
         e = launch_aosoa_to_soa((const float *)tmp, (const float *)((char *)tmp + rawx), rec->x, rec->y, nf, nbatch,
                                 stride, ctx->num_sms, ctx->stream);
         ctx->launches++;
-        cudaStreamSynchronize(ctx->stream);
+        const cudaError_t se = cudaStreamSynchronize(ctx->stream);
+        if (e == cudaSuccess) e = se;
         cudaFree(tmp);
     } else {
         // columns: features[f*n + i] with n = nsamples, zero padded

@@ -34,13 +34,84 @@ def test_library_exports_every_declared_symbol():
     assert set(N.exported_symbols()) <= declared
 
 
-def test_rust_bindings_cover_the_header():
-    """The Rust binding a maintainer adds declares every entry point of the
-    header, under the same name, and nothing the header lacks."""
+_C_SCALAR = {"int": "c_int", "uint32_t": "u32", "int32_t": "i32", "uint64_t": "u64", "double": "f64",
+             "float": "f32", "size_t": "usize", "char": "c_char", "uint8_t": "u8", "rsr_dataset": "RsrDataset"}
+
+
+def _rust_type(c: str) -> str:
+    """The Rust spelling of a C parameter or field type of the header."""
+    c = " ".join(c.replace("*", " * ").split())
+    stars = c.count("*")
+    base = c.replace("*", "").replace("const", "").strip()
+    rust = _C_SCALAR.get(base) or "Rsr" + "".join(w.capitalize() for w in base[len("rsr_"):].split("_"))
+    if stars == 0:
+        return rust
+    first = "*const " if c.startswith("const") else "*mut "
+    return first + "*mut " * (stars - 1) + rust
+
+
+def _c_functions():
     header = (ROOT / "include" / "rsr_gpu.h").read_text()
-    declared = set(re.findall(r"RSR_API [^;]*?\b(rsr_\w+)\(", header))
-    rust = set(re.findall(r"pub fn (rsr_\w+)\(", (ROOT / "INTEGRATION.md").read_text()))
-    assert rust == declared, (sorted(declared - rust), sorted(rust - declared))
+    out = {}
+    for ret, name, args in re.findall(r"RSR_API ([^;]*?)\b(rsr_\w+)\(([^;]*?)\);", header, re.S):
+        params = [] if args.strip() == "void" else [" ".join(a.split()) for a in args.split(",")]
+        types = []
+        for a in params:
+            m = re.match(r"(.*?)(\w+)$", a)
+            types.append(_rust_type(m.group(1)))
+        r = " ".join(ret.split())
+        out[name] = (types, None if r == "void" else _rust_type(r))
+    return out
+
+
+def _rust_functions():
+    text = (ROOT / "integration" / "rust" / "gpu.rs").read_text()
+    out = {}
+    for name, args, ret in re.findall(r"pub fn (rsr_\w+)\(([^)]*)\)\s*(?:->\s*([^;{]+?))?\s*;", text, re.S):
+        types = [" ".join(a.split(":", 1)[1].split()) for a in args.split(",") if a.strip()]
+        out[name] = (types, " ".join(ret.split()) if ret else None)
+    return out
+
+
+def test_rust_bindings_cover_the_header():
+    """The Rust binding a maintainer adds (integration/rust/gpu.rs) declares
+    every entry point of the header under the same name, with the same
+    parameter and return types, and nothing the header lacks."""
+    c, rust = _c_functions(), _rust_functions()
+    assert set(rust) == set(c), (sorted(set(c) - set(rust)), sorted(set(rust) - set(c)))
+    for name in c:
+        assert rust[name] == c[name], (name, rust[name], c[name])
+
+
+def test_rust_structs_mirror_the_header():
+    """Every struct of the header has a #[repr(C)] Rust mirror with the same
+    fields, in order, of the same types."""
+    header = (ROOT / "include" / "rsr_gpu.h").read_text()
+    text = (ROOT / "integration" / "rust" / "gpu.rs").read_text()
+    structs = re.findall(r"typedef struct (rsr_\w+) \{(.*?)\} \1;", header, re.S)
+    assert len(structs) >= 9
+    for cname, body in structs:
+        fields = []
+        for decl in re.sub(r"/\*.*?\*/", "", body, flags=re.S).split(";"):
+            decl = " ".join(decl.split())
+            if not decl:
+                continue
+            m = re.match(r"((?:const )?\w+ \**)\s*(.*)$", decl)
+            ctype, names = m.group(1), m.group(2)
+            for n in names.split(","):
+                n = n.strip()
+                arr = re.match(r"(\w+)\[(\d+)\]", n)
+                if arr:
+                    fields.append((arr.group(1), f"[{_rust_type(ctype)}; {arr.group(2)}]"))
+                else:
+                    stars = n.count("*")
+                    fields.append((n.strip("* "), _rust_type(ctype + "*" * stars)))
+        rname = _rust_type(cname)
+        m = re.search(r"#\[repr\(C\)\]\s*pub struct " + rname + r" \{(.*?)\}", text, re.S)
+        assert m, rname
+        rfields = [(f.split(":")[0].replace("pub", "").strip(), " ".join(f.split(":", 1)[1].split()))
+                   for f in m.group(1).split(",") if ":" in f]
+        assert rfields == fields, (cname, rfields, fields)
 
 
 def test_opcode_numbering_matches_device_header():

@@ -164,3 +164,26 @@ def test_simd_baseline_matches_oracle_mse():
     m64, m32 = O.mse_batch(pk, ds, threads=4)
     simd = O.simd_mse_batch(pk, ds, threads=4)
     assert np.array_equal(simd, m32)
+
+
+def test_dual_gradient_with_f64_sums_and_l1_scale():
+    """orc_grad_dual_f64 applies the same per-point dual rules as
+    orc_mse_grad_dual and differs only in summing over points in f64; its L1
+    scale bounds the gradient's magnitude."""
+    from rsr_b200 import workloads as W
+    ds = W.transform_dataset(4000, seed=91)
+    checked = 0
+    for p in W.transform_population(40, seed=92):
+        md, gd = O.mse_grad_dual(p, ds)
+        m64, g64, l1 = O.grad_dual_f64(p, ds)
+        n = min(32, p.param_count())
+        if not (np.isfinite(gd[:n]).all() and np.isfinite(m64) and m64 < 1e4):
+            continue
+        # the value of the dual pass may differ from the plain pass by an ulp
+        # in a few points (as the reference's does)
+        assert abs(m64 - O.mse_f64(p, ds)) <= 1e-7 * max(1e-3, m64)
+        assert np.all(np.abs(g64[:n]) <= l1[:n] * (1 + 1e-12))
+        assert np.all(np.abs(gd[:n] - g64[:n]) <= 1e-5 * l1[:n] + 1e-30)
+        assert np.all(g64[n:] == 0) and np.all(l1[n:] == 0)
+        checked += 1
+    assert checked >= 10
