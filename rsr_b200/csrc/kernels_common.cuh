@@ -23,6 +23,8 @@ struct LaunchArgs {
     uint32_t *item_counter;   // persistent kernels: next work item
     uint32_t *status;         // sticky error flags (bit 0: bad micro-op)
     const uint8_t *active;    // optional per-program mask (launch order): 0 = skip
+    const uint32_t *run_if;   // optional: the launch does nothing when *run_if == 0 (device-side
+                              // loops whose later rounds may have no work, e.g. line searches)
     uint32_t n_items;
     uint32_t mode;
     uint32_t smem_code_words; // per warp

@@ -384,6 +384,7 @@ __global__ void __launch_bounds__(kGradThreads, 16) grad_kernel(const LaunchArgs
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t item_id = blockIdx.x * (blockDim.x >> 5) + warp;
     if (item_id >= a.n_items) return;
+    if (a.run_if && *a.run_if == 0u) return;
     const uint32_t cw = align4g(a.smem_code_words), cf = align4g(a.smem_const_floats);
     const uint32_t gp = min(kGradParams, a.smem_const_floats);
     const uint32_t region = cw + cf + gp * 32u + (a.smem_slots + a.smem_adj_slots) * 32u * P;

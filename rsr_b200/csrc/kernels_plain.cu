@@ -122,6 +122,7 @@ __global__ void __launch_bounds__(kPlainThreads) plain_eval_kernel(const LaunchA
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t item_id = blockIdx.x * (blockDim.x >> 5) + warp;
     if (item_id >= a.n_items) return;
+    if (a.run_if && *a.run_if == 0u) return;
     const uint32_t region = align4u(a.smem_code_words) + align4u(a.smem_const_floats) + a.smem_slots * 32u * P;
     float *base = smem + (size_t)warp * region;
     uint32_t *scode = reinterpret_cast<uint32_t *>(base);

@@ -360,6 +360,7 @@ constexpr int reg_min_blocks() {
 template <int PROF, int P, int OMIT>
 __global__ void __launch_bounds__(kRegThreads, reg_min_blocks<PROF, P, OMIT>()) reg_eval_kernel(const LaunchArgs a) {
     extern __shared__ __align__(16) float smem[];
+    if (a.run_if && *a.run_if == 0u) return;  // the same for every thread of the launch
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nw = blockDim.x >> 5;
     uint32_t *scode = reinterpret_cast<uint32_t *>(smem);

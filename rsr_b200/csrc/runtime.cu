@@ -26,10 +26,19 @@ int cuda_fail(cudaError_t e, const char *what) {
                 std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Growth is geometric below 64 MB (at least 1.5x the old capacity): a buffer
+// reused by calls of slowly growing size is reallocated a few times, not at
+// every call, and each cudaFree of the old buffer synchronises the device.
+static size_t grow_to(size_t bytes, size_t cap, size_t floor) {
+    size_t want = std::max(bytes, floor);
+    if (cap && want < ((size_t)64 << 20)) want = std::max(want, std::min(cap + cap / 2, (size_t)64 << 20));
+    return want;
+}
+
 cudaError_t DevBuf::reserve(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
+    const size_t want = grow_to(bytes, cap, 256);
     release();
-    size_t want = std::max<size_t>(bytes, 256);
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
         p = nullptr;
@@ -47,8 +56,8 @@ void DevBuf::release() {
 
 cudaError_t HostBuf::reserve(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
+    const size_t want = grow_to(bytes, cap, (size_t)1 << 20);
     release();
-    size_t want = std::max<size_t>(bytes, 1 << 20);
     cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
     if (e != cudaSuccess) {
         p = nullptr;
@@ -234,9 +243,11 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
     for (uint32_t i = 0; i < n; ++i) {
         if (gradient) {
             // adjoint launches by tape size, so that a block's shared memory
-            // follows its own programs' tapes: <= 32, 64, 128, 256, more slots
+            // follows its own programs' tapes: steps of 16 slots up to 256,
+            // then <= 512 and more (a launch sizes every warp's tape for its
+            // largest program, and a finer step packs more tapes per SM)
             const uint32_t nt = enc[i].n_tape_val + enc[i].n_tape_adj;
-            const int bucket = nt <= 32 ? 0 : nt <= 64 ? 1 : nt <= 128 ? 2 : nt <= 256 ? 3 : 4;
+            const int bucket = nt <= 256 ? (int)((nt + 15) / 16) : nt <= 512 ? 17 : 18;
             // Points per lane: the most (4, 2, 1) whose tape fits
             // kGradTapeBudget, decided from the program alone, so that its
             // sums do not depend on the other programs of the call.

@@ -241,6 +241,8 @@ rsr_dataset register_dataset(rsr_ctx *ctx, std::unique_ptr<DatasetRec> rec);
 struct FitWorkspace {
     DevicePlan grad, mse;
     DevBuf grad_active, mse_active;
+    DevBuf lbfgs_state;   // device-resident L-BFGS state of every program (lbfgs.cu)
+    HostBuf lbfgs_counts; // pinned copy of the per-iteration counters
 };
 int fit_population(rsr_ctx *ctx, const rsr_population *pop, const uint64_t *dsp, uint64_t ds,
                    uint32_t max_iterations, cudaStream_t stream, std::mutex *plan_mu,
