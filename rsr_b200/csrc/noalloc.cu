@@ -196,6 +196,16 @@ int scratch_for(int device, cudaStream_t st, unsigned char **out) {
 }
 
 }  // namespace
+
+// The fixed-array slot encoder behind a diagnostic entry point
+// (rsr_program_encoding, form 4), so that tests can hold it against the
+// slot form of encode_program.  words must hold kNoAllocMaxInstr * 5 words.
+int noalloc_slot_form(const rsr_program &p, uint32_t num_features, uint32_t *words, uint32_t *n_words,
+                      uint32_t *n_slots, uint32_t *flags, const char **err) {
+    return encode_slots_fixed(p, num_features, words, n_words, n_slots, flags, err);
+}
+uint32_t noalloc_max_words() { return kNoAllocMaxInstr * 5; }
+
 }  // namespace rsr
 
 using namespace rsr;

@@ -1319,7 +1319,28 @@ int rsr_program_encoding(const rsr_program *prog, uint32_t num_features, int for
     int rc = encode_program(prog->code, prog->len, prog->const_kinds, prog->n_consts, prog->params, prog->n_params,
                             num_features, &E, &err);
     if (rc) return fail(rc, err);
-    const std::vector<uint32_t> &v = form == 0 ? E.slot_code : form == 1 ? E.reg_code : E.tape_code;
+    std::vector<uint32_t> v;
+    if (form == 0 || form == 3) {
+        v = E.slot_code;
+        if (form == 3) {
+            v.push_back(E.n_slots);
+            v.push_back((E.result_zero ? PF_RESULT_ZERO : 0u) | (E.needs_zero_init ? PF_NEEDS_ZERO_INIT : 0u));
+        }
+    } else if (form == 1) {
+        v = E.reg_code;
+    } else if (form == 2) {
+        v = E.tape_code;
+    } else if (form == 4) {
+        v.resize(noalloc_max_words());
+        uint32_t nw = 0, ns = 0, fl = 0;
+        const char *msg = "";
+        if ((rc = noalloc_slot_form(*prog, num_features, v.data(), &nw, &ns, &fl, &msg))) return fail(rc, msg);
+        v.resize(nw);
+        v.push_back(ns);
+        v.push_back(fl);
+    } else {
+        return fail(RSR_EINVAL, "unknown encoding form");
+    }
     *len = (uint32_t)v.size();
     for (uint32_t i = 0; i < cap && i < v.size(); ++i) out[i] = v[i];
     return RSR_OK;

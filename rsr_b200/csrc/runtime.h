@@ -260,4 +260,9 @@ int fit_cma_es(rsr_ctx *ctx, const rsr_population *pop, const uint64_t *dsp, uin
 // while capturing a graph.
 int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st, cudaEvent_t ev_mid,
                  cudaEvent_t *group_events = nullptr);
+// The no-allocation entry point's fixed-array slot encoder (noalloc.cu), for
+// diagnostics; words must hold noalloc_max_words() words.
+int noalloc_slot_form(const rsr_program &p, uint32_t num_features, uint32_t *words, uint32_t *n_words,
+                      uint32_t *n_slots, uint32_t *flags, const char **err);
+uint32_t noalloc_max_words();
 }  // namespace rsr

@@ -215,3 +215,31 @@ def test_generator_is_seeded_and_in_range():
     assert all(4 <= len(p.code) <= 48 for p in a)
     t = W.transform_population(50, seed=4)
     assert all(1 <= len(p.constants) <= 8 and 8 <= len(p.code) <= 40 for p in t)
+
+
+def test_noalloc_slot_encoder_matches_encode_program():
+    """rsr_compute_mse_noalloc encodes the slot form into fixed arrays by its
+    own pass; it must give the words, slot count and flags of the engine's
+    encoder on every program it accepts: random programs of every workload,
+    stale constant loads, B/I loads, empty programs and 32-deep stacks."""
+    pops = [(W.scalar_population(150, seed=61), 1), (W.lorentz_population(150, seed=62), 9),
+            (W.transform_population(100, seed=63), 15), (W.inverse_population(150, seed=64), 8)]
+    edge = [Program([]), Program([I.word(2, 0), I.word(4, 1), I.load_var(FLOAT, 0)]),
+            Program([I.load_const(FLOAT, 0), I.load_var(FLOAT, 0), I.op("AddF")], [Scalar(VEC3, (1.0, 2.0, 3.0))]),
+            Program([I.load_var(FLOAT, 1), I.load_const(FLOAT, 0)], [Scalar(VEC2, (5.0, 6.0))]),
+            Program([I.load_var(FLOAT, 0)] * 32 + [I.op("AddF")] * 31),
+            Program([I.load_var(FLOAT, 0), I.load_var(FLOAT, 1), I.op("MakeVec2")])]
+    pops.append((edge, 4))
+    checked = 0
+    for pop, nf in pops:
+        for p in pop:
+            a = E.encoding(p, nf, 3)
+            b = E.encoding(p, nf, 4)
+            np.testing.assert_array_equal(a, b)
+            checked += 1
+    assert checked >= 550
+    # beyond the fixed arrays' limit the fixed encoder refuses
+    long = Program([I.load_var(FLOAT, 0)] + [I.load_var(FLOAT, 0), I.op("AddF")] * 256)
+    with pytest.raises(N.RsrError) as ei:
+        E.encoding(long, 1, 4)
+    assert ei.value.code == N.RSR_EINVAL
