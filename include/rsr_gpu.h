@@ -366,8 +366,9 @@ RSR_API int rsr_program_analyze(const rsr_program *prog, uint32_t num_features, 
  * micro-op), 2 = tape form (adjoint), 3 = slot form followed by its slot
  * count and flags (1: stack_f[0] never written, 2: slots need zeroing),
  * 4 = the same three from rsr_compute_mse_noalloc's fixed-array encoder
- * (RSR_EINVAL beyond its limits).  Writes up to cap words and the full
- * length to *len. */
+ * (RSR_EINVAL beyond its limits), 5 = the register adjoint's code preceded
+ * by its kernel profile (0xFFFFFFFF: none), tape slots and five stack
+ * depths.  Writes up to cap words and the full length to *len. */
 RSR_API int rsr_program_encoding(const rsr_program *prog, uint32_t num_features, int form, uint32_t *out,
                                  uint32_t cap, uint32_t *len);
 

@@ -513,6 +513,9 @@ class AccEmitter {
         }
     }
 
+    uint32_t writes_of(int id) const { return writes_[id]; }
+    int size_of(int id) const { return size_[id]; }
+
     std::vector<uint32_t> &code;
     int max_sp[N_STACKS] = {0, 0, 0, 0, 0};
     uint32_t types_ = 0;  // accumulator types used
@@ -556,6 +559,215 @@ class AccEmitter {
     std::vector<uint32_t> &writes_;
     std::vector<int> &size_;
     int sp_[N_STACKS] = {0, 0, 0, 0, 0};
+};
+
+// Register-adjoint code (uops.h, kAdjHeaderWords) of a tree an AccEmitter
+// has analysed: the accumulator form's evaluation order without load
+// fusion, every PUSH to its own stack slot, TAPE micro-ops next to the ops
+// whose reverse rules read forward values, and one reverse entry per
+// micro-op.  Tape slots hold (first | second << 16):
+//   F MUL: A before; DIV: A after; RDIV: A before, A after;
+//   sin cos sqr ln: A before; exp sqrt: A after;
+//   V CROSS/RCROSS, M MUL/RMUL, DOT, DET: the accumulator before;
+//   SCALE, MULM: the accumulator before, and (A forms) the other operand's
+//   accumulator (A_F, or the matrix);
+//   NORM: A_F after, the vector; INVERSE: after, before.
+class AdjEmitter {
+   public:
+    AdjEmitter(const std::vector<Node> &nodes, const AccEmitter &an) : nodes_(nodes), an_(an) {}
+
+    void gen(int id) {
+        const Node &n = nodes_[id];
+        const int opc = n.opcode;
+        if (is_load(opc)) {
+            op(kBlockBase[n.out] + (is_const_load(opc) ? KV_LDC : KV_LDX), n.arg);
+            return;
+        }
+        const Node *in[3] = {n.n_in > 0 ? &nodes_[n.in[0]] : nullptr, n.n_in > 1 ? &nodes_[n.in[1]] : nullptr,
+                             n.n_in > 2 ? &nodes_[n.in[2]] : nullptr};
+        switch (op_class(opc)) {
+            case C_BIN: {
+                const int t = n.out, base = kBlockBase[t] + KV_BIN;
+                const BinIdx b = bin_index(opc);
+                int j, src;
+                uint32_t arg;
+                if (leaf(*in[1])) {
+                    gen(n.in[0]);
+                    j = b.op, src = src_of(*in[1]), arg = in[1]->arg;
+                } else if (leaf(*in[0])) {
+                    gen(n.in[1]);
+                    j = b.rop, src = src_of(*in[0]), arg = in[0]->arg;
+                } else if (an_.size_of(n.in[1]) > an_.size_of(n.in[0])) {
+                    gen(n.in[1]);
+                    arg = (uint32_t)push(t);
+                    gen(n.in[0]);
+                    j = b.op, src = SRC_S;
+                } else {
+                    gen(n.in[0]);
+                    arg = (uint32_t)push(t);
+                    gen(n.in[1]);
+                    j = b.rop, src = SRC_S;
+                }
+                const int kind = base + 3 * j + src;
+                const bool before = (t == SF && (j == 3 || j == 5)) || (t != SF && t != SV2 && (j == 3 || j == 4));
+                const bool after = t == SF && (j == 4 || j == 5);
+                const uint32_t ta = take(t), tb = before && after ? take(t) : 0u;
+                if (before) store(t, ta);
+                op(kind, arg, ta, tb);
+                if (after) store(t, before ? tb : ta);
+                if (!before && !after) tape -= (uint32_t)kStackWidth[t];  // not needed after all
+                break;
+            }
+            case C_DOT: {
+                const int t = in[0]->out;
+                const int base = kBlockBase[t] + kv_dot(kBinOps[t]);
+                uint32_t arg;
+                int src;
+                if (leaf(*in[1])) { gen(n.in[0]); src = src_of(*in[1]); arg = in[1]->arg; }
+                else if (leaf(*in[0])) { gen(n.in[1]); src = src_of(*in[0]); arg = in[0]->arg; }
+                else { gen(n.in[0]); arg = (uint32_t)push(t); gen(n.in[1]); src = SRC_S; }
+                const uint32_t ta = take(t);
+                store(t, ta);
+                op(base + src, arg, ta);
+                break;
+            }
+            case C_SCALE: {
+                const int t = n.out;
+                cross_type(n, kBlockBase[t] + (t == SM2 || t == SM3 ? (int)KM_SCALE : kv_scale(kBinOps[t])), SF, t);
+                break;
+            }
+            case C_MULMV: {
+                const int t = n.out;
+                cross_type(n, kBlockBase[t] + kv_mulm(kBinOps[t], t == SV2 ? 2 : 3), in[0]->out, t);
+                break;
+            }
+            case C_UNARY_F: {
+                gen(n.in[0]);
+                const int u = opc - SIN_F;  // sin cos exp sqr sqrt ln
+                const uint32_t ta = take(SF);
+                const bool after = u == 2 || u == 4;
+                if (!after) store(SF, ta);
+                op(K_F_UN + u, 0, ta);
+                if (after) store(SF, ta);
+                break;
+            }
+            case C_NORM: case C_GET: {
+                const int t = in[0]->out, nb = kBinOps[t];
+                gen(n.in[0]);
+                int k = kv_norm(nb);
+                if (opc == GET_X_V2 || opc == GET_X_V3) k += 1;
+                if (opc == GET_Y_V2 || opc == GET_Y_V3) k += 2;
+                if (opc == GET_Z_V3) k += 3;
+                if (op_class(opc) == C_NORM) {
+                    const uint32_t tb = take(t), ta = take(SF);
+                    store(t, tb);
+                    op(kBlockBase[t] + k, 0, ta, tb);
+                    store(SF, ta);
+                } else {
+                    op(kBlockBase[t] + k, 0);
+                }
+                break;
+            }
+            case C_DET: case C_TRACE: case C_MAT_UN: {
+                const int t = in[0]->out;
+                gen(n.in[0]);
+                if (opc == DET_M2 || opc == DET_M3) {
+                    const uint32_t ta = take(t);
+                    store(t, ta);
+                    op(kBlockBase[t] + KM_DET, 0, ta);
+                } else if (opc == TRACE_M2 || opc == TRACE_M3) {
+                    op(kBlockBase[t] + KM_TRACE, 0);
+                } else if (opc == TRANSPOSE_M2 || opc == TRANSPOSE_M3) {
+                    op(kBlockBase[t] + KM_TRANSPOSE, 0);
+                } else {
+                    const uint32_t tb = take(t), ta = take(t);
+                    store(t, tb);
+                    op(kBlockBase[t] + KM_INVERSE, 0, ta, tb);
+                    store(t, ta);
+                }
+                break;
+            }
+            case C_MAKE: {  // operands pushed to consecutive slots reserved up front
+                const int tin = in[0]->out, t = n.out;
+                const int first = n_push[tin];
+                n_push[tin] += n.n_in - 1;
+                for (int i = 0; i + 1 < n.n_in; ++i) {
+                    gen(n.in[i]);
+                    op(kBlockBase[tin] + KV_PUSH, (uint32_t)(first + i));
+                }
+                gen(n.in[n.n_in - 1]);
+                const int k = t == SM2 || t == SM3 ? (int)KM_MAKE : kv_make(kBinOps[t], t == SV2 ? 2 : 3);
+                op(kBlockBase[t] + k, (uint32_t)first);
+                break;
+            }
+            case C_LOAD: break;
+        }
+    }
+
+    // The code: header, forward words, reverse entries in reverse order.
+    void finish(std::vector<uint32_t> *out) const {
+        out->clear();
+        out->push_back((uint32_t)fwd.size());
+        out->push_back((uint32_t)(rev.size() / 2));
+        out->insert(out->end(), fwd.begin(), fwd.end());
+        for (size_t i = rev.size(); i >= 2; i -= 2) {
+            out->push_back(rev[i - 2]);
+            out->push_back(rev[i - 1]);
+        }
+    }
+
+    std::vector<uint32_t> fwd, rev;
+    uint32_t tape = 0;
+    int n_push[N_STACKS] = {0, 0, 0, 0, 0};
+
+   private:
+    // Scale / mat-vec: the operand of another type (tother) is fused when it
+    // is a leaf, pushed when the result subtree overwrites its accumulator,
+    // else read from its accumulator (A form, taped); base + {0 A, 1 X, 2 C, 3 S}.
+    void cross_type(const Node &n, int base, int tother, int t) {
+        const Node &o = nodes_[n.in[0]];
+        if (leaf(o)) {
+            gen(n.in[1]);
+            const uint32_t ta = take(t);
+            store(t, ta);
+            op(base + 1 + src_of(o), o.arg, ta);
+            return;
+        }
+        gen(n.in[0]);
+        if (an_.writes_of(n.in[1]) & (1u << tother)) {
+            const int slot = push(tother);
+            gen(n.in[1]);
+            const uint32_t ta = take(t);
+            store(t, ta);
+            op(base + 3, (uint32_t)slot, ta);
+        } else {
+            gen(n.in[1]);
+            const uint32_t ta = take(t), tb = take(tother);
+            store(t, ta);
+            store(tother, tb);
+            op(base + 0, 0, ta, tb);
+        }
+    }
+    static int src_of(const Node &leafn) { return is_const_load(leafn.opcode) ? SRC_C : SRC_X; }
+    uint32_t take(int t) {
+        const uint32_t s = tape;
+        tape += (uint32_t)kStackWidth[t];
+        return s;
+    }
+    void store(int t, uint32_t slot) { fwd.push_back(uop_word((uint32_t)kTapeKind[t], slot)); }
+    void op(int kind, uint32_t arg, uint32_t ta = 0, uint32_t tb = 0) {
+        fwd.push_back(uop_word((uint32_t)kind, arg));
+        rev.push_back(uop_word((uint32_t)kind, arg));
+        rev.push_back(ta | (tb << 16));
+    }
+    int push(int t) {
+        const int slot = n_push[t]++;
+        op(kBlockBase[t] + KV_PUSH, (uint32_t)slot);
+        return slot;
+    }
+
+    const std::vector<Node> &nodes_;
+    const AccEmitter &an_;
 };
 
 // Peephole pass over the accumulator form: a PUSH directly followed by a
@@ -794,6 +1006,26 @@ int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uin
             for (int p = 0; fits && p < N_PROFILES; ++p)
                 if ((em.types_ & ~kProfileTypes[p]) == 0) { E.profile = p; break; }
             if (E.profile >= 0) E.reg_code.assign(em.code.begin(), em.code.end());
+        }
+    }
+
+    // ---- register adjoint form
+    if ((forms & FORM_ADJ) && root >= 0 && !has_stale_live && n_params < (1u << kLdOffsetBits)) {
+        AccEmitter an(nodes);
+        if (an.analyze(root)) {
+            AdjEmitter em(nodes, an);
+            em.gen(root);
+            bool fits = em.tape < (1u << 16);
+            for (int t = 0; t < N_STACKS; ++t) {
+                E.adj_depth[t] = em.n_push[t];
+                fits = fits && em.n_push[t] <= kMaxAccStack;
+            }
+            for (int p = 0; fits && p < N_PROFILES; ++p)
+                if ((an.types_ & ~kProfileTypes[p]) == 0) { E.adj_profile = p; break; }
+            if (E.adj_profile >= 0) {
+                em.finish(&E.adj_code);
+                E.adj_tape = em.tape;
+            }
         }
     }
     return RSR_OK;

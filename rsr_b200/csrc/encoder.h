@@ -47,22 +47,30 @@ struct EncodedProgram {
     std::vector<uint32_t> tape_code;      // 2 header words + 5 words per live node
     uint32_t n_tape_val = 0, n_tape_adj = 0;  // scalar value / adjoint slots
     int tape_profile = P_ALL;             // smallest kernel profile covering the live values' types
+    // register adjoint (uops.h, kAdjHeaderWords): empty when the program
+    // needs the slot-file adjoint
+    std::vector<uint32_t> adj_code;
+    uint32_t adj_tape = 0;                // tape slots (scalar values)
+    int adj_depth[N_STACKS] = {0, 0, 0, 0, 0};  // stack slots per type (one per PUSH)
+    int adj_profile = -1;
 
     // Back to the default state; the vectors keep their capacity, so an
     // EncodedProgram reused across calls stops allocating.
     void reset() {
         std::vector<float> c = std::move(consts);
-        std::vector<uint32_t> sc = std::move(slot_code), rc = std::move(reg_code), tc = std::move(tape_code);
+        std::vector<uint32_t> sc = std::move(slot_code), rc = std::move(reg_code), tc = std::move(tape_code),
+                              ac = std::move(adj_code);
         *this = EncodedProgram();
-        c.clear(); sc.clear(); rc.clear(); tc.clear();
+        c.clear(); sc.clear(); rc.clear(); tc.clear(); ac.clear();
         consts = std::move(c); slot_code = std::move(sc); reg_code = std::move(rc); tape_code = std::move(tc);
+        adj_code = std::move(ac);
     }
 };
 
 // Validates and encodes.  num_features == 0 skips feature-range checks.
 // Returns 0 or an rsr_status code, with a message in *err.
 // Device forms to emit (validation and the analysis run for every call).
-enum EncodeForms : unsigned { FORM_SLOT = 1u, FORM_TAPE = 2u, FORM_ACC = 4u, FORM_ALL = 7u };
+enum EncodeForms : unsigned { FORM_SLOT = 1u, FORM_TAPE = 2u, FORM_ACC = 4u, FORM_ADJ = 8u, FORM_ALL = 15u };
 int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uint32_t n_consts,
                    const float *params, uint32_t n_params, uint32_t num_features, EncodedProgram *out,
                    std::string *err, bool fuse_loads = true, unsigned forms = FORM_ALL);

@@ -1330,6 +1330,10 @@ int rsr_program_encoding(const rsr_program *prog, uint32_t num_features, int for
         v = E.reg_code;
     } else if (form == 2) {
         v = E.tape_code;
+    } else if (form == 5) {
+        v = {E.adj_profile < 0 ? 0xFFFFFFFFu : (uint32_t)E.adj_profile, E.adj_tape};
+        for (int t = 0; t < N_STACKS; ++t) v.push_back((uint32_t)E.adj_depth[t]);
+        v.insert(v.end(), E.adj_code.begin(), E.adj_code.end());
     } else if (form == 4) {
         v.resize(noalloc_max_words());
         uint32_t nw = 0, ns = 0, fl = 0;

@@ -82,6 +82,10 @@ enum AccKind : int {
 };
 // number of binary ops in each block
 static constexpr int kBinOps[5] = {6, 3, 5, 5, 5};
+// Register adjoint (kernels_adj.cu): one TAPE kind per block, just past the
+// block's last kind; arg = first tape slot.  It stores the type's
+// accumulator to the tape, for the reverse rules that read forward values.
+static constexpr int kTapeKind[5] = {K_F + 27, K_V2 + 27, K_V3 + 34, K_M2 + 27, K_M3 + 27};
 static constexpr int kBlockBase[5] = {K_F, K_V2, K_V3, K_M2, K_M3};
 // V-block offsets after the binary ops
 RSR_HD static constexpr int kv_scale(int nbin) { return KV_BIN + 3 * nbin; }       // 4 kinds: A X C S
@@ -121,6 +125,16 @@ static constexpr uint32_t kProfileTypes[N_PROFILES] = {
     1u << SF, (1u << SF) | (1u << SV3), (1u << SF) | (1u << SV2) | (1u << SM2), (1u << SF) | (1u << SV3) | (1u << SM3),
     0x1Fu};
 static constexpr int kMaxAccStack = 16;   // shared-memory stack slots per type
+
+// Register adjoint code of a program (EncodedProgram::adj_code): word 0 the
+// forward length F, word 1 the reverse length R, then F forward micro-op
+// words (accumulator form without load fusion, TAPE kinds between them,
+// every PUSH to its own stack slot so that spilled values survive the
+// forward sweep), then R reverse entries of two words each, in the order the
+// reverse sweep runs them: the forward word of the micro-op being reversed,
+// and its tape slots (first | second << 16; which forward values they hold
+// depends on the kind, kernels_adj.cu).
+static constexpr int kAdjHeaderWords = 2;
 
 // Program descriptor for the kernels (one per program in a launch).
 struct ProgDesc {

@@ -366,7 +366,8 @@ def analyze(program: Program, num_features: int = 0) -> dict:
 def encoding(program: Program, num_features: int = 0, form: int = 1) -> np.ndarray:
     """Device encoding of a program (0 slot form, 1 accumulator form, 2 tape
     form; 3 slot form + slot count + flags, 4 the same from the
-    no-allocation entry point's fixed-array encoder)."""
+    no-allocation entry point's fixed-array encoder; 5 register adjoint:
+    profile, tape slots, 5 stack depths, then its code)."""
     s, keep = _as_program(program)
     n = C.c_uint32()
     N.check(N.lib().rsr_program_encoding(C.byref(s), num_features, form, None, 0, C.byref(n)))

@@ -1,0 +1,80 @@
+"""The register adjoint's code (encoder.cpp AdjEmitter), run on the CPU by a
+numpy emulator of its forward and reverse sweeps (tests/accvm.py): the
+gradients it gives are the dual-number oracle's (evaluator.rs:177-388) on
+random programs of every workload, within the per-component bound of the
+GPU tests; programs with an inverse, whose dual rule in the reference is a
+no-op, are held against central differences instead."""
+import warnings
+
+import numpy as np
+
+import accvm
+from oracle import binding as O
+from rsr_b200 import evaluator as E
+from rsr_b200 import isa as I
+from rsr_b200 import workloads as W
+
+CASES = [("scalar", lambda: W.scalar_dataset(300, seed=3), lambda: W.scalar_population(40, seed=4)),
+         ("vector", lambda: W.lorentz_dataset(240, seed=5), lambda: W.lorentz_population(40, seed=6)),
+         ("matrix", lambda: W.transform_dataset(240, seed=7), lambda: W.transform_population(40, seed=8)),
+         ("uneven", lambda: W.inverse_dataset(240, seed=9), lambda: W.inverse_population(40, seed=10))]
+
+
+def test_register_adjoint_code_gives_the_dual_gradients():
+    checked = {}
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)  # random programs divide by zero
+        for name, dsf, popf in CASES:
+            ds, pop = dsf(), popf()
+            checked[name] = 0
+            for i, p in enumerate(pop):
+                n = min(32, p.param_count())
+                if n == 0:
+                    continue
+                m64, gd, l1 = O.grad_dual_f64(p, ds)
+                if not (np.isfinite(gd[:n]).all() and np.isfinite(m64) and m64 < 1e4):
+                    continue
+                m, g = accvm.run(p, ds)
+                inverse = any(I.OP_NAMES[w & 255].startswith("Inverse") for w in p.code)
+                # the reference's dual pass skips inverses in its value too
+                m_ref = O.mse_f64(p, ds) if inverse else m64
+                assert abs(m - m_ref) <= 1e-5 * max(m_ref, 1e-6), (name, i, m, m_ref)
+                floor = 1e-4 * l1[:n] + 1e-6 * l1[:n].max() + 1e-12
+                if inverse:
+                    # an inverse near a singular matrix somewhere in the data
+                    # makes central differences unstable: such programs are
+                    # skipped, the others must agree within the noise
+                    fd, fd4 = O.grad_fd(p, ds, 1e-3)[:n], O.grad_fd(p, ds, 1e-4)[:n]
+                    if not (np.abs(fd - fd4) <= 1e-2 * np.abs(fd) + floor).all():
+                        continue
+                    noise = 2 * np.abs(fd - O.grad_fd(p, ds, 2e-3)[:n]) + 2 * np.abs(fd - fd4)
+                    ok = np.abs(g[:n] - fd) <= 1e-3 * np.abs(fd) + floor + noise
+                    checked["inverse"] = checked.get("inverse", 0) + 1
+                else:
+                    ok = np.abs(g[:n] - gd[:n]) <= 1e-3 * np.abs(gd[:n]) + floor
+                assert ok.all(), (name, i, g[:n], gd[:n])
+                checked[name] += 1
+    assert all(checked[name] >= 10 for name, _, _ in CASES) and checked.get("inverse", 0) >= 3, checked
+
+
+def test_register_adjoint_code_layout():
+    """Header words, one reverse entry per non-TAPE forward micro-op, PUSH
+    slots all distinct, tape slots inside the reported tape."""
+    for p in W.lorentz_population(30, seed=11) + W.inverse_population(30, seed=12):
+        enc = E.encoding(p, 9, 5)
+        if enc[0] == 0xFFFFFFFF:
+            continue
+        tape, depth, code = int(enc[1]), [int(x) for x in enc[2:7]], enc[7:]
+        nf, nr = int(code[0]), int(code[1])
+        assert len(code) == 2 + nf + 2 * nr
+        fwd = [int(w) for w in code[2:2 + nf]]
+        tapes = [w for w in fwd if (w & 255) in accvm.TAPE]
+        assert nr == nf - len(tapes)
+        assert all((w >> 8) < tape for w in tapes)
+        pushes = {}
+        for w in fwd:
+            t = accvm.block(w & 255)
+            if (w & 255) - accvm.BASE[t] == 2:
+                pushes.setdefault(t, []).append(w >> 8)
+        for t, slots in pushes.items():
+            assert sorted(slots) == list(range(len(slots))) and len(slots) == depth[t]
