@@ -100,6 +100,8 @@ typedef struct rsr_options {
 
 /* rsr_options.flags */
 #define RSR_OPT_NO_LOAD_FUSION 1u   /* register kernel: keep loads as separate micro-ops */
+#define RSR_OPT_SLOT_ADJOINT 2u     /* gradients: the slot-file adjoint for every program (else the
+                                       register adjoint where a program fits it) */
 
 /* ------------------------------------------------------------- context */
 RSR_API void rsr_options_default(rsr_options *opts);

@@ -17,6 +17,7 @@ STATUS_NAMES = ["OK", "EINVAL", "EPROGRAM", "ENOMEM", "ENODEV", "ECUDA", "ETIMED
                 "ECANCELED"]
 KERNEL_AUTO, KERNEL_PLAIN, KERNEL_BATCHED = 0, 1, 2
 OPT_NO_LOAD_FUSION = 1
+OPT_SLOT_ADJOINT = 2
 
 
 class RsrError(RuntimeError):

@@ -19,7 +19,7 @@ ROOT = PKG.parent
 BUILD = PKG / "_build"
 LIB = PKG / "librsrgpu.so"
 
-SOURCES = ["runtime.cu", "kernels_plain.cu", "kernels_reg.cu", "kernels_grad.cu", "encoder.cpp",
+SOURCES = ["runtime.cu", "kernels_plain.cu", "kernels_reg.cu", "kernels_grad.cu", "kernels_adj.cu", "encoder.cpp",
            "serving.cu", "lbfgs.cu", "nelder_mead.cu", "cma_es.cu", "ingest.cu", "noalloc.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-lineinfo", "-fmad=false",
               "-prec-div=true", "-prec-sqrt=true", "-Xcompiler", "-fPIC,-fvisibility=hidden,-ffp-contract=off",

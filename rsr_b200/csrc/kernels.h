@@ -11,6 +11,7 @@ namespace rsr {
 constexpr int kPlainThreads = 128;  // 4 warps per block, one work item per warp
 constexpr int kRegThreads = 256;  // 8 warps share one work item
 constexpr int kGradThreads = 32;  // one warp per block, one item per warp
+constexpr int kAdjThreads = 128;  // register adjoint: 4 warps share one work item
 
 cudaError_t launch_plain(const LaunchArgs &a, int P, uint32_t warps_per_block, size_t smem, cudaStream_t st);
 size_t plain_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t slots, int P);
@@ -38,6 +39,16 @@ int reg_max_p(int profile);
 size_t reg_smem_bytes(uint32_t code_words, uint32_t const_floats, const uint32_t *stack_depth, int P, int G);
 constexpr size_t kRegSmemBudget = 200 * 1024;  // at least one block per SM, below the 227 KB cap
 int reg_max_blocks_per_sm(int profile, int P, unsigned omit, size_t smem);
+
+// register adjoint (kernels_adj.cu): profiles F, F+V3, F+V2+M2, F+V3+M3;
+// P (points per lane) 2 or 4
+bool adj_supported(int profile);
+void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t tape_slots, const uint32_t *stack_depth, int P,
+                LaunchArgs *a);
+size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t tape_slots, const uint32_t *stack_depth,
+                      int P);
+cudaError_t launch_adj(const LaunchArgs &a, int profile, int P, uint32_t grid, size_t smem, cudaStream_t st);
+int adj_max_blocks_per_sm(int profile, int P, size_t smem);
 
 // adjoint kernel (kernels_grad.cu)
 cudaError_t launch_grad(const LaunchArgs &a, int profile, bool no_unary, uint32_t warps_per_block, size_t smem,

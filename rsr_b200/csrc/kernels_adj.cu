@@ -1,0 +1,619 @@
+// kernels_adj.cu -- the register adjoint: MSE and d(MSE)/d(constants) with
+// the forward and the reverse sweep both on accumulator registers.
+//
+// Replaces compute_mse_with_gradient (src/engine/eval/evaluator.rs:177-224)
+// and its one dual-number pass per flat parameter (eval_simd_dual,
+// evaluator.rs:228-388) for the programs the accumulator machine takes.
+// Per tile of 32*P points a warp runs
+//   forward  the accumulator form (acc_ops.cuh) without load fusion, every
+//            PUSH to its own stack slot, and TAPE micro-ops that store the
+//            forward values the reverse rules read into a per-warp tape in
+//            shared memory;
+//   seed     G_F = 2 (pred - y) on counted points (evaluator.rs:207);
+//   reverse  the reverse entries (uops.h, kAdjHeaderWords): each maps the
+//            adjoint accumulators G_t of the micro-op's output to those of
+//            its inputs.  A second operand's adjoint goes to the constant
+//            sums (LoadConst), to the adjoint stack slot of its PUSH (a
+//            spilled value), or nowhere (a feature).
+// The reverse rules follow autodiff.rs's forward rules (product and quotient
+// rules, g/(2 sqrt x), norms through sqrt of dot); InverseM2/M3, whose dual
+// rule is a no-op in the reference (src/domains/linalg/mod.rs:643,687), get
+// the exact adjoint -A^-T G A^-T, zero on the singular branch.  The tape is
+// recorded and consumed tile by tile: the population x points x length tape
+// is never stored.  The encoder's tape slot conventions are listed with
+// AdjEmitter (encoder.cpp).
+#include <cuda_runtime.h>
+#include <float.h>
+
+#include "acc_ops.cuh"
+#include "kernels.h"
+#include "kernels_common.cuh"
+
+namespace rsr {
+
+constexpr uint32_t kAdjParams = 32;
+
+// Reverse-sweep access: the forward machine's operand fetches (features,
+// constants, forward stack values), the adjoint stacks, the tape and the
+// lane's gradient sums.
+template <int P>
+struct RevIO : AccIO<P> {
+    Vf<P> *gstk[N_STACKS];  // adjoint stacks of this lane: [(slot*W + c)*32]
+    Vf<P> *tape;            // tape of this lane: [slot*32]
+    float *gacc;            // this lane's f32 gradient sums: gacc[k*32]
+    uint32_t valid;         // bit q: point q of the lane is counted
+    __device__ __forceinline__ Vf<P> T(uint32_t slot) const { return tape[slot * 32]; }
+    template <int W>
+    __device__ __forceinline__ Vf<P> &GS(int t, uint32_t slot, int c) const { return gstk[t][(slot * W + c) * 32]; }
+    // adds the lane's counted points of g to the sum of flat parameter k
+    // (points past the dataset's end may carry 0*inf = NaN adjoints)
+    __device__ __forceinline__ void grad_add(uint32_t k, const Vf<P> &g) const {
+        if (k >= kAdjParams) return;
+        float s = 0.0f;
+#pragma unroll
+        for (int q = 0; q < P; ++q)
+            if ((valid >> q) & 1u) s = s + g.v[q];
+        gacc[k * 32] += s;
+    }
+};
+
+template <int P, int W>
+__device__ __forceinline__ void zero_acc(Vf<P> *G) {
+#pragma unroll
+    for (int c = 0; c < W; ++c) G[c] = splat<P>(0.0f);
+}
+
+template <int P, int W>
+__device__ __forceinline__ void load_tape(Vf<P> *v, const RevIO<P> &io, uint32_t slot) {
+#pragma unroll
+    for (int c = 0; c < W; ++c) v[c] = io.T(slot + c);
+}
+
+// The adjoint of a second operand from source SRC: a constant's goes to the
+// parameter sums, a spilled value's to its adjoint stack slot (its PUSH adds
+// it back), a feature's nowhere.
+template <int P, int W, int SRC>
+__device__ __forceinline__ void send(const RevIO<P> &io, int t, uint32_t arg, const Vf<P> *gb) {
+    if constexpr (SRC == SRC_C) {
+#pragma unroll
+        for (int c = 0; c < W; ++c) io.grad_add(arg + c, gb[c]);
+    } else if constexpr (SRC == SRC_S) {
+#pragma unroll
+        for (int c = 0; c < W; ++c) io.template GS<W>(t, arg, c) = gb[c];
+    }
+}
+
+// out(r,c) = sum_j G(r,j) B(c,j) = (G B^T)(r,c), column-major N x N.
+template <int P, int N>
+__device__ __forceinline__ void mm_nt(const Vf<P> *G, const Vf<P> *B, Vf<P> *out) {
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int c = 0; c < N; ++c) {
+            Vf<P> s = splat<P>(0.0f);
+#pragma unroll
+            for (int j = 0; j < N; ++j) s = s + G[N * j + r] * B[N * j + c];
+            out[N * c + r] = s;
+        }
+}
+// out(r,c) = sum_j A(j,r) G(j,c) = (A^T G)(r,c).
+template <int P, int N>
+__device__ __forceinline__ void mm_tn(const Vf<P> *A, const Vf<P> *G, Vf<P> *out) {
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int c = 0; c < N; ++c) {
+            Vf<P> s = splat<P>(0.0f);
+#pragma unroll
+            for (int j = 0; j < N; ++j) s = s + A[N * r + j] * G[N * c + j];
+            out[N * c + r] = s;
+        }
+}
+
+// Reverse of one micro-op of kind K: g holds the adjoints of the machine's
+// accumulators after the micro-op and is left holding those before it.
+template <int PROF, int P, int K>
+__device__ __forceinline__ void rev_op(Acc<PROF, P> &g, const RevIO<P> &io, uint32_t arg, uint32_t w1) {
+    constexpr int t = K >= K_M3 ? SM3 : K >= K_M2 ? SM2 : K >= K_V3 ? SV3 : K >= K_V2 ? SV2 : SF;
+    if constexpr (((kProfileTypes[PROF] >> t) & 1u) != 0u) {
+        constexpr int W = kStackWidth[t];
+        constexpr int k = K - kBlockBase[t];
+        constexpr int nb = kBinOps[t];
+        Vf<P> *G = acc_of<PROF, P, t>(g);
+        const uint32_t ta = w1 & 0xFFFFu, tb = w1 >> 16;
+        if constexpr (k == KV_LDX) {
+            zero_acc<P, W>(G);
+        } else if constexpr (k == KV_LDC) {
+#pragma unroll
+            for (int c = 0; c < W; ++c) io.grad_add(arg + c, G[c]);
+            zero_acc<P, W>(G);
+        } else if constexpr (k == KV_PUSH) {
+#pragma unroll
+            for (int c = 0; c < W; ++c) G[c] = G[c] + io.template GS<W>(t, arg, c);
+        } else if constexpr (k >= KV_BIN && k < KV_BIN + 3 * nb) {
+            constexpr int j = (k - KV_BIN) / 3, src = (k - KV_BIN) % 3;
+            constexpr int op = bin_code<t, j>();
+            if constexpr (op == BIN_ADD) {
+                send<P, W, src>(io, t, arg, G);
+            } else if constexpr (op == BIN_SUB || op == BIN_RSUB) {
+                Vf<P> n[W];
+#pragma unroll
+                for (int c = 0; c < W; ++c) n[c] = -G[c];
+                if constexpr (op == BIN_SUB) {
+                    send<P, W, src>(io, t, arg, n);
+                } else {
+                    send<P, W, src>(io, t, arg, G);
+#pragma unroll
+                    for (int c = 0; c < W; ++c) G[c] = n[c];
+                }
+            } else if constexpr (op == BIN_MUL) {        // a * b: tape a
+                Vf<P> b;
+                fetch<P, 1, src>(&b, io, t, arg);
+                const Vf<P> gb = G[0] * io.T(ta);
+                send<P, 1, src>(io, t, arg, &gb);
+                G[0] = G[0] * b;
+            } else if constexpr (op == BIN_DIV) {        // a / b: tape the quotient
+                Vf<P> b;
+                fetch<P, 1, src>(&b, io, t, arg);
+                const Vf<P> q = G[0] / b;
+                const Vf<P> gb = -(q * io.T(ta));
+                send<P, 1, src>(io, t, arg, &gb);
+                G[0] = q;
+            } else if constexpr (op == BIN_RDIV) {       // b / a: tape a, the quotient
+                const Vf<P> q = G[0] / io.T(ta);
+                send<P, 1, src>(io, t, arg, &q);
+                G[0] = -(q * io.T(tb));
+            } else if constexpr (op == BIN_CROSS || op == BIN_RCROSS) {  // tape a
+                Vf<P> a[3], b[3], gb[3];
+                load_tape<P, 3>(a, io, ta);
+                fetch<P, 3, src>(b, io, t, arg);
+                if constexpr (op == BIN_CROSS) {   // o = a x b: da = b x g, db = g x a
+                    cross3(G, a, gb);
+                    cross3(b, G, G);
+                } else {                           // o = b x a: db = a x g, da = g x b
+                    cross3(a, G, gb);
+                    cross3(G, b, G);
+                }
+                send<P, 3, src>(io, t, arg, gb);
+            } else {                                     // matrix products: tape a
+                constexpr int N = W == 4 ? 2 : 3;
+                Vf<P> a[W], b[W], gb[W], ga[W];
+                load_tape<P, W>(a, io, ta);
+                fetch<P, W, src>(b, io, t, arg);
+                if constexpr (op == BIN_MMUL) {    // o = a b: da = g b^T, db = a^T g
+                    mm_tn<P, N>(a, G, gb);
+                    mm_nt<P, N>(G, b, ga);
+                } else {                           // o = b a: db = g a^T, da = b^T g
+                    mm_nt<P, N>(G, a, gb);
+                    mm_tn<P, N>(b, G, ga);
+                }
+                send<P, W, src>(io, t, arg, gb);
+#pragma unroll
+                for (int c = 0; c < W; ++c) G[c] = ga[c];
+            }
+        } else if constexpr (t == SF) {                  // unary: sin cos exp sqr sqrt ln
+            constexpr int u = k - (K_F_UN - K_F);
+            const Vf<P> v = io.T(ta);  // the operand, or the result for exp and sqrt
+            if constexpr (u == 0) G[0] = G[0] * vcos(v);
+            else if constexpr (u == 1) G[0] = G[0] * (-vsin(v));
+            else if constexpr (u == 2) G[0] = G[0] * v;
+            else if constexpr (u == 3) G[0] = G[0] * (splat<P>(2.0f) * v);
+            else if constexpr (u == 4) G[0] = G[0] / (splat<P>(2.0f) * v);
+            else if constexpr (u == 5) G[0] = G[0] / v;
+        } else if constexpr (t == SV2 || t == SV3) {
+            constexpr int ks = kv_scale(nb), kd = kv_dot(nb), kn = kv_norm(nb), km = kv_mulm(nb, W),
+                          kk = kv_make(nb, W);
+            if constexpr (k >= ks && k < ks + 4) {       // SCALE {A X C S}: tape the vector (and A_F)
+                Vf<P> a[W], s;
+                load_tape<P, W>(a, io, ta);
+                if constexpr (k == ks) s = io.T(tb);
+                else fetch<P, 1, k - ks - 1>(&s, io, SF, arg);
+                Vf<P> gs = splat<P>(0.0f);
+#pragma unroll
+                for (int c = 0; c < W; ++c) gs = gs + G[c] * a[c];
+                if constexpr (k == ks) g.F[0] = g.F[0] + gs;
+                else send<P, 1, k - ks - 1>(io, SF, arg, &gs);
+#pragma unroll
+                for (int c = 0; c < W; ++c) G[c] = G[c] * s;
+            } else if constexpr (k >= kd && k < kd + 3) { // DOT {X C S}: tape the vector
+                Vf<P> a[W], b[W], gb[W];
+                load_tape<P, W>(a, io, ta);
+                fetch<P, W, k - kd>(b, io, t, arg);
+                const Vf<P> gf = g.F[0];
+#pragma unroll
+                for (int c = 0; c < W; ++c) {
+                    G[c] = G[c] + gf * b[c];
+                    gb[c] = gf * a[c];
+                }
+                send<P, W, k - kd>(io, t, arg, gb);
+                g.F[0] = splat<P>(0.0f);
+            } else if constexpr (k == kn) {              // NORM: tape the norm, the vector
+                const Vf<P> q = g.F[0] / io.T(ta);
+#pragma unroll
+                for (int c = 0; c < W; ++c) G[c] = G[c] + q * io.T(tb + c);
+                g.F[0] = splat<P>(0.0f);
+            } else if constexpr (k > kn && k <= kn + W) { // GET x/y/z
+                G[k - kn - 1] = G[k - kn - 1] + g.F[0];
+                g.F[0] = splat<P>(0.0f);
+            } else if constexpr (k >= km && k < km + 4) { // MULM {A X C S}: tape the vector (and A_M)
+                constexpr int tm = W == 2 ? SM2 : SM3;
+                constexpr int MW = W * W;
+                if constexpr (((kProfileTypes[PROF] >> tm) & 1u) != 0u || k != km) {
+                    Vf<P> v[W], m[MW], gm[MW];
+                    load_tape<P, W>(v, io, ta);
+                    if constexpr (k == km) load_tape<P, MW>(m, io, tb);
+                    else fetch<P, MW, k - km - 1>(m, io, tm, arg);
+#pragma unroll
+                    for (int c = 0; c < W; ++c)
+#pragma unroll
+                        for (int r = 0; r < W; ++r) gm[W * c + r] = G[r] * v[c];
+                    if constexpr (k == km) {
+                        if constexpr (((kProfileTypes[PROF] >> tm) & 1u) != 0u) {
+                            Vf<P> *GM = acc_of<PROF, P, tm>(g);
+#pragma unroll
+                            for (int i = 0; i < MW; ++i) GM[i] = GM[i] + gm[i];
+                        }
+                    } else {
+                        send<P, MW, k - km - 1>(io, tm, arg, gm);
+                    }
+                    Vf<P> nv[W];
+#pragma unroll
+                    for (int c = 0; c < W; ++c) {
+                        Vf<P> s = splat<P>(0.0f);
+#pragma unroll
+                        for (int r = 0; r < W; ++r) s = s + m[W * c + r] * G[r];
+                        nv[c] = s;
+                    }
+#pragma unroll
+                    for (int c = 0; c < W; ++c) G[c] = nv[c];
+                }
+            } else if constexpr (k == kk) {              // MAKE from F stack slots + A_F
+                g.F[0] = g.F[0] + G[W - 1];
+#pragma unroll
+                for (int c = 0; c + 1 < W; ++c) io.template GS<1>(SF, arg + c, 0) = G[c];
+                zero_acc<P, W>(G);
+            }
+        } else {  // M2 / M3
+            constexpr int N = W == 4 ? 2 : 3;
+            constexpr int tv = W == 4 ? SV2 : SV3;
+            if constexpr (k >= KM_SCALE && k < KM_SCALE + 4) {
+                Vf<P> a[W], s;
+                load_tape<P, W>(a, io, ta);
+                if constexpr (k == KM_SCALE) s = io.T(tb);
+                else fetch<P, 1, k - KM_SCALE - 1>(&s, io, SF, arg);
+                Vf<P> gs = splat<P>(0.0f);
+#pragma unroll
+                for (int c = 0; c < W; ++c) gs = gs + G[c] * a[c];
+                if constexpr (k == KM_SCALE) g.F[0] = g.F[0] + gs;
+                else send<P, 1, k - KM_SCALE - 1>(io, SF, arg, &gs);
+#pragma unroll
+                for (int c = 0; c < W; ++c) G[c] = G[c] * s;
+            } else if constexpr (k == KM_DET) {          // tape the matrix
+                Vf<P> m[W];
+                load_tape<P, W>(m, io, ta);
+                const Vf<P> gf = g.F[0];
+                if constexpr (N == 2) {
+                    G[0] = G[0] + gf * m[3];
+                    G[3] = G[3] + gf * m[0];
+                    G[1] = G[1] + (-(gf * m[2]));
+                    G[2] = G[2] + (-(gf * m[1]));
+                } else {
+#pragma unroll
+                    for (int r = 0; r < 3; ++r)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            const int r1 = (r + 1) % 3, r2 = (r + 2) % 3, c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+                            const Vf<P> cof = m[3 * c1 + r1] * m[3 * c2 + r2] - m[3 * c2 + r1] * m[3 * c1 + r2];
+                            G[3 * c + r] = G[3 * c + r] + gf * cof;
+                        }
+                }
+                g.F[0] = splat<P>(0.0f);
+            } else if constexpr (k == KM_TRACE) {
+#pragma unroll
+                for (int i = 0; i < N; ++i) G[(N + 1) * i] = G[(N + 1) * i] + g.F[0];
+                g.F[0] = splat<P>(0.0f);
+            } else if constexpr (k == KM_TRANSPOSE) {
+                Vf<P> tr[W];
+#pragma unroll
+                for (int r = 0; r < N; ++r)
+#pragma unroll
+                    for (int c = 0; c < N; ++c) tr[N * r + c] = G[N * c + r];
+#pragma unroll
+                for (int i = 0; i < W; ++i) G[i] = tr[i];
+            } else if constexpr (k == KM_INVERSE) {      // tape the inverse, the matrix
+                Vf<P> o[W], m[W], h[W];
+                load_tape<P, W>(o, io, ta);
+                load_tape<P, W>(m, io, tb);
+                Vf<P> det;
+                if constexpr (N == 2) det = det_m2(m); else det = det_m3(m);
+                // h = O^T G, then dA = -(h O^T), zero where singular
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+#pragma unroll
+                    for (int l = 0; l < N; ++l) {
+                        Vf<P> s = splat<P>(0.0f);
+#pragma unroll
+                        for (int q = 0; q < N; ++q) s = s + o[N * i + q] * G[N * l + q];
+                        h[N * l + i] = s;
+                    }
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+#pragma unroll
+                    for (int j = 0; j < N; ++j) {
+                        Vf<P> s = splat<P>(0.0f);
+#pragma unroll
+                        for (int l = 0; l < N; ++l) s = s + h[N * l + i] * o[N * l + j];
+                        Vf<P> d;
+#pragma unroll
+                        for (int q = 0; q < P; ++q) d.v[q] = fabsf(det.v[q]) < 1e-9f ? 0.0f : -s.v[q];
+                        m[N * j + i] = d;  // m is no longer needed
+                    }
+#pragma unroll
+                for (int i = 0; i < W; ++i) G[i] = m[i];
+            } else if constexpr (k == KM_MAKE) {         // columns: vector stack slots + A_V
+                if constexpr (((kProfileTypes[PROF] >> tv) & 1u) != 0u) {
+                    Vf<P> *GV = acc_of<PROF, P, tv>(g);
+#pragma unroll
+                    for (int r = 0; r < N; ++r) GV[r] = GV[r] + G[N * (N - 1) + r];
+#pragma unroll
+                    for (int col = 0; col + 1 < N; ++col)
+#pragma unroll
+                        for (int r = 0; r < N; ++r) io.template GS<N>(tv, arg + col, r) = G[N * col + r];
+                }
+                zero_acc<P, W>(G);
+            }
+        }
+    }
+}
+
+// Forward: a micro-op of kind K, or a TAPE store of its block's accumulator.
+template <int PROF, int P, int t>
+__device__ __forceinline__ void tape_store(Acc<PROF, P> &a, const RevIO<P> &io, uint32_t slot) {
+    if constexpr (((kProfileTypes[PROF] >> t) & 1u) != 0u) {
+        constexpr int W = kStackWidth[t];
+        const Vf<P> *A = acc_of<PROF, P, t>(a);
+#pragma unroll
+        for (int c = 0; c < W; ++c) io.tape[(slot + c) * 32] = A[c];
+    }
+}
+
+#define RSR_F(K) case (K): acc_op<PROF, P, (K)>(a, io, arg); break;
+#define RSR_R(K) case (K): rev_op<PROF, P, (K)>(g, io, arg, w1); break;
+#define RSR_X4(M, K) M(K) M(K + 1) M(K + 2) M(K + 3)
+#define RSR_X9(M, K) RSR_X4(M, K) RSR_X4(M, K + 4) M(K + 8)
+#define RSR_X27(M, K) RSR_X9(M, K) RSR_X9(M, K + 9) RSR_X9(M, K + 18)
+#define RSR_X34(M, K) RSR_X27(M, K) RSR_X4(M, K + 27) M(K + 31) M(K + 32) M(K + 33)
+// The kinds of each profile's blocks (F 0..26, V2 32..58, V3 64..97, M2
+// 104..130, M3 136..162): a profile's switch lists only its own.
+#define RSR_SWITCH(M, EXTRA)                                                                         \
+    if constexpr (PROF == P_F) {                                                                     \
+        switch (kind) { EXTRA RSR_X27(M, K_F) default: break; }                                      \
+    } else if constexpr (PROF == P_FV3) {                                                            \
+        switch (kind) { EXTRA RSR_X27(M, K_F) RSR_X34(M, K_V3) default: break; }                     \
+    } else if constexpr (PROF == P_FV2M2) {                                                          \
+        switch (kind) { EXTRA RSR_X27(M, K_F) RSR_X27(M, K_V2) RSR_X27(M, K_M2) default: break; }    \
+    } else {                                                                                         \
+        switch (kind) { EXTRA RSR_X27(M, K_F) RSR_X34(M, K_V3) RSR_X27(M, K_M3) default: break; }    \
+    }
+#define RSR_TAPES                                                            \
+    case kTapeKind[SF]: tape_store<PROF, P, SF>(a, io, arg); break;          \
+    case kTapeKind[SV2]: tape_store<PROF, P, SV2>(a, io, arg); break;        \
+    case kTapeKind[SV3]: tape_store<PROF, P, SV3>(a, io, arg); break;        \
+    case kTapeKind[SM2]: tape_store<PROF, P, SM2>(a, io, arg); break;        \
+    case kTapeKind[SM3]: tape_store<PROF, P, SM3>(a, io, arg); break;
+#define RSR_NONE
+
+template <int PROF, int P>
+__device__ __forceinline__ void run_forward(Acc<PROF, P> &a, const RevIO<P> &io, const uint32_t *code, uint32_t len) {
+    uint32_t w = code[0];
+    for (uint32_t pc = 0; pc < len; ++pc) {
+        const uint32_t wn = code[pc + 1];
+        const uint32_t arg = w >> 8, kind = w & 0xFFu;
+        RSR_SWITCH(RSR_F, RSR_TAPES)
+        w = wn;
+    }
+}
+
+template <int PROF, int P>
+__device__ __forceinline__ void run_reverse(Acc<PROF, P> &g, const RevIO<P> &io, const uint32_t *rev, uint32_t n) {
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t w0 = rev[2 * i], w1 = rev[2 * i + 1];
+        const uint32_t arg = w0 >> 8, kind = w0 & 0xFFu;
+        RSR_SWITCH(RSR_R, RSR_NONE)
+    }
+}
+
+#undef RSR_NONE
+#undef RSR_TAPES
+#undef RSR_SWITCH
+#undef RSR_X34
+#undef RSR_X27
+#undef RSR_X9
+#undef RSR_X4
+#undef RSR_R
+#undef RSR_F
+
+// Block-cooperative persistent kernel: a block's warps take the tiles of one
+// work item (one program on a chunk of points).  Shared memory: block
+// header (code | constants | meta | cross-warp sums), then one region per
+// warp: tape | stacks | adjoint stacks | gradient sums | Kahan state.
+template <int PROF, int P>
+__global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchArgs a) {
+    extern __shared__ __align__(16) float smem[];
+    if (a.run_if && *a.run_if == 0u) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nw = blockDim.x >> 5;
+    uint32_t *scode = reinterpret_cast<uint32_t *>(smem);
+    float *sconst = smem + ((a.smem_code_words + 1u + 3u) & ~3u);  // code and its pad word
+    uint32_t *meta = reinterpret_cast<uint32_t *>(sconst + ((a.smem_const_floats + 3u) & ~3u));  // [0] item
+    double *red = reinterpret_cast<double *>(meta + 4);  // [warp][1 + kAdjParams]
+    float *wbase = smem + a.block_hdr_floats + (size_t)warp * a.region_floats;
+
+    RevIO<P> io;
+    io.tape = reinterpret_cast<Vf<P> *>(wbase + a.tape_off) + lane;
+#pragma unroll
+    for (int t = 0; t < N_STACKS; ++t) {
+        io.stk[t] = reinterpret_cast<Vf<P> *>(wbase + a.stack_off[t]) + lane;
+        io.gstk[t] = reinterpret_cast<Vf<P> *>(wbase + a.gstack_off[t]) + lane;
+    }
+    io.gacc = wbase + a.acc_off + lane;
+    float *kahan = wbase + a.acc_off + kAdjParams * 32;  // [2][32]
+    io.consts = sconst;
+
+    for (;;) {
+        if (threadIdx.x == 0) meta[0] = atomicAdd(a.item_counter, 1u);
+        __syncthreads();
+        const uint32_t item_id = meta[0];
+        if (item_id >= a.n_items) break;
+        const WorkItem it = a.items[item_id];
+        if (a.active && !a.active[it.prog_begin]) {
+            __syncthreads();  // meta[0] is rewritten by the next item fetch
+            continue;
+        }
+        const ProgDesc pd = a.progs[it.prog_begin];
+        for (uint32_t i = threadIdx.x; i < pd.uop_len; i += blockDim.x) scode[i] = __ldg(a.code + pd.uop_off + i);
+        if (threadIdx.x == 0) scode[pd.uop_len] = 0u;  // prefetch pad of the forward loop
+        for (uint32_t i = threadIdx.x; i < pd.n_consts; i += blockDim.x) sconst[i] = __ldg(a.consts + pd.const_off + i);
+        const uint32_t np = min(pd.n_consts, kAdjParams);
+        for (uint32_t k = 0; k < np; ++k) io.gacc[k * 32] = 0.0f;
+        kahan[lane] = 0.0f;
+        kahan[32 + lane] = 0.0f;
+        __syncthreads();
+        const DatasetDesc ds = a.datasets[pd.dataset];
+        io.stride = (uint32_t)ds.stride;
+        const uint32_t n_fwd = scode[0], n_rev = scode[1];
+        const uint32_t *fwd = scode + kAdjHeaderWords, *rev = fwd + n_fwd;
+        for (uint32_t tile = it.tile_begin + warp; tile < it.tile_end; tile += nw) {
+            const uint64_t p0 = (uint64_t)tile * (32u * P) + (uint64_t)lane * P;
+            io.xl = ds.x + p0;
+            uint32_t valid = 0;
+#pragma unroll
+            for (int q = 0; q < P; ++q) valid |= (p0 + q < ds.n_eval ? 1u : 0u) << q;
+            io.valid = valid;
+            Acc<PROF, P> acc;
+            run_forward<PROF, P>(acc, io, fwd, n_fwd);
+            const Vf<P> y = load_pts<P>(ds.y + p0);
+            Acc<PROF, P> g;
+            g.F[0] = splat<P>(0.0f);
+            if constexpr (Types<PROF>::V2) zero_acc<P, 2>(g.V2);
+            if constexpr (Types<PROF>::V3) zero_acc<P, 3>(g.V3);
+            if constexpr (Types<PROF>::M2) zero_acc<P, 4>(g.M2);
+            if constexpr (Types<PROF>::M3) zero_acc<P, 9>(g.M3);
+            Kahan ks;
+            ks.s = kahan[lane];
+            ks.c = kahan[32 + lane];
+#pragma unroll
+            for (int q = 0; q < P; ++q) {
+                const bool ok = (valid >> q) & 1u;
+                const float d = acc.F[0].v[q] - y.v[q];
+                if (ok) ks.add(d * d);
+                g.F[0].v[q] = ok ? 2.0f * d : 0.0f;  // d(diff^2)/d pred, as in evaluator.rs:207
+            }
+            kahan[lane] = ks.s;
+            kahan[32 + lane] = ks.c;
+            run_reverse<PROF, P>(g, io, rev, n_rev);
+        }
+        // per-warp sums in f64, then across warps in a fixed order
+        {
+            Kahan ks;
+            ks.s = kahan[lane];
+            ks.c = kahan[32 + lane];
+            const double s = warp_sum(ks.value());
+            if (lane == 0) red[warp * (1 + kAdjParams)] = s;
+            for (uint32_t k = 0; k < kAdjParams; ++k) {
+                const double gk = k < np ? warp_sum((double)io.gacc[k * 32]) : 0.0;
+                if (lane == 0) red[warp * (1 + kAdjParams) + 1 + k] = gk;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < 1 + kAdjParams) {
+            double s = 0.0;
+            for (int w = 0; w < nw; ++w) s += red[w * (1 + kAdjParams) + threadIdx.x];
+            a.partials[(size_t)(pd.part_off + it.chunk) * (1 + kAdjParams) + threadIdx.x] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------- launchers
+// Shared-memory layout (floats).  Block header: code (+1 pad) | constants |
+// meta (4 words) | cross-warp sums (warps x 33 doubles).  Per warp: tape |
+// stacks (per type) | adjoint stacks (per type) | gradient sums (32 x 32)
+// | Kahan state (2 x 32).
+void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t tape_slots, const uint32_t *stack_depth, int P,
+                LaunchArgs *a) {
+    const uint32_t nw = kAdjThreads / 32;
+    a->block_hdr_floats = ((code_words + 1u + 3u) & ~3u) + ((const_floats + 3u) & ~3u) + 4u +
+                          2u * nw * (1u + kAdjParams);
+    uint32_t off = 0;
+    a->tape_off = off;
+    off += tape_slots * 32u * (uint32_t)P;
+    for (int t = 0; t < N_STACKS; ++t) {
+        a->stack_off[t] = off;
+        off += stack_depth[t] * (uint32_t)kStackWidth[t] * 32u * (uint32_t)P;
+    }
+    for (int t = 0; t < N_STACKS; ++t) {
+        a->gstack_off[t] = off;
+        off += stack_depth[t] * (uint32_t)kStackWidth[t] * 32u * (uint32_t)P;
+    }
+    a->acc_off = off;
+    off += kAdjParams * 32u + 2u * 32u;
+    a->region_floats = (off + 3u) & ~3u;
+}
+
+size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t tape_slots, const uint32_t *stack_depth,
+                      int P) {
+    LaunchArgs a{};
+    adj_layout(code_words, const_floats, tape_slots, stack_depth, P, &a);
+    return ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (kAdjThreads / 32)) * 4u;
+}
+
+template <int PROF, int P>
+static cudaError_t launch_adj_pp(const LaunchArgs &a, uint32_t grid, size_t smem, cudaStream_t st) {
+    auto k = adj_eval_kernel<PROF, P>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin);
+    if (e != cudaSuccess) return e;
+    k<<<grid, kAdjThreads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int PROF, int P>
+static int adj_occ(size_t smem) {
+    auto k = adj_eval_kernel<PROF, P>;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin) != cudaSuccess) return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kAdjThreads, smem) != cudaSuccess) return 0;
+    return n;
+}
+
+bool adj_supported(int profile) { return profile >= P_F && profile <= P_FV3M3; }
+
+cudaError_t launch_adj(const LaunchArgs &a, int profile, int P, uint32_t grid, size_t smem, cudaStream_t st) {
+    switch (profile * 2 + (P >= 4 ? 1 : 0)) {
+        case 0: return launch_adj_pp<P_F, 2>(a, grid, smem, st);
+        case 1: return launch_adj_pp<P_F, 4>(a, grid, smem, st);
+        case 2: return launch_adj_pp<P_FV3, 2>(a, grid, smem, st);
+        case 3: return launch_adj_pp<P_FV3, 4>(a, grid, smem, st);
+        case 4: return launch_adj_pp<P_FV2M2, 2>(a, grid, smem, st);
+        case 5: return launch_adj_pp<P_FV2M2, 4>(a, grid, smem, st);
+        case 6: return launch_adj_pp<P_FV3M3, 2>(a, grid, smem, st);
+        case 7: return launch_adj_pp<P_FV3M3, 4>(a, grid, smem, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+int adj_max_blocks_per_sm(int profile, int P, size_t smem) {
+    switch (profile * 2 + (P >= 4 ? 1 : 0)) {
+        case 0: return adj_occ<P_F, 2>(smem);
+        case 1: return adj_occ<P_F, 4>(smem);
+        case 2: return adj_occ<P_FV3, 2>(smem);
+        case 3: return adj_occ<P_FV3, 4>(smem);
+        case 4: return adj_occ<P_FV2M2, 2>(smem);
+        case 5: return adj_occ<P_FV2M2, 4>(smem);
+        case 6: return adj_occ<P_FV3M3, 2>(smem);
+        case 7: return adj_occ<P_FV3M3, 4>(smem);
+        default: return 0;
+    }
+}
+
+}  // namespace rsr

@@ -135,6 +135,12 @@ static constexpr int kRegPathStride = 8;
 // 40 KB and 81.6 ms at 20 KB; the vector and matrix workloads' tapes fit
 // 40 KB at 4 points and do not change.
 static constexpr size_t kGradTapeBudget = 80 * 1024;
+// Register adjoint: shared memory a warp's tape, stacks, adjoint stacks and
+// gradient sums may take (4 warps per block), and the first path number of
+// its launches in a gradient plan.
+static constexpr size_t kAdjWarpBudget = 40 * 1024;
+static constexpr int kAdjPathBase = 0;
+static constexpr uint32_t kNoDepth[N_STACKS] = {0, 0, 0, 0, 0};
 // Points per work-item chunk (all P).  8192 measured slower on every kernel
 // (vector register 4.32 ms against 4.30, matrix register 4.84 against 4.69,
 // vector adjoint 6.68 against 5.90): coarser items balance worse.
@@ -209,7 +215,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             pop.param_off[i + 1] < pop.param_off[i])
             return fail(RSR_EINVAL, "population offsets decrease at " + std::to_string(i));
     const bool fuse = (ctx->opts.flags & RSR_OPT_NO_LOAD_FUSION) == 0;
-    const unsigned forms = gradient ? FORM_TAPE : kernel == RSR_KERNEL_PLAIN ? FORM_SLOT : FORM_ACC;
+    const unsigned forms = gradient ? (FORM_TAPE | FORM_ADJ) : kernel == RSR_KERNEL_PLAIN ? FORM_SLOT : FORM_ACC;
     if (ctx->enc_cache.size() < n) {
         ctx->enc_cache.resize(n);
         ctx->enc_rc.resize(n);
@@ -238,9 +244,34 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
     }
     for (uint32_t i = 0; i < n; ++i)
         if (erc[i] != RSR_OK) return fail(erc[i], "program " + std::to_string(i) + ": " + emsg[i]);
-    // path per program: -2 adjoint, -1 plain, >= 0 register profile
+    // path per program: <= -2 slot-file adjoint, -1 plain, >= 0 register
+    // profile (MSE plans) or register adjoint (gradient plans)
     std::vector<int> path(n);
     for (uint32_t i = 0; i < n; ++i) {
+        if (gradient && enc[i].adj_profile >= 0 && adj_supported(enc[i].adj_profile) &&
+            !(ctx->opts.flags & RSR_OPT_SLOT_ADJOINT)) {
+            // register adjoint: 4 points per lane when a warp's tape, stacks
+            // and adjoint stacks fit kAdjWarpBudget, else 2; launches by that
+            // size in steps of 16 slots, so that a block's shared memory
+            // follows its own programs
+            const EncodedProgram &E = enc[i];
+            uint32_t depth[N_STACKS], slots = E.adj_tape;
+            for (int t = 0; t < N_STACKS; ++t) {
+                depth[t] = (uint32_t)E.adj_depth[t];
+                slots += 2u * depth[t] * (uint32_t)kStackWidth[t];
+            }
+            const uint32_t cw = (uint32_t)E.adj_code.size(), cf = (uint32_t)E.consts.size();
+            auto per_warp = [&](int Pp) {
+                return (adj_smem_bytes(cw, cf, E.adj_tape, depth, Pp) - adj_smem_bytes(cw, cf, 0, kNoDepth, Pp)) /
+                           (kAdjThreads / 32) + 32 * 33 * 4;
+            };
+            const int p4 = per_warp(4) <= kAdjWarpBudget ? 1 : 0;
+            if (p4 || per_warp(2) <= kAdjWarpBudget) {
+                const int bucket = std::min<int>((int)((slots + 15) / 16), 63);
+                path[i] = kAdjPathBase + ((bucket * 2 + p4) * N_PROFILES + E.adj_profile);
+                continue;
+            }
+        }
         if (gradient) {
             // adjoint launches by tape size, so that a block's shared memory
             // follows its own programs' tapes: steps of 16 slots up to 256,
@@ -317,7 +348,8 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         size_t cw = 0, cf = 0;
         for (uint32_t i = 0; i < n; ++i) {
             const EncodedProgram &E = enc[i];
-            cw += path[i] <= -2 ? E.tape_code.size() : path[i] == -1 ? E.slot_code.size() : E.reg_code.size();
+            cw += path[i] <= -2 ? E.tape_code.size() : path[i] == -1 ? E.slot_code.size()
+                : gradient ? E.adj_code.size() : E.reg_code.size();
             cf += E.consts.size();
         }
         P.code.reserve(cw);
@@ -327,7 +359,8 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
     for (uint32_t li = 0; li < n; ++li) {
         const uint32_t i = order[li];
         const EncodedProgram &E = enc[i];
-        const std::vector<uint32_t> &code = path[i] <= -2 ? E.tape_code : path[i] == -1 ? E.slot_code : E.reg_code;
+        const std::vector<uint32_t> &code = path[i] <= -2 ? E.tape_code : path[i] == -1 ? E.slot_code
+                                            : gradient ? E.adj_code : E.reg_code;
         ProgDesc d{};
         d.uop_off = (uint32_t)P.code.size();
         d.uop_len = (uint32_t)code.size();
@@ -359,11 +392,15 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         uint32_t end = li;
         while (end < n && path[order[end]] == pth) ++end;
         Group g;
-        g.kind = pth <= -2 ? 2 : pth == -1 ? 0 : 1;
-        g.profile = pth >= 0 ? pth % kRegPathStride : pth <= -2 ? (-2 - pth) % N_PROFILES : -1;
-        g.omit = pth >= 0 ? (unsigned)(pth / kRegPathStride / 3) : 0u;
+        g.kind = pth <= -2 ? 2 : pth == -1 ? 0 : gradient ? 3 : 1;
+        g.profile = g.kind == 3 ? (pth - kAdjPathBase) % N_PROFILES
+                  : pth >= 0 ? pth % kRegPathStride : pth <= -2 ? (-2 - pth) % N_PROFILES : -1;
+        g.omit = g.kind == 1 ? (unsigned)(pth / kRegPathStride / 3) : 0u;
         g.item_begin = (uint32_t)P.items.size();
-        if (g.kind == 1) {
+        if (g.kind == 3) {
+            g.G = 1;
+            g.P = ((pth - kAdjPathBase) / N_PROFILES) % 2 ? 4 : 2;
+        } else if (g.kind == 1) {
             // P and G are per profile and dataset size; one launch uses one P,
             // the largest dataset's choice.
             uint64_t max_eval = 0;
@@ -397,6 +434,11 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                 if (g.kind == 1)
                     for (int t = 0; t < N_STACKS; ++t)
                         g.stack_depth[t] = std::max(g.stack_depth[t], (uint32_t)enc[order[q]].depth_fast[t]);
+                if (g.kind == 3) {
+                    sl = std::max(sl, enc[order[q]].adj_tape);
+                    for (int t = 0; t < N_STACKS; ++t)
+                        g.stack_depth[t] = std::max(g.stack_depth[t], (uint32_t)enc[order[q]].adj_depth[t]);
+                }
             }
             g.code_words = std::max(g.code_words, cw);
             g.const_floats = std::max(g.const_floats, cf);
@@ -578,6 +620,14 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             g.smem = smem;
             g.warps_per_block = kRegThreads / 32;
             e = launch_reg(a, g.profile, g.P, g.omit, g.grid, gs);
+        } else if (g.kind == 3) {
+            adj_layout(g.code_words, g.const_floats, g.slots, g.stack_depth, g.P, &a);
+            const size_t smem = adj_smem_bytes(g.code_words, g.const_floats, g.slots, g.stack_depth, g.P);
+            const int bps = std::max(1, adj_max_blocks_per_sm(g.profile, g.P, smem));
+            g.grid = std::max(1u, (uint32_t)std::min<uint64_t>((uint64_t)bps * ctx->num_sms, g.n_items));
+            g.smem = smem;
+            g.warps_per_block = kAdjThreads / 32;
+            e = launch_adj(a, g.profile, g.P, g.grid, smem, gs);
         } else {
             const size_t per = grad_smem_per_warp(g.code_words, g.const_floats, g.slots, g.adj_slots, g.P);
             a.smem_adj_slots = g.adj_slots;
@@ -1147,7 +1197,7 @@ int rsr_batch_describe(rsr_ctx *ctx, rsr_batch *b, char *buf, size_t len) {
                     ", \"program_points\": " + std::to_string(b->plan.program_points) + ", \"groups\": [";
     for (size_t i = 0; i < b->plan.groups.size(); ++i) {
         const Group &g = b->plan.groups[i];
-        const char *kn = g.kind == 0 ? "slot" : g.kind == 1 ? "register" : "adjoint";
+        const char *kn = g.kind == 0 ? "slot" : g.kind == 1 ? "register" : g.kind == 2 ? "adjoint" : "register_adjoint";
         s += (i ? ", " : "") + std::string("{\"kernel\": \"") + kn + "\", \"profile\": " + std::to_string(g.profile) +
              ", \"no_unary\": " + ((g.kind == 1 ? (g.omit & 1u) != 0 : g.no_unary) ? "true" : "false") +
              ", \"no_matrix_operand\": " + ((g.kind == 1 && (g.omit & 2u)) ? "true" : "false") +

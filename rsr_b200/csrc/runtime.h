@@ -99,7 +99,7 @@ struct TuneChoice {
 
 // One kernel launch inside a plan.
 struct Group {
-    int kind = 0;        // 0 plain, 1 register, 2 adjoint
+    int kind = 0;        // 0 plain, 1 register, 2 slot-file adjoint, 3 register adjoint
     int profile = -1;
     unsigned omit = 0;      // register kernel: handler sets its programs do not need (launch_reg)
     bool no_unary = false;  // adjoint kernel: no unary Float op in the launch's programs

@@ -297,3 +297,29 @@ def test_full_size_vector_workload_properties():
     idx = np.arange(0, 4096, 64)
     m64, _ = O.mse_batch(I.pack([pop[i] for i in idx]), ds)
     check_mse(fast[idx], m64, ds.num_samples)
+
+
+@pytest.mark.parametrize("wl", ["scalar", "lorentz", "transform", "inverse"])
+def test_register_and_slot_adjoints_agree(wl):
+    """Gradients of the register adjoint (the default where a program fits
+    it) against the slot-file adjoint (RSR_OPT_SLOT_ADJOINT): both reverse
+    sweeps of the same programs, within 1e-3 relative per component plus
+    f32 resolution against the gradient's scale; MSEs within 1e-6."""
+    ds, pop = WORKLOADS[wl][0](), WORKLOADS[wl][1]()
+    with Engine() as e, Engine(flags=N.OPT_SLOT_ADJOINT) as s:
+        m1, g1 = e.compute_mse_grad_batch(pop, ds)
+        m2, g2 = s.compute_mse_grad_batch(pop, ds)
+        b = e.prepare(pop, ds, gradient=True)
+        kinds = {g["kernel"] for g in b.describe()["groups"]}
+        b.close()
+    assert "register_adjoint" in kinds, kinds
+    fin = (m2 < FMAX) & np.isfinite(g2).all(1) & np.isfinite(g1).all(1)
+    assert np.array_equal(m1 < FMAX, m2 < FMAX)
+    np.testing.assert_allclose(m1[fin], m2[fin], rtol=1e-6)
+    for i in np.nonzero(fin)[0]:
+        n = min(32, pop[i].param_count())
+        if n == 0:
+            continue
+        scale = np.abs(g2[i, :n]).max()
+        assert (np.abs(g1[i, :n] - g2[i, :n]) <= 1e-3 * np.abs(g2[i, :n]) + 1e-5 * scale + 1e-30).all(), \
+            (wl, i, g1[i, :n], g2[i, :n])
