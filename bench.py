@@ -376,7 +376,7 @@ def matrix_bench(eng, eng_nog, fp32_peak: float, reps: int):
     per, groups = _group_ms(eng_nog, bg2, reps)
     bg2.close()
     d2.release()
-    adj = [i for i, g in enumerate(groups) if g["kernel"] == "adjoint"]
+    adj = [i for i, g in enumerate(groups) if g["kernel"] in ("adjoint", "register_adjoint")]
     k_ms = statistics.median([sum(r[i] for i in adj) for r in per])
     k_flops = sum(groups[i]["flops"] for i in adj)
     fit = [p for p in pop if p.is_differentiable()]
@@ -565,7 +565,21 @@ def run_engine(args):
         if i >= 3:
             ams.append(t)
     adj_value = pp_rank * world * len(ams) / (max_over_ranks(sum(ams)) * 1e-3)
+    adj_kinds = sorted({g["kernel"] for g in bg.describe()["groups"]})
     bg.close()
+    # the same gradients on the slot-file adjoint alone, for comparison
+    eng_s = Engine(device=local, flags=N.OPT_SLOT_ADJOINT)
+    bs = eng_s.prepare(pk, eng_s.upload(ds), gradient=True)
+    sms = []
+    for i in range(3 + max(3, min(args.steps, 10))):
+        eng_s.flush_l2()
+        bs.run()
+        bs.results()
+        t = bs.timing()[1]
+        if i >= 3:
+            sms.append(t)
+    bs.close()
+    eng_s.close()
 
     # ------------------- register interpreter without the batching extras
     # one program per work item, 4 points per lane, no autotuning, no graph:
@@ -603,6 +617,17 @@ def run_engine(args):
     serving = None
     if not args.no_serving:
         serving = serving_bench(eng, args.serving_jobs, args.serving_rate, slots=8)
+        # the mix's capacity is what the saturated run completed per second;
+        # the same mix offered at 50% and 90% of it gives the latency below
+        # saturation
+        capacity = serving["completed"] / serving["drain_s"]
+        serving["capacity_jobs_per_s"] = capacity
+        serving["at_fraction_of_capacity"] = {}
+        for frac, jobs in ((0.5, 60), (0.9, 100)):
+            r = serving_bench(eng, jobs, frac * capacity, slots=8, seed=17)
+            serving["at_fraction_of_capacity"][str(frac)] = {
+                "arrival_rate_jobs_per_s": r["arrival_rate_jobs_per_s"], "jobs": jobs, "completed": r["completed"],
+                "latency_ms": r["latency_ms"], "drain_s": r["drain_s"]}
     serving_light = None
     if not args.no_serving:
         serving_light = serving_light_bench(eng)
@@ -630,8 +655,10 @@ def run_engine(args):
             "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                            "max": float(max(step_ms))},
             "adjoint": {"value": adj_value, "unit": UNIT, "ms_per_step": float(np.median(ams)),
-                        "what": "MSE and d(MSE)/d(constants) of the same batch, reverse-mode adjoint kernel, "
-                                "graph replay"},
+                        "over_mse": float(np.median(ams)) / (total_ms / len(step_ms)), "kernels": adj_kinds,
+                        "slot_file_adjoint_ms": float(np.median(sms)),
+                        "what": "MSE and d(MSE)/d(constants) of the same batch, reverse-mode adjoint kernels, "
+                                "graph replay; slot_file_adjoint_ms: the same with RSR_OPT_SLOT_ADJOINT"},
             "register_one_program_per_item": {
                 "value": reg1_value, "unit": UNIT, "speedup_of_batched": value / reg1_value,
                 "ms_per_step": float(np.median(rms)),
