@@ -183,7 +183,7 @@ static TuneChoice choice_for(rsr_ctx *ctx, int profile, uint64_t n_eval) {
 }
 
 int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_prog, uint64_t ds_all, int kernel,
-               bool gradient, int mode, Plan *plan) {
+               bool gradient, int mode, Plan *plan, EncodeScratch *scratch, std::mutex *table_mu) {
     NvtxRange nvtx_range("rsr: encode + plan");
     Plan &P = *plan;
     P.reset();
@@ -195,6 +195,8 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
     // datasets
     std::map<uint64_t, uint32_t> ds_index;
     std::vector<uint32_t> prog_ds(n);
+    std::unique_lock<std::mutex> table_lock;
+    if (table_mu) table_lock = std::unique_lock<std::mutex>(*table_mu);
     for (uint32_t i = 0; i < n; ++i) {
         uint64_t h = ds_per_prog ? ds_per_prog[i] : ds_all;
         auto f = ds_index.find(h);
@@ -208,6 +210,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         }
         prog_ds[i] = f->second;
     }
+    if (table_lock.owns_lock()) table_lock.unlock();
     // encode: each program only in the form its kernel needs, in parallel
     // for large populations
     for (uint32_t i = 0; i < n; ++i)
@@ -216,14 +219,14 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             return fail(RSR_EINVAL, "population offsets decrease at " + std::to_string(i));
     const bool fuse = (ctx->opts.flags & RSR_OPT_NO_LOAD_FUSION) == 0;
     const unsigned forms = gradient ? (FORM_TAPE | FORM_ADJ) : kernel == RSR_KERNEL_PLAIN ? FORM_SLOT : FORM_ACC;
-    if (ctx->enc_cache.size() < n) {
-        ctx->enc_cache.resize(n);
-        ctx->enc_rc.resize(n);
-        ctx->enc_msg.resize(n);
+    std::vector<EncodedProgram> &enc = scratch ? scratch->enc : ctx->enc_cache;
+    std::vector<int> &erc = scratch ? scratch->rc : ctx->enc_rc;
+    std::vector<std::string> &emsg = scratch ? scratch->msg : ctx->enc_msg;
+    if (enc.size() < n) {
+        enc.resize(n);
+        erc.resize(n);
+        emsg.resize(n);
     }
-    std::vector<EncodedProgram> &enc = ctx->enc_cache;
-    std::vector<int> &erc = ctx->enc_rc;
-    std::vector<std::string> &emsg = ctx->enc_msg;
     auto encode_one = [&](uint32_t i, unsigned f) {
         const uint64_t c0 = pop.code_off[i], k0 = pop.kind_off[i], p0 = pop.param_off[i];
         erc[i] = encode_program(pop.code + c0, (uint32_t)(pop.code_off[i + 1] - c0), pop.const_kinds + k0,
@@ -232,11 +235,13 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                                 &emsg[i], fuse, f);
     };
     if (n >= 256) {
-        if (!ctx->encoders)
-            ctx->encoders = std::make_unique<TaskPool>(std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+        std::unique_ptr<TaskPool> &pool = scratch ? scratch->pool : ctx->encoders;
+        if (!pool)
+            pool = std::make_unique<TaskPool>(
+                scratch ? scratch->threads : std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
         // programs in blocks of 16 per task
         const uint32_t nb = (n + 15) / 16;
-        ctx->encoders->run(nb, [&](uint32_t b) {
+        pool->run(nb, [&](uint32_t b) {
             for (uint32_t i = b * 16; i < std::min(n, b * 16 + 16); ++i) encode_one(i, forms);
         });
     } else {
@@ -405,7 +410,9 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             // the largest dataset's choice.
             uint64_t max_eval = 0;
             for (uint32_t j = li; j < end; ++j) max_eval = std::max(max_eval, P.datasets[P.progs[j].dataset].n_eval);
+            if (table_mu) table_lock = std::unique_lock<std::mutex>(*table_mu);
             TuneChoice c = choice_for(ctx, g.profile, max_eval);
+            if (table_lock.owns_lock()) table_lock.unlock();
             g.P = c.P;
             g.G = c.G;
             P.n_reg += end - li;

@@ -226,9 +226,22 @@ struct rsr_batch {
 };
 
 namespace rsr {
+// Encoding storage and threads of one planner: a caller that plans with its
+// own (a serving slot) needs the context's lock only for the dataset and
+// tuning tables, not for the encoding.
+struct EncodeScratch {
+    std::vector<EncodedProgram> enc;
+    std::vector<int> rc;
+    std::vector<std::string> msg;
+    std::unique_ptr<TaskPool> pool;
+    unsigned threads = 4;
+};
 // Planning and execution (runtime.cu), shared with the serving loop.
+// scratch == nullptr: the context's own encoding storage and threads (the
+// caller holds ctx->mu).  With scratch, table_mu (ctx->mu) is taken only
+// around the reads of the context's dataset and tuning tables.
 int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_prog, uint64_t ds_all, int kernel,
-               bool gradient, int mode, Plan *plan);
+               bool gradient, int mode, Plan *plan, EncodeScratch *scratch = nullptr, std::mutex *table_mu = nullptr);
 int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st);
 // A zero-filled resident dataset of the given shape (columns padded to the
 // stride), and its registration in the context's table (caller holds ctx->mu).

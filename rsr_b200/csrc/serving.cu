@@ -78,6 +78,7 @@ using JobPtr = std::shared_ptr<Job>;
 
 struct Slot {
     cudaStream_t st = nullptr;
+    EncodeScratch enc;  // the slot plans with its own encoding storage and threads
     DevicePlan dev;
     FitWorkspace fit;
     std::vector<float> host;
@@ -202,11 +203,8 @@ int run_eval(rsr_server *S, Slot &slot, const std::vector<JobPtr> &batch) {
     rsr_population pop{n, code.data(), code_off.data(), kinds.data(), kind_off.data(), params.data(),
                        param_off.data()};
     Plan plan;
-    int rc;
-    {
-        std::lock_guard<std::mutex> lk(ctx->mu);
-        rc = build_plan(ctx, pop, dsp.data(), 0, RSR_KERNEL_AUTO, gradient, MODE_MSE, &plan);
-    }
+    // ctx->mu only around the dataset and tuning tables: slots encode in parallel
+    int rc = build_plan(ctx, pop, dsp.data(), 0, RSR_KERNEL_AUTO, gradient, MODE_MSE, &plan, &slot.enc, &ctx->mu);
     if (rc) return rc;
     if ((rc = upload_plan(ctx, plan, &slot.dev, slot.st))) return rc;
     if ((rc = enqueue_plan(ctx, plan, &slot.dev, slot.st, nullptr))) return rc;
