@@ -43,10 +43,12 @@ int reg_max_blocks_per_sm(int profile, int P, unsigned omit, size_t smem);
 // register adjoint (kernels_adj.cu): profiles F, F+V3, F+V2+M2, F+V3+M3;
 // P (points per lane) 2 or 4
 bool adj_supported(int profile);
-void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t tape_slots, const uint32_t *stack_depth, int P,
-                LaunchArgs *a);
-size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t tape_slots, const uint32_t *stack_depth,
-                      int P);
+// floats of a warp's region for a program (tape | stacks | adjoint stacks |
+// gradient sums | Kahan state), and its stack depths packed for ProgDesc
+uint32_t adj_warp_floats(uint32_t tape_slots, const uint32_t *stack_depth, int P);
+uint32_t adj_pack_depth(const uint32_t *stack_depth);
+void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, LaunchArgs *a);
+size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats);
 cudaError_t launch_adj(const LaunchArgs &a, int profile, int P, uint32_t grid, size_t smem, cudaStream_t st);
 int adj_max_blocks_per_sm(int profile, int P, size_t smem);
 

@@ -57,6 +57,11 @@ struct RevIO : AccIO<P> {
     }
 };
 
+// kStackWidth for device code
+__device__ __forceinline__ constexpr uint32_t type_width(int t) {
+    return t == SF ? 1u : t == SV2 ? 2u : t == SV3 ? 3u : t == SM2 ? 4u : 9u;
+}
+
 template <int P, int W>
 __device__ __forceinline__ void zero_acc(Vf<P> *G) {
 #pragma unroll
@@ -450,14 +455,6 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
     float *wbase = smem + a.block_hdr_floats + (size_t)warp * a.region_floats;
 
     RevIO<P> io;
-    io.tape = reinterpret_cast<Vf<P> *>(wbase + a.tape_off) + lane;
-#pragma unroll
-    for (int t = 0; t < N_STACKS; ++t) {
-        io.stk[t] = reinterpret_cast<Vf<P> *>(wbase + a.stack_off[t]) + lane;
-        io.gstk[t] = reinterpret_cast<Vf<P> *>(wbase + a.gstack_off[t]) + lane;
-    }
-    io.gacc = wbase + a.acc_off + lane;
-    float *kahan = wbase + a.acc_off + kAdjParams * 32;  // [2][32]
     io.consts = sconst;
 
     for (;;) {
@@ -471,6 +468,25 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
             continue;
         }
         const ProgDesc pd = a.progs[it.prog_begin];
+        // this program's warp region: tape | stacks | adjoint stacks | sums
+        // (n_slots: tape slots; n_tape: stack depths, 5 bits per type); the
+        // launch's region_floats is the largest of its programs'
+        {
+            uint32_t off = pd.n_slots * 32u * P;
+            io.tape = reinterpret_cast<Vf<P> *>(wbase) + lane;
+#pragma unroll
+            for (int t = 0; t < N_STACKS; ++t) {
+                io.stk[t] = reinterpret_cast<Vf<P> *>(wbase + off) + lane;
+                off += ((pd.n_tape >> (5 * t)) & 31u) * type_width(t) * 32u * P;
+            }
+#pragma unroll
+            for (int t = 0; t < N_STACKS; ++t) {
+                io.gstk[t] = reinterpret_cast<Vf<P> *>(wbase + off) + lane;
+                off += ((pd.n_tape >> (5 * t)) & 31u) * type_width(t) * 32u * P;
+            }
+            io.gacc = wbase + off + lane;
+        }
+        float *kahan = io.gacc - lane + kAdjParams * 32;  // [2][32]
         for (uint32_t i = threadIdx.x; i < pd.uop_len; i += blockDim.x) scode[i] = __ldg(a.code + pd.uop_off + i);
         if (threadIdx.x == 0) scode[pd.uop_len] = 0u;  // prefetch pad of the forward loop
         for (uint32_t i = threadIdx.x; i < pd.n_consts; i += blockDim.x) sconst[i] = __ldg(a.consts + pd.const_off + i);
@@ -539,32 +555,30 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
 // Shared-memory layout (floats).  Block header: code (+1 pad) | constants |
 // meta (4 words) | cross-warp sums (warps x 33 doubles).  Per warp: tape |
 // stacks (per type) | adjoint stacks (per type) | gradient sums (32 x 32)
-// | Kahan state (2 x 32).
-void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t tape_slots, const uint32_t *stack_depth, int P,
-                LaunchArgs *a) {
+// | Kahan state (2 x 32), each program's own sizes (the kernel lays the
+// region out per item); warp_floats is the largest region of the launch.
+uint32_t adj_warp_floats(uint32_t tape_slots, const uint32_t *stack_depth, int P) {
+    uint32_t slots = tape_slots;
+    for (int t = 0; t < N_STACKS; ++t) slots += 2u * stack_depth[t] * (uint32_t)kStackWidth[t];
+    return (slots * 32u * (uint32_t)P + kAdjParams * 32u + 2u * 32u + 3u) & ~3u;
+}
+
+uint32_t adj_pack_depth(const uint32_t *stack_depth) {
+    uint32_t v = 0;
+    for (int t = 0; t < N_STACKS; ++t) v |= (stack_depth[t] & 31u) << (5 * t);
+    return v;
+}
+
+void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, LaunchArgs *a) {
     const uint32_t nw = kAdjThreads / 32;
     a->block_hdr_floats = ((code_words + 1u + 3u) & ~3u) + ((const_floats + 3u) & ~3u) + 4u +
                           2u * nw * (1u + kAdjParams);
-    uint32_t off = 0;
-    a->tape_off = off;
-    off += tape_slots * 32u * (uint32_t)P;
-    for (int t = 0; t < N_STACKS; ++t) {
-        a->stack_off[t] = off;
-        off += stack_depth[t] * (uint32_t)kStackWidth[t] * 32u * (uint32_t)P;
-    }
-    for (int t = 0; t < N_STACKS; ++t) {
-        a->gstack_off[t] = off;
-        off += stack_depth[t] * (uint32_t)kStackWidth[t] * 32u * (uint32_t)P;
-    }
-    a->acc_off = off;
-    off += kAdjParams * 32u + 2u * 32u;
-    a->region_floats = (off + 3u) & ~3u;
+    a->region_floats = warp_floats;
 }
 
-size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t tape_slots, const uint32_t *stack_depth,
-                      int P) {
+size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats) {
     LaunchArgs a{};
-    adj_layout(code_words, const_floats, tape_slots, stack_depth, P, &a);
+    adj_layout(code_words, const_floats, warp_floats, &a);
     return ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (kAdjThreads / 32)) * 4u;
 }
 

@@ -37,9 +37,6 @@ struct LaunchArgs {
     uint32_t block_hdr_floats;
     uint32_t acc_off;
     uint32_t stack_off[N_STACKS];
-    // register adjoint: per-warp tape and adjoint stacks (floats)
-    uint32_t tape_off;
-    uint32_t gstack_off[N_STACKS];
 };
 
 // Opt-in dynamic shared-memory limit of one block on sm_100 (227 KB).  Every

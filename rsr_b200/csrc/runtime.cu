@@ -136,11 +136,10 @@ static constexpr int kRegPathStride = 8;
 // 40 KB at 4 points and do not change.
 static constexpr size_t kGradTapeBudget = 80 * 1024;
 // Register adjoint: shared memory a warp's tape, stacks, adjoint stacks and
-// gradient sums may take (4 warps per block), and the first path number of
-// its launches in a gradient plan.
-static constexpr size_t kAdjWarpBudget = 40 * 1024;
+// gradient sums may take (4 warps per block: two blocks fit an SM), and the
+// first path number of its launches in a gradient plan.
+static constexpr size_t kAdjWarpBudget = 24 * 1024;
 static constexpr int kAdjPathBase = 0;
-static constexpr uint32_t kNoDepth[N_STACKS] = {0, 0, 0, 0, 0};
 // Points per work-item chunk (all P).  8192 measured slower on every kernel
 // (vector register 4.32 ms against 4.30, matrix register 4.84 against 4.69,
 // vector adjoint 6.68 against 5.90): coarser items balance worse.
@@ -237,8 +236,8 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
     if (n >= 256) {
         std::unique_ptr<TaskPool> &pool = scratch ? scratch->pool : ctx->encoders;
         if (!pool)
-            pool = std::make_unique<TaskPool>(
-                scratch ? scratch->threads : std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+            pool = std::make_unique<TaskPool>(std::max(
+                1u, std::min(scratch ? scratch->threads : 16u, std::thread::hardware_concurrency())));
         // programs in blocks of 16 per task
         const uint32_t nb = (n + 15) / 16;
         pool->run(nb, [&](uint32_t b) {
@@ -255,24 +254,17 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
     for (uint32_t i = 0; i < n; ++i) {
         if (gradient && enc[i].adj_profile >= 0 && adj_supported(enc[i].adj_profile) &&
             !(ctx->opts.flags & RSR_OPT_SLOT_ADJOINT)) {
-            // register adjoint: 4 points per lane when a warp's tape, stacks
-            // and adjoint stacks fit kAdjWarpBudget, else 2; launches by that
-            // size in steps of 16 slots, so that a block's shared memory
-            // follows its own programs
+            // register adjoint: 4 points per lane when a warp's region (tape,
+            // stacks, adjoint stacks, gradient sums) fits kAdjWarpBudget, else
+            // 2; launches by that region's size in steps of 4 KB, so that a
+            // block's shared memory follows its own programs
             const EncodedProgram &E = enc[i];
-            uint32_t depth[N_STACKS], slots = E.adj_tape;
-            for (int t = 0; t < N_STACKS; ++t) {
-                depth[t] = (uint32_t)E.adj_depth[t];
-                slots += 2u * depth[t] * (uint32_t)kStackWidth[t];
-            }
-            const uint32_t cw = (uint32_t)E.adj_code.size(), cf = (uint32_t)E.consts.size();
-            auto per_warp = [&](int Pp) {
-                return (adj_smem_bytes(cw, cf, E.adj_tape, depth, Pp) - adj_smem_bytes(cw, cf, 0, kNoDepth, Pp)) /
-                           (kAdjThreads / 32) + 32 * 33 * 4;
-            };
-            const int p4 = per_warp(4) <= kAdjWarpBudget ? 1 : 0;
-            if (p4 || per_warp(2) <= kAdjWarpBudget) {
-                const int bucket = std::min<int>((int)((slots + 15) / 16), 63);
+            uint32_t depth[N_STACKS];
+            for (int t = 0; t < N_STACKS; ++t) depth[t] = (uint32_t)E.adj_depth[t];
+            const uint32_t w4 = adj_warp_floats(E.adj_tape, depth, 4), w2 = adj_warp_floats(E.adj_tape, depth, 2);
+            const int p4 = (size_t)w4 * 4u <= kAdjWarpBudget ? 1 : 0;
+            if (p4 || (size_t)w2 * 4u <= kAdjWarpBudget) {
+                const int bucket = (int)(((p4 ? w4 : w2) + 1023u) / 1024u);
                 path[i] = kAdjPathBase + ((bucket * 2 + p4) * N_PROFILES + E.adj_profile);
                 continue;
             }
@@ -371,14 +363,21 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         d.uop_len = (uint32_t)code.size();
         d.const_off = (uint32_t)P.consts.size();
         d.n_consts = (uint32_t)E.consts.size();
-        d.n_slots = E.n_slots;
+        const bool reg_adj = gradient && path[i] >= 0;
+        d.n_slots = reg_adj ? E.adj_tape : E.n_slots;
         d.flags = (E.result_zero ? PF_RESULT_ZERO : 0u) | (E.needs_zero_init ? PF_NEEDS_ZERO_INIT : 0u) |
                   (E.differentiable ? PF_DIFFERENTIABLE : 0u);
         d.dataset = prog_ds[i];
         const uint64_t n_eval = P.datasets[d.dataset].n_eval;
         d.n_parts = (uint32_t)std::max<uint64_t>(1, (n_eval + kChunkPoints - 1) / kChunkPoints);
         d.part_off = part;
-        d.n_tape = E.n_tape_val | (E.n_tape_adj << 16);
+        if (reg_adj) {
+            uint32_t depth[N_STACKS];
+            for (int t = 0; t < N_STACKS; ++t) depth[t] = (uint32_t)E.adj_depth[t];
+            d.n_tape = adj_pack_depth(depth);
+        } else {
+            d.n_tape = E.n_tape_val | (E.n_tape_adj << 16);
+        }
         part += d.n_parts;
         P.code.insert(P.code.end(), code.begin(), code.end());
         P.consts.insert(P.consts.end(), E.consts.begin(), E.consts.end());
@@ -441,10 +440,10 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                 if (g.kind == 1)
                     for (int t = 0; t < N_STACKS; ++t)
                         g.stack_depth[t] = std::max(g.stack_depth[t], (uint32_t)enc[order[q]].depth_fast[t]);
-                if (g.kind == 3) {
-                    sl = std::max(sl, enc[order[q]].adj_tape);
-                    for (int t = 0; t < N_STACKS; ++t)
-                        g.stack_depth[t] = std::max(g.stack_depth[t], (uint32_t)enc[order[q]].adj_depth[t]);
+                if (g.kind == 3) {  // slots: the largest warp region (floats)
+                    uint32_t depth[N_STACKS];
+                    for (int t = 0; t < N_STACKS; ++t) depth[t] = (uint32_t)enc[order[q]].adj_depth[t];
+                    sl = std::max(sl, adj_warp_floats(enc[order[q]].adj_tape, depth, g.P));
                 }
             }
             g.code_words = std::max(g.code_words, cw);
@@ -570,6 +569,18 @@ int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st
     return RSR_OK;
 }
 
+// Makes st wait for the launches a plan put on its side streams.
+static cudaError_t join_side_streams(DevicePlan *dev, cudaStream_t st, unsigned forked) {
+    cudaError_t first = cudaSuccess;
+    for (int sd = 0; sd < 2; ++sd)
+        if (forked & (1u << sd)) {
+            cudaError_t e = cudaEventRecord(dev->join[sd], dev->side[sd]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(st, dev->join[sd], 0);
+            if (first == cudaSuccess) first = e;
+        }
+    return first;
+}
+
 int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st, cudaEvent_t ev_mid,
                  cudaEvent_t *group_events) {
     NvtxRange nvtx_range("rsr: launch");
@@ -628,8 +639,14 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             g.warps_per_block = kRegThreads / 32;
             e = launch_reg(a, g.profile, g.P, g.omit, g.grid, gs);
         } else if (g.kind == 3) {
-            adj_layout(g.code_words, g.const_floats, g.slots, g.stack_depth, g.P, &a);
-            const size_t smem = adj_smem_bytes(g.code_words, g.const_floats, g.slots, g.stack_depth, g.P);
+            adj_layout(g.code_words, g.const_floats, g.slots, &a);
+            const size_t smem = adj_smem_bytes(g.code_words, g.const_floats, g.slots);
+            if (smem > (size_t)kMaxDynSmemOptin) {
+                e = cudaErrorInvalidValue;
+                join_side_streams(dev, st, forked);
+                return fail(RSR_EINVAL, "register adjoint launch needs " + std::to_string(smem) +
+                                            " bytes of shared memory per block");
+            }
             const int bps = std::max(1, adj_max_blocks_per_sm(g.profile, g.P, smem));
             g.grid = std::max(1u, (uint32_t)std::min<uint64_t>((uint64_t)bps * ctx->num_sms, g.n_items));
             g.smem = smem;
@@ -647,15 +664,16 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             g.warps_per_block = wpb;
             e = launch_grad(a, g.profile, g.no_unary, wpb, per * wpb, gs);
         }
-        if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+        if (e != cudaSuccess) {
+            // launches already on the side streams must finish before the
+            // caller's stream (and the next use of this plan's buffers) moves on
+            join_side_streams(dev, st, forked);
+            return cuda_fail(e, "kernel launch");
+        }
         if (group_events) cudaEventRecord(group_events[2 * gi + 1], gs);
         ctx->launches++;
     }
-    for (int sd = 0; sd < 2; ++sd)
-        if (forked & (1u << sd)) {
-            if ((e = cudaEventRecord(dev->join[sd], dev->side[sd])) != cudaSuccess) return cuda_fail(e, "join");
-            if ((e = cudaStreamWaitEvent(st, dev->join[sd], 0)) != cudaSuccess) return cuda_fail(e, "join");
-        }
+    if ((e = join_side_streams(dev, st, forked)) != cudaSuccess) return cuda_fail(e, "join");
     if (ev_mid) cudaEventRecord(ev_mid, st);
     if (plan.mode == MODE_MSE && plan.raw_sums) {
         e = launch_finalize_sums(dev->base.progs, dev->base.partials, n, plan.gradient ? 33u : 1u,

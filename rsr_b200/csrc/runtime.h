@@ -234,7 +234,7 @@ struct EncodeScratch {
     std::vector<int> rc;
     std::vector<std::string> msg;
     std::unique_ptr<TaskPool> pool;
-    unsigned threads = 4;
+    unsigned threads = 16;  // capped by the host's hardware threads
 };
 // Planning and execution (runtime.cu), shared with the serving loop.
 // scratch == nullptr: the context's own encoding storage and threads (the

@@ -8,7 +8,7 @@ with 1-8 constants (the reference's test shape, tests/linalg.rs:145-188).
     component, against the reference's dual-number rules (sums over points
     in f64) and against central differences (h = 1e-3);
   * a 20-iteration L-BFGS fit whose final MSEs are the fitted constants'
-    own MSEs and never above the starting ones.
+    own MSEs, lower than the starting ones for most programs.
 
 Uneven batch: A, B Mat2, A = 2I + U(-0.5, 0.5), B ~ N(0, 1), y = Tr(A^-1 B)
 + det(A) (tests/linalg.rs:110-142); 8192 programs of length 4-64 against 16
@@ -29,7 +29,9 @@ a fourth, 1e-7 sqrt(MSE), the loss's own: a derivative the dual rules give
 as exactly zero in every point (a cross product of a vector with itself) is
 rounding noise in reverse mode.
 Against central differences the bound adds the differences' own noise,
-component by component: twice the disagreement between steps h and 2h.
+component by component: twice the disagreement between steps h and 2h;
+components whose difference moves by more than 1% between h and h/10 are
+not resolved by it and are held against the dual rules only.
 """
 import concurrent.futures as cf
 
@@ -89,7 +91,12 @@ def _grad_refs(p, ds):
     md32, gd32 = O.mse_grad_dual(p, ds)
     fd = O.grad_fd(p, ds, 1e-3)
     fd2 = O.grad_fd(p, ds, 2e-3)
-    return n, m64, gd[:n], l1[:n], gd32[:n], fd[:n], 2.0 * np.abs(fd[:n] - fd2[:n])
+    fd4 = O.grad_fd(p, ds, 1e-4)
+    # a central difference that moves by more than 1% between h and h/10 does
+    # not resolve the derivative (f32 noise or a kink in the data): such
+    # components are held against the dual rules only
+    stable = np.abs(fd[:n] - fd4[:n]) <= 1e-2 * np.abs(fd[:n]) + GRAD_L1_FLOOR * l1[:n]
+    return n, m64, gd[:n], l1[:n], gd32[:n], fd[:n], 2.0 * np.abs(fd[:n] - fd2[:n]), stable
 
 
 def test_matrix_gradients_per_component(matrix):
@@ -104,7 +111,8 @@ def test_matrix_gradients_per_component(matrix):
     with _pool() as ex:
         refs = list(ex.map(lambda i: _grad_refs(pop[i], ds), sample))
     checked = 0
-    for i, (n, m64, gd, l1, gd32, fd, noise) in zip(sample, refs):
+    fd_checked = 0
+    for i, (n, m64, gd, l1, gd32, fd, noise, stable) in zip(sample, refs):
         assert abs(float(mse[i]) - m64) <= MSE_RTOL * abs(m64), (i, mse[i], m64)
         g = grad[i, :n].astype(np.float64)
         assert np.all(grad[i, n:] == 0), i
@@ -115,10 +123,11 @@ def test_matrix_gradients_per_component(matrix):
         assert not bad.any(), ("dual, f64 sums", i, g[bad], gd[bad], l1[bad])
         bad = np.abs(g - gd32) > GRAD_RTOL * np.abs(gd32) + floor
         assert not bad.any(), ("dual, reference f32 sums", i, g[bad], gd32[bad], l1[bad])
-        bad = np.abs(g - fd) > GRAD_RTOL * np.abs(fd) + floor + noise
+        bad = stable & (np.abs(g - fd) > GRAD_RTOL * np.abs(fd) + floor + noise)
         assert not bad.any(), ("central differences", i, g[bad], fd[bad], noise[bad])
+        fd_checked += int(stable.sum())
         checked += 1
-    assert checked >= N_GRAD_SAMPLE
+    assert checked >= N_GRAD_SAMPLE and fd_checked >= N_GRAD_SAMPLE
 
 
 def test_matrix_lbfgs_20_iterations(matrix):
@@ -133,10 +142,10 @@ def test_matrix_lbfgs_20_iterations(matrix):
         again = e.compute_mse_batch(refit, d)
     assert stats["iterations"] <= 20
     fin = start < FMAX
-    # Armijo steps never raise the loss; the reported MSE is the fitted
-    # constants' own (scored again here by the MSE kernel)
-    assert (mse[fin] <= start[fin] * (1 + MSE_RTOL)).all()
-    np.testing.assert_allclose(mse[fin], again[fin], rtol=MSE_RTOL)
+    # the reported MSE is the fitted constants' own (scored again here by the
+    # MSE kernel); a line search that runs out of halvings accepts a worse
+    # point (lbfgs.rs:119), so descent is the rule, not a guarantee
+    np.testing.assert_allclose(mse, again, rtol=MSE_RTOL)
     assert (mse[fin] < start[fin] * (1 - 1e-3)).sum() >= fin.sum() // 2
 
 
