@@ -41,8 +41,9 @@ constexpr size_t kRegSmemBudget = 200 * 1024;  // at least one block per SM, bel
 int reg_max_blocks_per_sm(int profile, int P, unsigned omit, size_t smem);
 
 // register adjoint (kernels_adj.cu): profiles F, F+V3, F+V2+M2, F+V3+M3;
-// P (points per lane) 2 or 4
+// P (points per lane) 2, 4, or 8 up to adj_max_p(profile)
 bool adj_supported(int profile);
+int adj_max_p(int profile);
 // floats of a warp's region for a program (tape | stacks | adjoint stacks |
 // gradient sums | Kahan state), and its stack depths packed for ProgDesc
 uint32_t adj_warp_floats(uint32_t tape_slots, const uint32_t *stack_depth, int P);

@@ -602,7 +602,15 @@ static int adj_occ(size_t smem) {
 
 bool adj_supported(int profile) { return profile >= P_F && profile <= P_FV3M3; }
 
+// P = 8 exists for the F and F+V3 profiles only (the others would spill).
+int adj_max_p(int profile) { return profile == P_F || profile == P_FV3 ? 8 : 4; }
+
 cudaError_t launch_adj(const LaunchArgs &a, int profile, int P, uint32_t grid, size_t smem, cudaStream_t st) {
+    if (P >= 8) {
+        if (profile == P_F) return launch_adj_pp<P_F, 8>(a, grid, smem, st);
+        if (profile == P_FV3) return launch_adj_pp<P_FV3, 8>(a, grid, smem, st);
+        return cudaErrorInvalidValue;
+    }
     switch (profile * 2 + (P >= 4 ? 1 : 0)) {
         case 0: return launch_adj_pp<P_F, 2>(a, grid, smem, st);
         case 1: return launch_adj_pp<P_F, 4>(a, grid, smem, st);
@@ -617,6 +625,7 @@ cudaError_t launch_adj(const LaunchArgs &a, int profile, int P, uint32_t grid, s
 }
 
 int adj_max_blocks_per_sm(int profile, int P, size_t smem) {
+    if (P >= 8) return profile == P_F ? adj_occ<P_F, 8>(smem) : profile == P_FV3 ? adj_occ<P_FV3, 8>(smem) : 0;
     switch (profile * 2 + (P >= 4 ? 1 : 0)) {
         case 0: return adj_occ<P_F, 2>(smem);
         case 1: return adj_occ<P_F, 4>(smem);

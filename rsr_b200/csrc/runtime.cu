@@ -259,18 +259,18 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
     for (uint32_t i = 0; i < n; ++i) {
         if (gradient && enc[i].adj_profile >= 0 && adj_supported(enc[i].adj_profile) &&
             !(ctx->opts.flags & RSR_OPT_SLOT_ADJOINT)) {
-            // register adjoint: 4 points per lane when a warp's region (tape,
-            // stacks, adjoint stacks, gradient sums) fits kAdjWarpBudget, else
-            // 2; launches by that region's size in steps of 4 KB, so that a
-            // block's shared memory follows its own programs
+            // register adjoint: the most points per lane (8, 4, 2) whose warp
+            // region (tape, stacks, adjoint stacks, gradient sums) fits
+            // kAdjWarpBudget; launches by that region's size in steps of 4 KB,
+            // so that a block's shared memory follows its own programs
             const EncodedProgram &E = enc[i];
             uint32_t depth[N_STACKS];
             for (int t = 0; t < N_STACKS; ++t) depth[t] = (uint32_t)E.adj_depth[t];
-            const uint32_t w4 = adj_warp_floats(E.adj_tape, depth, 4), w2 = adj_warp_floats(E.adj_tape, depth, 2);
-            const int p4 = (size_t)w4 * 4u <= kAdjWarpBudget ? 1 : 0;
-            if (p4 || (size_t)w2 * 4u <= kAdjWarpBudget) {
-                const int bucket = (int)(((p4 ? w4 : w2) + 1023u) / 1024u);
-                path[i] = kAdjPathBase + ((bucket * 2 + p4) * N_PROFILES + E.adj_profile);
+            int pc = adj_max_p(E.adj_profile) >= 8 ? 2 : 1;  // points per lane 2 << pc: the most that fits
+            while (pc >= 0 && (size_t)adj_warp_floats(E.adj_tape, depth, 2 << pc) * 4u > kAdjWarpBudget) --pc;
+            if (pc >= 0) {
+                const int bucket = (int)((adj_warp_floats(E.adj_tape, depth, 2 << pc) + 1023u) / 1024u);
+                path[i] = kAdjPathBase + ((bucket * 3 + pc) * N_PROFILES + E.adj_profile);
                 continue;
             }
         }
@@ -408,7 +408,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         g.item_begin = (uint32_t)P.items.size();
         if (g.kind == 3) {
             g.G = 1;
-            g.P = ((pth - kAdjPathBase) / N_PROFILES) % 2 ? 4 : 2;
+            g.P = 2 << (((pth - kAdjPathBase) / N_PROFILES) % 3);
         } else if (g.kind == 1) {
             // P and G are per profile and dataset size; one launch uses one P,
             // the largest dataset's choice.
