@@ -102,8 +102,6 @@ typedef struct rsr_options {
 #define RSR_OPT_NO_LOAD_FUSION 1u   /* register kernel: keep loads as separate micro-ops */
 #define RSR_OPT_SLOT_ADJOINT 2u     /* gradients: the slot-file adjoint for every program (else the
                                        register adjoint where a program fits it) */
-#define RSR_OPT_PROGRAM_PER_WARP 4u /* register kernel: each warp of a block runs one of a work item's
-                                       8 programs on all its tiles (else as tuned) */
 
 /* ------------------------------------------------------------- context */
 RSR_API void rsr_options_default(rsr_options *opts);

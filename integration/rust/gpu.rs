@@ -30,7 +30,6 @@ pub const RSR_KERNEL_BATCHED: c_int = 2;
 
 pub const RSR_OPT_NO_LOAD_FUSION: u32 = 1;
 pub const RSR_OPT_SLOT_ADJOINT: u32 = 2;
-pub const RSR_OPT_PROGRAM_PER_WARP: u32 = 4;
 
 // --------------------------------------------------------- rsr_job_kind
 pub const RSR_JOB_MSE: u32 = 0;

@@ -18,7 +18,6 @@ STATUS_NAMES = ["OK", "EINVAL", "EPROGRAM", "ENOMEM", "ENODEV", "ECUDA", "ETIMED
 KERNEL_AUTO, KERNEL_PLAIN, KERNEL_BATCHED = 0, 1, 2
 OPT_NO_LOAD_FUSION = 1
 OPT_SLOT_ADJOINT = 2
-OPT_PROGRAM_PER_WARP = 4
 
 
 class RsrError(RuntimeError):

@@ -37,7 +37,6 @@ struct LaunchArgs {
     uint32_t block_hdr_floats;
     uint32_t acc_off;
     uint32_t stack_off[N_STACKS];
-    uint32_t warp_per_program;  // register kernel: warp w runs the item's program w on every tile
 };
 
 // Opt-in dynamic shared-memory limit of one block on sm_100 (227 KB).  Every

@@ -181,22 +181,12 @@ __global__ void __launch_bounds__(kRegThreads, reg_min_blocks<PROF, P, OMIT>()) 
         const DatasetDesc ds = a.datasets[a.progs[it.prog_begin].dataset];
         io.stride = (uint32_t)ds.stride;
         Acc<PROF, P> acc;
-        // Two shapes: the warps split the item's tiles and run every program
-        // on each (features shared by the programs of a warp), or warp w runs
-        // program w on every tile (features shared by the warps of a block,
-        // which move through the tiles together).  Either way each program's
-        // per-lane sums end in its cross-warp reduction below (other warps add
-        // zeros), in a fixed order.
-        const bool wpp = a.warp_per_program != 0;
-        const uint32_t g_first = wpp ? (uint32_t)warp : 0u, g_end = wpp ? min((uint32_t)warp + 1u, G) : G;
-        const uint32_t t_first = wpp ? (g_first < g_end ? it.tile_begin : it.tile_end) : it.tile_begin + warp;
-        const uint32_t t_step = wpp ? 1u : (uint32_t)nw;
-        for (uint32_t tile = t_first; tile < it.tile_end; tile += t_step) {
+        for (uint32_t tile = it.tile_begin + warp; tile < it.tile_end; tile += nw) {
             const uint64_t p0 = (uint64_t)tile * (32u * P) + (uint64_t)lane * P;
             io.xl = ds.x + p0;
             const Vf<P> y = load_pts<P>(ds.y + p0);
             const bool full = p0 + P <= ds.n_eval;
-            for (uint32_t g = g_first; g < g_end; ++g) {
+            for (uint32_t g = 0; g < G; ++g) {
                 if (a.active && !a.active[it.prog_begin + g]) continue;
                 io.consts = sconst + meta[3 * g + 2];
                 run_program<PROF, P, OMIT>(acc, io, scode + meta[3 * g], meta[3 * g + 1]);

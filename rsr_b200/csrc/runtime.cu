@@ -171,18 +171,13 @@ static TuneChoice choice_for(rsr_ctx *ctx, int profile, uint64_t n_eval) {
     auto it = ctx->tune.find({profile, log2_bucket(n_eval)});
     if (it != ctx->tune.end()) c = it->second;
     if (ctx->opts.points_per_thread > 0) c.P = ctx->opts.points_per_thread;
-    if (ctx->opts.programs_per_warp > 0) {
-        c.G = ctx->opts.programs_per_warp;
-        c.wpp = 0;
-    }
-    if (ctx->opts.flags & RSR_OPT_PROGRAM_PER_WARP) c.wpp = 1;
+    if (ctx->opts.programs_per_warp > 0) c.G = ctx->opts.programs_per_warp;
     if (ctx->force.P > 0) c = ctx->force;
     // variants that exist (kernels_reg.cu): P in {2, 4, 8} up to reg_max_p
     const int maxP = reg_max_p(profile);
     if (c.P > maxP) c.P = maxP;
     if (c.P != 2 && c.P != 4 && c.P != 8) c.P = c.P < 2 ? 2 : 4;
     c.G = std::max(1, std::min(c.G, 8));
-    if (c.wpp) c.G = kRegThreads / 32;  // one program per warp of the block
     return c;
 }
 
@@ -419,7 +414,6 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             if (table_lock.owns_lock()) table_lock.unlock();
             g.P = c.P;
             g.G = c.G;
-            g.wpp = c.wpp;
             P.n_reg += end - li;
         } else if (g.kind == 0) {
             g.G = 1;
@@ -637,7 +631,6 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
         } else if (g.kind == 1) {
             reg_layout(g.code_words, g.const_floats, g.stack_depth, g.P, g.G, a.stack_off, &a.acc_off, &a.region_floats,
                        &a.block_hdr_floats);
-            a.warp_per_program = (uint32_t)g.wpp;
             const size_t smem = ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (kRegThreads / 32)) * 4u;
             int bps = std::max(1, reg_max_blocks_per_sm(g.profile, g.P, g.omit, smem));
             uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)bps * ctx->num_sms, g.n_items);
@@ -1234,7 +1227,7 @@ int rsr_batch_describe(rsr_ctx *ctx, rsr_batch *b, char *buf, size_t len) {
              ", \"no_unary\": " + ((g.kind == 1 ? (g.omit & 1u) != 0 : g.no_unary) ? "true" : "false") +
              ", \"no_matrix_operand\": " + ((g.kind == 1 && (g.omit & 2u)) ? "true" : "false") +
              ", \"points_per_thread\": " + std::to_string(g.P) + ", \"programs_per_warp\": " + std::to_string(g.G) +
-             ", \"program_per_warp\": " + (g.wpp ? "true" : "false") + ", \"items\": " + std::to_string(g.n_items) + ", \"flops\": " + std::to_string(g.flops) +
+             ", \"items\": " + std::to_string(g.n_items) + ", \"flops\": " + std::to_string(g.flops) +
              ", \"program_points\": " + std::to_string(g.program_points) + ", \"grid\": " + std::to_string(g.grid) +
              ", \"warps_per_block\": " + std::to_string(g.warps_per_block) + ", \"smem_bytes\": " +
              std::to_string(g.smem) + ", \"last_ms\": " +
@@ -1307,17 +1300,9 @@ int rsr_autotune(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const 
     DevicePlan dev;
     std::vector<cudaEvent_t> ev;
     int rc = RSR_OK;
-    // candidates: P x G with the warps splitting an item's tiles, and P with
-    // one program per warp (G = 8)
-    std::vector<TuneChoice> cands;
-    for (int P : Ps) {
-        for (int G : Gs) cands.push_back(TuneChoice{P, G, 0});
-        cands.push_back(TuneChoice{P, kRegThreads / 32, 1});
-    }
-    for (const TuneChoice &cand : cands) {
-        const int P = cand.P, G = cand.G;
-        {
-            ctx->force = cand;
+    for (int P : Ps)
+        for (int G : Gs) {
+            ctx->force = TuneChoice{P, G};
             Plan plan;
             rc = build_plan(ctx, *pop, dsp, ds, RSR_KERNEL_BATCHED, false, MODE_MSE, &plan);
             if (!rc) rc = upload_plan(ctx, plan, &dev, ctx->stream);
@@ -1355,16 +1340,15 @@ int rsr_autotune(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const 
                 Best &b = best[kv.first];
                 if (kv.second.first < b.ms) {
                     b.ms = kv.second.first;
-                    b.c = cand;
+                    b.c = TuneChoice{P, G};
                     b.bucket = log2_bucket(kv.second.second);
                 }
                 rep += std::string(first ? "" : ", ") + "{\"profile\": " + std::to_string(kv.first) +
                        ", \"P\": " + std::to_string(P) + ", \"G\": " + std::to_string(G) +
-                       ", \"wpp\": " + std::to_string(cand.wpp) + ", \"ms\": " + std::to_string(kv.second.first) + "}";
+                       ", \"ms\": " + std::to_string(kv.second.first) + "}";
                 first = false;
             }
         }
-    }
     ctx->force = TuneChoice{};
     for (auto &e : ev) cudaEventDestroy(e);
     dev.pool.release(); dev.partials.release(); dev.out.release(); dev.counters.release();
@@ -1374,8 +1358,8 @@ int rsr_autotune(rsr_ctx *ctx, const rsr_population *pop, rsr_dataset ds, const 
     for (auto &kv : best) {
         ctx->tune[{kv.first, kv.second.bucket}] = kv.second.c;
         rep += std::string(first ? "" : ", ") + "{\"profile\": " + std::to_string(kv.first) + ", \"P\": " +
-               std::to_string(kv.second.c.P) + ", \"G\": " + std::to_string(kv.second.c.G) + ", \"wpp\": " +
-               std::to_string(kv.second.c.wpp) + ", \"ms\": " + std::to_string(kv.second.ms) + "}";
+               std::to_string(kv.second.c.P) + ", \"G\": " + std::to_string(kv.second.c.G) + ", \"ms\": " +
+               std::to_string(kv.second.ms) + "}";
         first = false;
     }
     rep += "]}";

@@ -95,7 +95,6 @@ struct DatasetRec {
 struct TuneChoice {
     int P = 0;
     int G = 0;
-    int wpp = 0;  // 1: each warp of a block runs one of the item's G = 8 programs on all its tiles
 };
 
 // One kernel launch inside a plan.
@@ -106,7 +105,6 @@ struct Group {
     bool no_unary = false;  // adjoint kernel: no unary Float op in the launch's programs
     int P = 4;
     int G = 1;
-    int wpp = 0;            // register kernel: one program per warp (TuneChoice::wpp)
     uint32_t item_begin = 0, n_items = 0;  // into the plan's item array
     uint32_t code_words = 0, const_floats = 0, slots = 0;  // per-warp staging maxima
     uint32_t adj_slots = 0;                                  // adjoint kernel: adjoint slots

@@ -341,23 +341,3 @@ def test_register_and_slot_adjoints_agree(wl):
         scale = np.abs(g2[i, :n]).max()
         assert (np.abs(g1[i, :n] - g2[i, :n]) <= 1e-3 * np.abs(g2[i, :n]) + 1e-5 * scale + 1e-30).all(), \
             (wl, i, g1[i, :n], g2[i, :n])
-
-
-@pytest.mark.parametrize("ppt", [2, 4, 8])
-def test_program_per_warp_shape(ppt):
-    """The register kernel's other launch shape (each warp of a block runs one
-    of an item's 8 programs on all its tiles): points bit-identical to the
-    oracle, MSE within 1e-6 of FP64, on every workload."""
-    with Engine(points_per_thread=ppt, flags=N.OPT_PROGRAM_PER_WARP) as e:
-        for wl in ("scalar", "lorentz", "transform", "inverse"):
-            ds, pop = WORKLOADS[wl][0](), WORKLOADS[wl][1]()
-            got = e.eval_points_batch(pop, ds)
-            want = oracle_points(pop, ds)
-            for i in range(len(pop)):
-                assert same_bits(got[i], want[i]), (wl, ppt, i)
-            m64, _ = O.mse_batch(I.pack(pop), ds)
-            check_mse(e.compute_mse_batch(pop, ds), m64, ds.num_samples)
-            b = e.prepare(pop, ds)
-            shapes = {g["program_per_warp"] for g in b.describe()["groups"] if g["kernel"] == "register"}
-            b.close()
-            assert shapes == {True}, (wl, shapes)
