@@ -486,11 +486,11 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
             }
             io.gacc = wbase + off + lane;
         }
-        float *kahan = io.gacc - lane + kAdjParams * 32;  // [2][32]
+        const uint32_t np = min(pd.n_consts, kAdjParams);
+        float *kahan = io.gacc - lane + np * 32u;  // [2][32], after the program's own gradient sums
         for (uint32_t i = threadIdx.x; i < pd.uop_len; i += blockDim.x) scode[i] = __ldg(a.code + pd.uop_off + i);
         if (threadIdx.x == 0) scode[pd.uop_len] = 0u;  // prefetch pad of the forward loop
         for (uint32_t i = threadIdx.x; i < pd.n_consts; i += blockDim.x) sconst[i] = __ldg(a.consts + pd.const_off + i);
-        const uint32_t np = min(pd.n_consts, kAdjParams);
         for (uint32_t k = 0; k < np; ++k) io.gacc[k * 32] = 0.0f;
         kahan[lane] = 0.0f;
         kahan[32 + lane] = 0.0f;
@@ -554,13 +554,14 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
 // ------------------------------------------------------------- launchers
 // Shared-memory layout (floats).  Block header: code (+1 pad) | constants |
 // meta (4 words) | cross-warp sums (warps x 33 doubles).  Per warp: tape |
-// stacks (per type) | adjoint stacks (per type) | gradient sums (32 x 32)
-// | Kahan state (2 x 32), each program's own sizes (the kernel lays the
+// stacks (per type) | adjoint stacks (per type) | gradient sums (one row of
+// 32 per parameter, at most 32) | Kahan state (2 x 32), each program's own sizes (the kernel lays the
 // region out per item); warp_floats is the largest region of the launch.
-uint32_t adj_warp_floats(uint32_t tape_slots, const uint32_t *stack_depth, int P) {
+uint32_t adj_warp_floats(uint32_t tape_slots, const uint32_t *stack_depth, int P, uint32_t n_params) {
     uint32_t slots = tape_slots;
     for (int t = 0; t < N_STACKS; ++t) slots += 2u * stack_depth[t] * (uint32_t)kStackWidth[t];
-    return (slots * 32u * (uint32_t)P + kAdjParams * 32u + 2u * 32u + 3u) & ~3u;
+    const uint32_t np = n_params < kAdjParams ? n_params : kAdjParams;
+    return (slots * 32u * (uint32_t)P + np * 32u + 2u * 32u + 3u) & ~3u;
 }
 
 uint32_t adj_pack_depth(const uint32_t *stack_depth) {

@@ -262,9 +262,10 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             uint32_t depth[N_STACKS];
             for (int t = 0; t < N_STACKS; ++t) depth[t] = (uint32_t)E.adj_depth[t];
             int pc = adj_max_p(E.adj_profile) >= 8 ? 2 : 1;  // points per lane 2 << pc: the most that fits
-            while (pc >= 0 && (size_t)adj_warp_floats(E.adj_tape, depth, 2 << pc) * 4u > kAdjWarpBudget) --pc;
+            const uint32_t np = (uint32_t)E.consts.size();
+            while (pc >= 0 && (size_t)adj_warp_floats(E.adj_tape, depth, 2 << pc, np) * 4u > kAdjWarpBudget) --pc;
             if (pc >= 0) {
-                const int bucket = (int)((adj_warp_floats(E.adj_tape, depth, 2 << pc) + 1023u) / 1024u);
+                const int bucket = (int)((adj_warp_floats(E.adj_tape, depth, 2 << pc, np) + 1023u) / 1024u);
                 path[i] = kAdjPathBase + ((bucket * 3 + pc) * N_PROFILES + E.adj_profile);
                 continue;
             }
@@ -443,7 +444,8 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                 if (g.kind == 3) {  // slots: the largest warp region (floats)
                     uint32_t depth[N_STACKS];
                     for (int t = 0; t < N_STACKS; ++t) depth[t] = (uint32_t)enc[order[q]].adj_depth[t];
-                    sl = std::max(sl, adj_warp_floats(enc[order[q]].adj_tape, depth, g.P));
+                    sl = std::max(sl, adj_warp_floats(enc[order[q]].adj_tape, depth, g.P,
+                                                      (uint32_t)enc[order[q]].consts.size()));
                 }
             }
             g.code_words = std::max(g.code_words, cw);
