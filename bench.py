@@ -717,7 +717,8 @@ def run_case(args):
     from rsr_b200 import workloads as W
     from rsr_b200.evaluator import Engine
     eng = Engine(use_graphs=False, points_per_thread=args.points_per_thread,
-                 programs_per_warp=args.programs_per_warp)
+                 programs_per_warp=args.programs_per_warp,
+                 flags=N.OPT_SLOT_ADJOINT if args.kernel == "slot-adjoint" else 0)
     if args.workload == "scalar":
         ds, pop = W.scalar_dataset(args.points or 400, seed=1), W.scalar_population(args.programs, seed=11)
     elif args.workload == "vector":
@@ -729,7 +730,7 @@ def run_case(args):
         ds, pop = None, W.inverse_population(args.programs, seed=14)
     pk = I.pack(pop)
     kernel = N.KERNEL_PLAIN if args.kernel == "plain" else N.KERNEL_AUTO
-    grad = args.kernel == "adjoint"
+    grad = args.kernel in ("adjoint", "slot-adjoint")
     if ds is None:
         dss = [eng.upload(W.inverse_dataset(n, seed=100 + i)) for i, n in enumerate(W.uneven_sizes(16))]
         which = np.random.default_rng(5).integers(0, 16, pk.n)
@@ -765,7 +766,8 @@ def main():
     ap.add_argument("--workload", default="vector", choices=["scalar", "vector", "matrix", "uneven"])
     ap.add_argument("--programs", type=int, default=1024)
     ap.add_argument("--points", type=int, default=0, help="--case: override the workload's point count")
-    ap.add_argument("--kernel", default="register", choices=["register", "plain", "adjoint"])
+    ap.add_argument("--kernel", default="register", choices=["register", "plain", "adjoint", "slot-adjoint"],
+                    help="--case: adjoint runs the register adjoint where it applies, slot-adjoint the slot-file one")
     ap.add_argument("--runs", type=int, default=3)
     ap.add_argument("--points-per-thread", type=int, default=0, help="--case: register kernel P (0: tuned)")
     ap.add_argument("--programs-per-warp", type=int, default=0, help="--case: register kernel G (0: tuned)")

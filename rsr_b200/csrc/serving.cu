@@ -77,17 +77,21 @@ struct Job {
 using JobPtr = std::shared_ptr<Job>;
 
 struct Slot {
-    cudaStream_t st = nullptr;
+    // a batch runs as up to two chunks of programs, each with its own plan
+    // buffers and stream: the second is planned while the first runs
+    cudaStream_t st = nullptr, st2 = nullptr;
     EncodeScratch enc;  // the slot plans with its own encoding storage and threads
-    DevicePlan dev;
+    DevicePlan dev, dev2;
     FitWorkspace fit;
-    std::vector<float> host;
+    HostBuf host;       // pinned results of a batch
     size_t cached() const {
-        return dev.pool.cap + dev.partials.cap + dev.out.cap + fit.grad.pool.cap + fit.grad.partials.cap +
-               fit.grad.out.cap + fit.mse.pool.cap + fit.mse.partials.cap + fit.mse.out.cap;
+        return dev.pool.cap + dev.partials.cap + dev.out.cap + dev2.pool.cap + dev2.partials.cap + dev2.out.cap +
+               fit.grad.pool.cap + fit.grad.partials.cap + fit.grad.out.cap + fit.mse.pool.cap +
+               fit.mse.partials.cap + fit.mse.out.cap;
     }
     void trim() {
         dev.pool.release(); dev.partials.release(); dev.out.release(); dev.counters.release();
+        dev2.pool.release(); dev2.partials.release(); dev2.out.release(); dev2.counters.release();
         for (DevicePlan *d : {&fit.grad, &fit.mse}) {
             d->pool.release(); d->partials.release(); d->out.release(); d->counters.release();
         }
@@ -200,29 +204,53 @@ int run_eval(rsr_server *S, Slot &slot, const std::vector<JobPtr> &batch) {
     }
     const uint32_t n = (uint32_t)dsp.size();
     if (n == 0) return RSR_OK;
-    rsr_population pop{n, code.data(), code_off.data(), kinds.data(), kind_off.data(), params.data(),
-                       param_off.data()};
-    Plan plan;
-    // ctx->mu only around the dataset and tuning tables: slots encode in parallel
-    int rc = build_plan(ctx, pop, dsp.data(), 0, RSR_KERNEL_AUTO, gradient, MODE_MSE, &plan, &slot.enc, &ctx->mu);
-    if (rc) return rc;
-    if ((rc = upload_plan(ctx, plan, &slot.dev, slot.st))) return rc;
-    if ((rc = enqueue_plan(ctx, plan, &slot.dev, slot.st, nullptr))) return rc;
-    const size_t nf = (size_t)n * (gradient ? 33 : 1);
-    slot.host.resize(nf);
+    // Batches of 512 programs or more run as two chunks (a third, then the
+    // rest): the second chunk is encoded while the first one's kernels run,
+    // and its launches fill the SMs the first one's tail frees.
+    const uint32_t split = n >= 512 ? n / 3 : n;
+    const uint32_t starts[3] = {0, split, n};
+    const int n_chunks = split < n ? 2 : 1;
+    const size_t stride = gradient ? 33 : 1;
     cudaError_t e;
-    if ((e = cudaMemcpyAsync(slot.host.data(), slot.dev.out.p, nf * sizeof(float), cudaMemcpyDeviceToHost,
-                             slot.st)) != cudaSuccess)
-        return cuda_fail(e, "result download");
-    if ((e = cudaStreamSynchronize(slot.st)) != cudaSuccess) return cuda_fail(e, "evaluation");
+    if ((e = slot.host.reserve((size_t)n * stride * sizeof(float))) != cudaSuccess) return cuda_fail(e, "cudaHostAlloc");
+    float *res = (float *)slot.host.p;
+    Plan plans[2];
+    int rc = RSR_OK;
+    int launched = 0;
+    for (int k = 0; k < n_chunks && !rc; ++k) {
+        const uint32_t s0 = starts[k], cnt = starts[k + 1] - s0;
+        rsr_population pop{cnt, code.data(), code_off.data() + s0, kinds.data(), kind_off.data() + s0,
+                           params.data(), param_off.data() + s0};
+        DevicePlan &dev = k ? slot.dev2 : slot.dev;
+        cudaStream_t st = k ? slot.st2 : slot.st;
+        // ctx->mu only around the dataset and tuning tables: slots encode in parallel
+        rc = build_plan(ctx, pop, dsp.data() + s0, 0, RSR_KERNEL_AUTO, gradient, MODE_MSE, &plans[k], &slot.enc,
+                        &ctx->mu);
+        if (!rc) rc = upload_plan(ctx, plans[k], &dev, st);
+        if (!rc) rc = enqueue_plan(ctx, plans[k], &dev, st, nullptr);
+        if (!rc && (e = cudaMemcpyAsync(res + (size_t)s0 * stride, dev.out.p, (size_t)cnt * stride * sizeof(float),
+                                        cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            rc = cuda_fail(e, "result download");
+        if (!rc) launched = k + 1;
+    }
+    // wait for whatever was launched, error or not, before buffers are reused
+    for (int k = 0; k < n_chunks; ++k) {
+        const cudaError_t se = cudaStreamSynchronize(k ? slot.st2 : slot.st);
+        if (!rc && se != cudaSuccess) rc = cuda_fail(se, "evaluation");
+    }
+    if (rc) return rc;
     // scatter: merged index -> (job, local index)
-    for (uint32_t li = 0; li < n; ++li) {
-        const uint32_t m = plan.orig[li];
-        const size_t b = std::upper_bound(first.begin(), first.end(), m) - first.begin() - 1;
-        Job &j = *batch[b];
-        const uint32_t k = m - first[b];
-        j.mse_out[k] = slot.host[li];
-        if (gradient) memcpy(j.grad_out + (size_t)k * 32, slot.host.data() + n + (size_t)li * 32, 32 * sizeof(float));
+    for (int k = 0; k < launched; ++k) {
+        const uint32_t s0 = starts[k], cnt = starts[k + 1] - s0;
+        const float *r = res + (size_t)s0 * stride;
+        for (uint32_t li = 0; li < cnt; ++li) {
+            const uint32_t m = s0 + plans[k].orig[li];
+            const size_t b = std::upper_bound(first.begin(), first.end(), m) - first.begin() - 1;
+            Job &j = *batch[b];
+            const uint32_t q = m - first[b];
+            j.mse_out[q] = r[li];
+            if (gradient) memcpy(j.grad_out + (size_t)q * 32, r + cnt + (size_t)li * 32, 32 * sizeof(float));
+        }
     }
     return RSR_OK;
 }
@@ -427,8 +455,15 @@ int rsr_server_create(rsr_ctx *ctx, const rsr_server_options *opts, rsr_server *
     for (uint32_t i = 0; i < S->opts.slots; ++i) {
         auto sl = std::make_unique<Slot>();
         cudaError_t e = cudaStreamCreateWithFlags(&sl->st, cudaStreamNonBlocking);
+        if (e == cudaSuccess) {
+            e = cudaStreamCreateWithFlags(&sl->st2, cudaStreamNonBlocking);
+            if (e != cudaSuccess) cudaStreamDestroy(sl->st);
+        }
         if (e != cudaSuccess) {
-            for (auto &s : S->slots) cudaStreamDestroy(s->st);
+            for (auto &s : S->slots) {
+                cudaStreamDestroy(s->st);
+                cudaStreamDestroy(s->st2);
+            }
             return cuda_fail(e, "cudaStreamCreate");
         }
         S->slots.push_back(std::move(sl));
@@ -461,11 +496,15 @@ int rsr_server_destroy(rsr_server *S) {
     cudaSetDevice(S->ctx->device);
     for (auto &sl : S->slots) {
         cudaStreamSynchronize(sl->st);
+        cudaStreamSynchronize(sl->st2);
         sl->trim();
         sl->dev.staging.release();
+        sl->dev2.staging.release();
         sl->fit.grad.staging.release();
         sl->fit.mse.staging.release();
+        sl->host.release();
         cudaStreamDestroy(sl->st);
+        cudaStreamDestroy(sl->st2);
     }
     delete S;
     return RSR_OK;
