@@ -29,16 +29,25 @@ struct Acc {
     Vf<P> M3[Types<PROF>::M3 ? 9 : 1];
 };
 
+// Operand sources of one lane.  Per-lane values (features, stack slots) use
+// the interleaved lane layout (kernels_common.cuh): a feature's tile and a
+// stack slot component are each one block of 32*P floats.
 template <int P>
 struct AccIO {
-    const float *xl;        // this lane's first point of feature 0 in the current tile
+    const float *xl;        // feature 0 of the current tile, at this lane's first point
     uint32_t stride;        // floats between features
     const float *consts;
-    Vf<P> *stk[N_STACKS];   // per-type shared-memory stacks of this lane: [(slot*W + c)*32]
-    __device__ __forceinline__ Vf<P> X(uint32_t f) const { return load_pts<P>(xl + (size_t)f * stride); }
+    float *stk[N_STACKS];   // per-type stacks, block (slot*W + c), at this lane's first value
+    __device__ __forceinline__ Vf<P> X(uint32_t f) const { return load_lane<P>(xl + (size_t)f * stride); }
     __device__ __forceinline__ Vf<P> C(uint32_t i) const { return splat<P>(consts[i]); }
     template <int W>
-    __device__ __forceinline__ Vf<P> &S(int t, uint32_t slot, int c) const { return stk[t][(slot * W + c) * 32]; }
+    __device__ __forceinline__ Vf<P> S(int t, uint32_t slot, int c) const {
+        return lds_lane<P>(stk[t] + (slot * W + c) * 32u * P);
+    }
+    template <int W>
+    __device__ __forceinline__ void put(int t, uint32_t slot, int c, const Vf<P> &v) const {
+        sts_lane<P>(stk[t] + (slot * W + c) * 32u * P, v);
+    }
 };
 
 template <int PROF, int P, int t>
@@ -150,7 +159,7 @@ __device__ __forceinline__ void acc_op(Acc<PROF, P> &a, const AccIO<P> &io, uint
         } else if constexpr (k == KV_PUSH) {
             const uint32_t slot = arg & 15u, lt = (arg >> 4) & 7u;
 #pragma unroll
-            for (int c = 0; c < W; ++c) io.template S<W>(t, slot, c) = A[c];
+            for (int c = 0; c < W; ++c) io.template put<W>(t, slot, c, A[c]);
             if (lt) load_any<PROF, P>(a, io, lt - 1u, (arg >> 7) & 1u, arg >> 8);
         } else if constexpr (k >= KV_BIN && k < KV_BIN + 3 * nb) {
             constexpr int j = (k - KV_BIN) / 3, src = (k - KV_BIN) % 3;

@@ -18,6 +18,14 @@ size_t plain_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t 
 // Loads the slot-file kernel's variants and the MSE epilogue ahead of their
 // first real launch (lazy module loading), with empty launches on st.
 cudaError_t preload_plain_mse(cudaStream_t st);
+// Every instance of the register, register-adjoint and slot-file adjoint
+// kernels, loaded by empty launches (zero: a device word holding 0, the
+// run_if that makes them return at once).  Module loading is lazy,
+// and a kernel's first launch otherwise also resizes the context's local
+// memory for its spills, which waits for all work on the device.
+cudaError_t preload_reg(const uint32_t *zero, cudaStream_t st);
+cudaError_t preload_adj(const uint32_t *zero, cudaStream_t st);
+cudaError_t preload_grad(const uint32_t *zero, cudaStream_t st);
 cudaError_t launch_aosoa_to_soa(const float *ff, const float *tb, float *x, float *y, uint32_t nf, uint64_t nbatch,
                                 uint64_t stride, int num_sms, cudaStream_t st);
 cudaError_t measure_fp32_peak(int num_sms, cudaStream_t st, double *lane_ops_per_s);

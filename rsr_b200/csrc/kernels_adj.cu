@@ -38,13 +38,24 @@ constexpr uint32_t kAdjParams = 32;
 // lane's gradient sums.
 template <int P>
 struct RevIO : AccIO<P> {
-    Vf<P> *gstk[N_STACKS];  // adjoint stacks of this lane: [(slot*W + c)*32]
-    Vf<P> *tape;            // tape of this lane: [slot*32]
+    // adjoint stacks and tape in the interleaved lane layout (blocks of 32*P
+    // floats), at this lane's first value
+    float *gstk[N_STACKS];  // adjoint stacks, block (slot*W + c)
+    float *tape;            // tape, block slot
     float *gacc;            // this lane's f32 gradient sums: gacc[k*32]
-    uint32_t valid;         // bit q: point q of the lane is counted
-    __device__ __forceinline__ Vf<P> T(uint32_t slot) const { return tape[slot * 32]; }
+    uint32_t valid;         // bit q: value q of the lane is a counted point
+    __device__ __forceinline__ Vf<P> T(uint32_t slot) const { return lds_lane<P>(tape + slot * 32u * P); }
+    __device__ __forceinline__ void put_tape(uint32_t slot, const Vf<P> &v) const {
+        sts_lane<P>(tape + slot * 32u * P, v);
+    }
     template <int W>
-    __device__ __forceinline__ Vf<P> &GS(int t, uint32_t slot, int c) const { return gstk[t][(slot * W + c) * 32]; }
+    __device__ __forceinline__ Vf<P> GS(int t, uint32_t slot, int c) const {
+        return lds_lane<P>(gstk[t] + (slot * W + c) * 32u * P);
+    }
+    template <int W>
+    __device__ __forceinline__ void put_g(int t, uint32_t slot, int c, const Vf<P> &v) const {
+        sts_lane<P>(gstk[t] + (slot * W + c) * 32u * P, v);
+    }
     // adds the lane's counted points of g to the sum of flat parameter k
     // (points past the dataset's end may carry 0*inf = NaN adjoints)
     __device__ __forceinline__ void grad_add(uint32_t k, const Vf<P> &g) const {
@@ -84,7 +95,7 @@ __device__ __forceinline__ void send(const RevIO<P> &io, int t, uint32_t arg, co
         for (int c = 0; c < W; ++c) io.grad_add(arg + c, gb[c]);
     } else if constexpr (SRC == SRC_S) {
 #pragma unroll
-        for (int c = 0; c < W; ++c) io.template GS<W>(t, arg, c) = gb[c];
+        for (int c = 0; c < W; ++c) io.template put_g<W>(t, arg, c, gb[c]);
     }
 }
 
@@ -275,7 +286,7 @@ __device__ __forceinline__ void rev_op(Acc<PROF, P> &g, const RevIO<P> &io, uint
             } else if constexpr (k == kk) {              // MAKE from F stack slots + A_F
                 g.F[0] = g.F[0] + G[W - 1];
 #pragma unroll
-                for (int c = 0; c + 1 < W; ++c) io.template GS<1>(SF, arg + c, 0) = G[c];
+                for (int c = 0; c + 1 < W; ++c) io.template put_g<1>(SF, arg + c, 0, G[c]);
                 zero_acc<P, W>(G);
             }
         } else {  // M2 / M3
@@ -363,7 +374,7 @@ __device__ __forceinline__ void rev_op(Acc<PROF, P> &g, const RevIO<P> &io, uint
 #pragma unroll
                     for (int col = 0; col + 1 < N; ++col)
 #pragma unroll
-                        for (int r = 0; r < N; ++r) io.template GS<N>(tv, arg + col, r) = G[N * col + r];
+                        for (int r = 0; r < N; ++r) io.template put_g<N>(tv, arg + col, r, G[N * col + r]);
                 }
                 zero_acc<P, W>(G);
             }
@@ -378,7 +389,7 @@ __device__ __forceinline__ void tape_store(Acc<PROF, P> &a, const RevIO<P> &io, 
         constexpr int W = kStackWidth[t];
         const Vf<P> *A = acc_of<PROF, P, t>(a);
 #pragma unroll
-        for (int c = 0; c < W; ++c) io.tape[(slot + c) * 32] = A[c];
+        for (int c = 0; c < W; ++c) io.put_tape(slot + c, A[c]);
     }
 }
 
@@ -472,16 +483,17 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
         // (n_slots: tape slots; n_tape: stack depths, 5 bits per type); the
         // launch's region_floats is the largest of its programs'
         {
+            const uint32_t l0 = lane_point<P>(lane, 0);
             uint32_t off = pd.n_slots * 32u * P;
-            io.tape = reinterpret_cast<Vf<P> *>(wbase) + lane;
+            io.tape = wbase + l0;
 #pragma unroll
             for (int t = 0; t < N_STACKS; ++t) {
-                io.stk[t] = reinterpret_cast<Vf<P> *>(wbase + off) + lane;
+                io.stk[t] = wbase + off + l0;
                 off += ((pd.n_tape >> (5 * t)) & 31u) * type_width(t) * 32u * P;
             }
 #pragma unroll
             for (int t = 0; t < N_STACKS; ++t) {
-                io.gstk[t] = reinterpret_cast<Vf<P> *>(wbase + off) + lane;
+                io.gstk[t] = wbase + off + l0;
                 off += ((pd.n_tape >> (5 * t)) & 31u) * type_width(t) * 32u * P;
             }
             io.gacc = wbase + off + lane;
@@ -500,15 +512,16 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
         const uint32_t n_fwd = scode[0], n_rev = scode[1];
         const uint32_t *fwd = scode + kAdjHeaderWords, *rev = fwd + n_fwd;
         for (uint32_t tile = it.tile_begin + warp; tile < it.tile_end; tile += nw) {
-            const uint64_t p0 = (uint64_t)tile * (32u * P) + (uint64_t)lane * P;
+            const uint64_t t0 = (uint64_t)tile * (32u * P);
+            const uint64_t p0 = t0 + lane_point<P>(lane, 0);
             io.xl = ds.x + p0;
             uint32_t valid = 0;
 #pragma unroll
-            for (int q = 0; q < P; ++q) valid |= (p0 + q < ds.n_eval ? 1u : 0u) << q;
+            for (int q = 0; q < P; ++q) valid |= (t0 + lane_point<P>(lane, q) < ds.n_eval ? 1u : 0u) << q;
             io.valid = valid;
             Acc<PROF, P> acc;
             run_forward<PROF, P>(acc, io, fwd, n_fwd);
-            const Vf<P> y = load_pts<P>(ds.y + p0);
+            const Vf<P> y = load_lane<P>(ds.y + p0);
             Acc<PROF, P> g;
             g.F[0] = splat<P>(0.0f);
             if constexpr (Types<PROF>::V2) zero_acc<P, 2>(g.V2);
@@ -623,6 +636,26 @@ cudaError_t launch_adj(const LaunchArgs &a, int profile, int P, uint32_t grid, s
         case 7: return launch_adj_pp<P_FV3M3, 4>(a, grid, smem, st);
         default: return cudaErrorInvalidValue;
     }
+}
+
+// Loads one instance ahead of its first real launch (an empty launch: run_if
+// points at a zero word, every thread returns at its first check).
+template <int PROF, int P>
+static cudaError_t adj_preload_pp(const uint32_t *zero, cudaStream_t st) {
+    LaunchArgs none{};
+    none.run_if = zero;
+    return launch_adj_pp<PROF, P>(none, 1, 0, st);
+}
+
+cudaError_t preload_adj(const uint32_t *zero, cudaStream_t st) {
+    const cudaError_t r[] = {adj_preload_pp<P_F, 2>(zero, st),     adj_preload_pp<P_F, 4>(zero, st),
+                             adj_preload_pp<P_F, 8>(zero, st),     adj_preload_pp<P_FV3, 2>(zero, st),
+                             adj_preload_pp<P_FV3, 4>(zero, st),   adj_preload_pp<P_FV3, 8>(zero, st),
+                             adj_preload_pp<P_FV2M2, 2>(zero, st), adj_preload_pp<P_FV2M2, 4>(zero, st),
+                             adj_preload_pp<P_FV3M3, 2>(zero, st), adj_preload_pp<P_FV3M3, 4>(zero, st)};
+    for (cudaError_t e : r)
+        if (e != cudaSuccess) return e;
+    return cudaSuccess;
 }
 
 int adj_max_blocks_per_sm(int profile, int P, size_t smem) {

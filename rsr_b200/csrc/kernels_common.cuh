@@ -89,4 +89,78 @@ __device__ __forceinline__ void store_pts(float *p, const Vf<P> &v, uint64_t fir
         if (first + k < limit) p[k] = v.v[k];
 }
 
+// ------------------------------------------------ interleaved lane layout
+// The register kernels give lane l of a warp the points of a 32*P-point
+// tile in runs of at most four: P <= 4, points l*P .. l*P+P-1; P = 8, points
+// 4l .. 4l+3 and 128+4l .. 128+4l+3.  Each 16-byte access of the warp then
+// covers 512 contiguous bytes -- four L1 wavefronts for a global load, no
+// bank conflict for shared memory -- where eight consecutive points a lane
+// would take eight (two lanes 32 bytes apart share a 128-byte line or a bank).
+// Per-lane values in shared memory use the same layout in blocks of 32*P
+// floats: [P/4 runs][32 lanes][4] (P >= 4), [32 lanes][P] below.
+template <int P>
+constexpr int kLaneRun = P < 4 ? P : 4;
+
+// Offset of value q of `lane` from the start of its tile (or block).
+template <int P>
+__host__ __device__ __forceinline__ constexpr uint32_t lane_point(int lane, int q) {
+    return (uint32_t)((q / kLaneRun<P>) * 32 * kLaneRun<P> + lane * kLaneRun<P> + q % kLaneRun<P>);
+}
+
+// Loads a lane's P values; p points at its first (tile start + lane_point(lane, 0)).
+template <int P>
+__device__ __forceinline__ Vf<P> load_lane(const float *__restrict__ p) {
+    if constexpr (P <= 4) {
+        return load_pts<P>(p);
+    } else {
+        Vf<P> r;
+#pragma unroll
+        for (int j = 0; j < P / 4; ++j) {
+            const float4 a = __ldg(reinterpret_cast<const float4 *>(p + j * 128));
+            r.v[4 * j] = a.x; r.v[4 * j + 1] = a.y; r.v[4 * j + 2] = a.z; r.v[4 * j + 3] = a.w;
+        }
+        return r;
+    }
+}
+
+// Shared-memory image of a lane's P values in a block of 32*P floats; p
+// points at the lane's first value (block start + lane_point(lane, 0)).
+template <int P>
+__device__ __forceinline__ Vf<P> lds_lane(const float *p) {
+    if constexpr (P <= 4) {
+        return *reinterpret_cast<const Vf<P> *>(p);
+    } else {
+        Vf<P> r;
+#pragma unroll
+        for (int j = 0; j < P / 4; ++j) {
+            const float4 a = *reinterpret_cast<const float4 *>(p + j * 128);
+            r.v[4 * j] = a.x; r.v[4 * j + 1] = a.y; r.v[4 * j + 2] = a.z; r.v[4 * j + 3] = a.w;
+        }
+        return r;
+    }
+}
+
+template <int P>
+__device__ __forceinline__ void sts_lane(float *p, const Vf<P> &v) {
+    if constexpr (P <= 4) {
+        *reinterpret_cast<Vf<P> *>(p) = v;
+    } else {
+#pragma unroll
+        for (int j = 0; j < P / 4; ++j)
+            *reinterpret_cast<float4 *>(p + j * 128) = make_float4(v.v[4 * j], v.v[4 * j + 1], v.v[4 * j + 2],
+                                                                  v.v[4 * j + 3]);
+    }
+}
+
+// Stores the lane's values whose points lie below `limit`; `tile` is the
+// tile's first point, p the output's value of point `tile`.
+template <int P>
+__device__ __forceinline__ void store_lane(float *p, int lane, const Vf<P> &v, uint64_t tile, uint64_t limit) {
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+        const uint32_t o = lane_point<P>(lane, q);
+        if (tile + o < limit) p[o] = v.v[q];
+    }
+}
+
 }  // namespace rsr

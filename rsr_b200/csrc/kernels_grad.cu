@@ -488,6 +488,33 @@ cudaError_t launch_grad(const LaunchArgs &a, int profile, bool no_unary, uint32_
     }
 }
 
+// Loads every instance and the epilogue ahead of their first real launches:
+// empty launches that return at once (one item, whose warp stops at run_if,
+// a zero word; no programs for the epilogue).
+template <int PROF, bool NU>
+static cudaError_t preload_grad_prof(const uint32_t *zero, cudaStream_t st) {
+    LaunchArgs none{};
+    none.n_items = 1;
+    none.run_if = zero;
+    cudaError_t e;
+    for (uint32_t ppw : {1u, 2u, 4u}) {
+        none.progs_per_warp = ppw;
+        if ((e = launch_grad_prof<PROF, NU>(none, 1, 0, st)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t preload_grad(const uint32_t *zero, cudaStream_t st) {
+    const cudaError_t r[] = {preload_grad_prof<P_F, true>(zero, st),      preload_grad_prof<P_F, false>(zero, st),
+                             preload_grad_prof<P_FV3, true>(zero, st),    preload_grad_prof<P_FV3, false>(zero, st),
+                             preload_grad_prof<P_FV2M2, false>(zero, st), preload_grad_prof<P_FV3M3, false>(zero, st),
+                             preload_grad_prof<P_ALL, false>(zero, st)};
+    for (cudaError_t e : r)
+        if (e != cudaSuccess) return e;
+    finalize_grad_kernel<<<1, 32, 0, st>>>(nullptr, nullptr, nullptr, 0u, nullptr, nullptr);  // n_progs = 0
+    return cudaGetLastError();
+}
+
 size_t grad_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t val_slots, uint32_t adj_slots,
                           int P) {
     const uint32_t gp = const_floats < kGradParams ? const_floats : kGradParams;

@@ -571,6 +571,25 @@ int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st
     return RSR_OK;
 }
 
+int preload_eval_kernels(rsr_ctx *ctx) {
+    if (ctx->kernels_loaded) return RSR_OK;
+    cudaSetDevice(ctx->device);
+    uint32_t *zero = nullptr;
+    cudaError_t e = cudaMalloc(&zero, sizeof(uint32_t));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+    cudaStream_t st = ctx->stream;
+    if ((e = cudaMemsetAsync(zero, 0, sizeof(uint32_t), st)) == cudaSuccess &&
+        (e = preload_plain_mse(st)) == cudaSuccess && (e = preload_reg(zero, st)) == cudaSuccess &&
+        (e = preload_adj(zero, st)) == cudaSuccess && (e = preload_grad(zero, st)) == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    else
+        cudaStreamSynchronize(st);  // the launches made so far finish before the word is freed
+    cudaFree(zero);
+    if (e != cudaSuccess) return cuda_fail(e, "kernel preload");
+    ctx->kernels_loaded = true;
+    return RSR_OK;
+}
+
 // Makes st wait for the launches a plan put on its side streams.
 static cudaError_t join_side_streams(DevicePlan *dev, cudaStream_t st, unsigned forked) {
     cudaError_t first = cudaSuccess;

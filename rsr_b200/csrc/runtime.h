@@ -211,6 +211,7 @@ struct rsr_ctx {
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     std::atomic<uint64_t> launches{0};
     std::atomic<uint64_t> last_h2d{0}, last_d2h{0};   // bytes copied by the last evaluation call
+    bool kernels_loaded = false;  // preload_eval_kernels has run
 };
 
 struct rsr_batch {
@@ -243,6 +244,9 @@ struct EncodeScratch {
 int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_prog, uint64_t ds_all, int kernel,
                bool gradient, int mode, Plan *plan, EncodeScratch *scratch = nullptr, std::mutex *table_mu = nullptr);
 int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st);
+// Loads every evaluation kernel instance once per context (caller holds
+// ctx->mu), so that no later call pays for a kernel's first launch.
+int preload_eval_kernels(rsr_ctx *ctx);
 // A zero-filled resident dataset of the given shape (columns padded to the
 // stride), and its registration in the context's table (caller holds ctx->mu).
 int alloc_dataset(rsr_ctx *ctx, uint32_t nf, uint64_t nbatch, uint64_t nsamples, std::unique_ptr<DatasetRec> *out);

@@ -449,6 +449,8 @@ int rsr_server_create(rsr_ctx *ctx, const rsr_server_options *opts, rsr_server *
         const uint64_t free_budget =
             ctx->opts.mem_budget_bytes > ctx->mem_in_use ? ctx->opts.mem_budget_bytes - ctx->mem_in_use : 0;
         S->budget = S->opts.mem_budget_bytes ? S->opts.mem_budget_bytes : free_budget / 2;
+        // every kernel a job may use is loaded now rather than on the job's time
+        if (const int rc = preload_eval_kernels(ctx)) return rc;
     }
     if (S->budget == 0) return fail(RSR_ENOMEM, "no device memory left for serving");
     cudaSetDevice(ctx->device);
