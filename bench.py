@@ -49,11 +49,11 @@ sys.path.insert(0, str(ROOT))
 
 # DRAM bytes (read + write) of the dominant kernel's launches in one step of
 # this workload (three spill-depth classes, P=8 G=4), from one ncu capture
-# (profiles/reg_eval_kernel_vector_1024x100k.md, "Full bench size"):
-# 4,856,832 + 4,630,016 + 4,114,944 read, 0 written.  ncu replays each launch
+# (profiles/launch_list_bench_vector_4096x100k.md, "DRAM traffic"):
+# 4,711,424 + 4,775,680 + 4,116,736 read, 512 written.  ncu replays each launch
 # with cold caches, so each re-reads the 4 MB dataset; in a step the second
 # and third launches find it in L2.
-DOMINANT_KERNEL_DRAM_BYTES = 13_601_792
+DOMINANT_KERNEL_DRAM_BYTES = 13_604_352
 METRIC = "program_points_per_sec"
 UNIT = "program*points/s"
 N_PROGRAMS = 4096

@@ -565,13 +565,18 @@ class AccEmitter {
 // has analysed: the accumulator form's evaluation order without load
 // fusion, every PUSH to its own stack slot, TAPE micro-ops next to the ops
 // whose reverse rules read forward values, and one reverse entry per
-// micro-op.  Tape slots hold (first | second << 16):
+// micro-op.  An input value that is still a plain feature or constant load
+// is not taped: its reference names the feature or constant (kTapeRefX,
+// kTapeRefC).  Tape references hold (first | second << 16):
 //   F MUL: A before; DIV: A after; RDIV: A before, A after;
 //   sin cos sqr ln: A before; exp sqrt: A after;
 //   V CROSS/RCROSS, M MUL/RMUL, DOT, DET: the accumulator before;
 //   SCALE, MULM: the accumulator before, and (A forms) the other operand's
 //   accumulator (A_F, or the matrix);
-//   NORM: A_F after, the vector; INVERSE: after, before.
+//   NORM: -, the vector (the rule recomputes the norm from it);
+//   INVERSE: after, before.
+int kind_block(int kind);
+
 class AdjEmitter {
    public:
     AdjEmitter(const std::vector<Node> &nodes, const AccEmitter &an) : nodes_(nodes), an_(an) {}
@@ -611,11 +616,11 @@ class AdjEmitter {
                 const int kind = base + 3 * j + src;
                 const bool before = (t == SF && (j == 3 || j == 5)) || (t != SF && t != SV2 && (j == 3 || j == 4));
                 const bool after = t == SF && (j == 4 || j == 5);
-                const uint32_t ta = take(t), tb = before && after ? take(t) : 0u;
-                if (before) store(t, ta);
+                uint32_t ta = 0, tb = 0;
+                if (before) ta = tape_in(t);
+                if (after) (before ? tb : ta) = take(t);
                 op(kind, arg, ta, tb);
                 if (after) store(t, before ? tb : ta);
-                if (!before && !after) tape -= (uint32_t)kStackWidth[t];  // not needed after all
                 break;
             }
             case C_DOT: {
@@ -626,8 +631,7 @@ class AdjEmitter {
                 if (leaf(*in[1])) { gen(n.in[0]); src = src_of(*in[1]); arg = in[1]->arg; }
                 else if (leaf(*in[0])) { gen(n.in[1]); src = src_of(*in[0]); arg = in[0]->arg; }
                 else { gen(n.in[0]); arg = (uint32_t)push(t); gen(n.in[1]); src = SRC_S; }
-                const uint32_t ta = take(t);
-                store(t, ta);
+                const uint32_t ta = tape_in(t);
                 op(base + src, arg, ta);
                 break;
             }
@@ -644,9 +648,8 @@ class AdjEmitter {
             case C_UNARY_F: {
                 gen(n.in[0]);
                 const int u = opc - SIN_F;  // sin cos exp sqr sqrt ln
-                const uint32_t ta = take(SF);
                 const bool after = u == 2 || u == 4;
-                if (!after) store(SF, ta);
+                const uint32_t ta = after ? take(SF) : tape_in(SF);
                 op(K_F_UN + u, 0, ta);
                 if (after) store(SF, ta);
                 break;
@@ -659,10 +662,9 @@ class AdjEmitter {
                 if (opc == GET_Y_V2 || opc == GET_Y_V3) k += 2;
                 if (opc == GET_Z_V3) k += 3;
                 if (op_class(opc) == C_NORM) {
-                    const uint32_t tb = take(t), ta = take(SF);
-                    store(t, tb);
-                    op(kBlockBase[t] + k, 0, ta, tb);
-                    store(SF, ta);
+                    // the reverse rule recomputes the norm from the vector
+                    const uint32_t tb = tape_in(t);
+                    op(kBlockBase[t] + k, 0, 0, tb);
                 } else {
                     op(kBlockBase[t] + k, 0);
                 }
@@ -672,16 +674,14 @@ class AdjEmitter {
                 const int t = in[0]->out;
                 gen(n.in[0]);
                 if (opc == DET_M2 || opc == DET_M3) {
-                    const uint32_t ta = take(t);
-                    store(t, ta);
+                    const uint32_t ta = tape_in(t);
                     op(kBlockBase[t] + KM_DET, 0, ta);
                 } else if (opc == TRACE_M2 || opc == TRACE_M3) {
                     op(kBlockBase[t] + KM_TRACE, 0);
                 } else if (opc == TRANSPOSE_M2 || opc == TRANSPOSE_M3) {
                     op(kBlockBase[t] + KM_TRANSPOSE, 0);
                 } else {
-                    const uint32_t tb = take(t), ta = take(t);
-                    store(t, tb);
+                    const uint32_t tb = tape_in(t), ta = take(t);
                     op(kBlockBase[t] + KM_INVERSE, 0, ta, tb);
                     store(t, ta);
                 }
@@ -728,8 +728,7 @@ class AdjEmitter {
         const Node &o = nodes_[n.in[0]];
         if (leaf(o)) {
             gen(n.in[1]);
-            const uint32_t ta = take(t);
-            store(t, ta);
+            const uint32_t ta = tape_in(t);
             op(base + 1 + src_of(o), o.arg, ta);
             return;
         }
@@ -737,14 +736,11 @@ class AdjEmitter {
         if (an_.writes_of(n.in[1]) & (1u << tother)) {
             const int slot = push(tother);
             gen(n.in[1]);
-            const uint32_t ta = take(t);
-            store(t, ta);
+            const uint32_t ta = tape_in(t);
             op(base + 3, (uint32_t)slot, ta);
         } else {
             gen(n.in[1]);
-            const uint32_t ta = take(t), tb = take(tother);
-            store(t, ta);
-            store(tother, tb);
+            const uint32_t ta = tape_in(t), tb = tape_in(tother);
             op(base + 0, 0, ta, tb);
         }
     }
@@ -755,11 +751,26 @@ class AdjEmitter {
         return s;
     }
     void store(int t, uint32_t slot) { fwd.push_back(uop_word((uint32_t)kTapeKind[t], slot)); }
+    // Reference to the current value of accumulator t as an input of the next
+    // op: the feature or constant it was loaded from when no op has changed
+    // it since, else a new tape slot stored now.
+    uint32_t tape_in(int t) {
+        if (plain_[t]) return plain_[t];
+        const uint32_t s = take(t);
+        store(t, s);
+        return s;
+    }
     void op(int kind, uint32_t arg, uint32_t ta = 0, uint32_t tb = 0) {
         fwd.push_back(uop_word((uint32_t)kind, arg));
         rev.push_back(uop_word((uint32_t)kind, arg));
         rev.push_back(ta | (tb << 16));
+        const int t = kind_block(kind), k = kind - kBlockBase[t];
+        const bool fits = arg + (uint32_t)kStackWidth[t] <= kTapeRefIndex;
+        if (k == KV_LDX) plain_[t] = fits ? kTapeRefX | arg : 0u;
+        else if (k == KV_LDC) plain_[t] = fits ? kTapeRefC | arg : 0u;
+        else if (k != KV_PUSH) plain_[t] = plain_[SF] = 0u;  // the op's own type and A_F may change
     }
+    uint32_t plain_[N_STACKS] = {0, 0, 0, 0, 0};
     int push(int t) {
         const int slot = n_push[t]++;
         op(kBlockBase[t] + KV_PUSH, (uint32_t)slot);
@@ -1015,7 +1026,7 @@ int encode_program(const uint32_t *code, uint32_t len, const uint8_t *kinds, uin
         if (an.analyze(root)) {
             AdjEmitter em(nodes, an);
             em.gen(root);
-            bool fits = em.tape < (1u << 16);
+            bool fits = em.tape <= kTapeRefIndex;
             for (int t = 0; t < N_STACKS; ++t) {
                 E.adj_depth[t] = em.n_push[t];
                 fits = fits && em.n_push[t] <= kMaxAccStack;

@@ -52,8 +52,9 @@ int reg_max_blocks_per_sm(int profile, int P, unsigned omit, size_t smem);
 // P (points per lane) 2, 4, or 8 up to adj_max_p(profile)
 bool adj_supported(int profile);
 int adj_max_p(int profile);
-// floats of a warp's region for a program (tape | stacks | adjoint stacks |
-// gradient sums | Kahan state), and its stack depths packed for ProgDesc
+// floats of a warp's region for a program (tape | stacks, shared by the
+// adjoint stacks | gradient sums | Kahan state), and its stack depths packed
+// for ProgDesc
 uint32_t adj_warp_floats(uint32_t tape_slots, const uint32_t *stack_depth, int P, uint32_t n_params);
 uint32_t adj_pack_depth(const uint32_t *stack_depth);
 void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, LaunchArgs *a);

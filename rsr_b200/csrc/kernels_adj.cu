@@ -14,7 +14,8 @@
 //            adjoint accumulators G_t of the micro-op's output to those of
 //            its inputs.  A second operand's adjoint goes to the constant
 //            sums (LoadConst), to the adjoint stack slot of its PUSH (a
-//            spilled value), or nowhere (a feature).
+//            spilled value, which takes the value's own slot), or nowhere
+//            (a feature).
 // The reverse rules follow autodiff.rs's forward rules (product and quotient
 // rules, g/(2 sqrt x), norms through sqrt of dot); InverseM2/M3, whose dual
 // rule is a no-op in the reference (src/domains/linalg/mod.rs:643,687), get
@@ -44,7 +45,13 @@ struct RevIO : AccIO<P> {
     float *tape;            // tape, block slot
     float *gacc;            // this lane's f32 gradient sums: gacc[k*32]
     uint32_t valid;         // bit q: value q of the lane is a counted point
-    __device__ __forceinline__ Vf<P> T(uint32_t slot) const { return lds_lane<P>(tape + slot * 32u * P); }
+    // a tape reference (uops.h, kTapeRefX): a tape slot, or the feature or
+    // constant the forward value was loaded from
+    __device__ __forceinline__ Vf<P> T(uint32_t ref) const {
+        if (ref & kTapeRefX) return this->X(ref & kTapeRefIndex);
+        if (ref & kTapeRefC) return this->C(ref & kTapeRefIndex);
+        return lds_lane<P>(tape + ref * 32u * P);
+    }
     __device__ __forceinline__ void put_tape(uint32_t slot, const Vf<P> &v) const {
         sts_lane<P>(tape + slot * 32u * P, v);
     }
@@ -243,10 +250,14 @@ __device__ __forceinline__ void rev_op(Acc<PROF, P> &g, const RevIO<P> &io, uint
                 }
                 send<P, W, k - kd>(io, t, arg, gb);
                 g.F[0] = splat<P>(0.0f);
-            } else if constexpr (k == kn) {              // NORM: tape the norm, the vector
-                const Vf<P> q = g.F[0] / io.T(ta);
+            } else if constexpr (k == kn) {              // NORM: tape the vector; the norm is recomputed
+                Vf<P> v[W];
+                load_tape<P, W>(v, io, tb);
+                Vf<P> nrm;
+                if constexpr (W == 2) nrm = norm2(v); else nrm = norm3(v);  // the forward's value, bit for bit
+                const Vf<P> q = g.F[0] / nrm;
 #pragma unroll
-                for (int c = 0; c < W; ++c) G[c] = G[c] + q * io.T(tb + c);
+                for (int c = 0; c < W; ++c) G[c] = G[c] + q * v[c];
                 g.F[0] = splat<P>(0.0f);
             } else if constexpr (k > kn && k <= kn + W) { // GET x/y/z
                 G[k - kn - 1] = G[k - kn - 1] + g.F[0];
@@ -430,12 +441,17 @@ __device__ __forceinline__ void run_forward(Acc<PROF, P> &a, const RevIO<P> &io,
     }
 }
 
+// The next entry is read while the current one runs (the code ends with two
+// pad words).
 template <int PROF, int P>
 __device__ __forceinline__ void run_reverse(Acc<PROF, P> &g, const RevIO<P> &io, const uint32_t *rev, uint32_t n) {
+    uint32_t w0 = rev[0], w1 = rev[1];
     for (uint32_t i = 0; i < n; ++i) {
-        const uint32_t w0 = rev[2 * i], w1 = rev[2 * i + 1];
+        const uint32_t w0n = rev[2 * i + 2], w1n = rev[2 * i + 3];
         const uint32_t arg = w0 >> 8, kind = w0 & 0xFFu;
         RSR_SWITCH(RSR_R, RSR_NONE)
+        w0 = w0n;
+        w1 = w1n;
     }
 }
 
@@ -452,7 +468,7 @@ __device__ __forceinline__ void run_reverse(Acc<PROF, P> &g, const RevIO<P> &io,
 // Block-cooperative persistent kernel: a block's warps take the tiles of one
 // work item (one program on a chunk of points).  Shared memory: block
 // header (code | constants | meta | cross-warp sums), then one region per
-// warp: tape | stacks | adjoint stacks | gradient sums | Kahan state.
+// warp: tape | stacks (then adjoint stacks) | gradient sums | Kahan state.
 template <int PROF, int P>
 __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchArgs a) {
     extern __shared__ __align__(16) float smem[];
@@ -460,7 +476,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nw = blockDim.x >> 5;
     uint32_t *scode = reinterpret_cast<uint32_t *>(smem);
-    float *sconst = smem + ((a.smem_code_words + 1u + 3u) & ~3u);  // code and its pad word
+    float *sconst = smem + ((a.smem_code_words + 2u + 3u) & ~3u);  // code and its two pad words
     uint32_t *meta = reinterpret_cast<uint32_t *>(sconst + ((a.smem_const_floats + 3u) & ~3u));  // [0] item
     double *red = reinterpret_cast<double *>(meta + 4);  // [warp][1 + kAdjParams]
     float *wbase = smem + a.block_hdr_floats + (size_t)warp * a.region_floats;
@@ -479,21 +495,21 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
             continue;
         }
         const ProgDesc pd = a.progs[it.prog_begin];
-        // this program's warp region: tape | stacks | adjoint stacks | sums
+        // this program's warp region: tape | stacks | sums
         // (n_slots: tape slots; n_tape: stack depths, 5 bits per type); the
         // launch's region_floats is the largest of its programs'
         {
             const uint32_t l0 = lane_point<P>(lane, 0);
             uint32_t off = pd.n_slots * 32u * P;
             io.tape = wbase + l0;
+            // A spilled value's adjoint takes the value's own slot: the one
+            // micro-op that pops the value reads it into registers (in both
+            // sweeps) before its reverse writes the adjoint, and no later
+            // reverse step reads the forward value (every PUSH has its own slot).
 #pragma unroll
             for (int t = 0; t < N_STACKS; ++t) {
                 io.stk[t] = wbase + off + l0;
-                off += ((pd.n_tape >> (5 * t)) & 31u) * type_width(t) * 32u * P;
-            }
-#pragma unroll
-            for (int t = 0; t < N_STACKS; ++t) {
-                io.gstk[t] = wbase + off + l0;
+                io.gstk[t] = io.stk[t];
                 off += ((pd.n_tape >> (5 * t)) & 31u) * type_width(t) * 32u * P;
             }
             io.gacc = wbase + off + lane;
@@ -501,7 +517,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
         const uint32_t np = min(pd.n_consts, kAdjParams);
         float *kahan = io.gacc - lane + np * 32u;  // [2][32], after the program's own gradient sums
         for (uint32_t i = threadIdx.x; i < pd.uop_len; i += blockDim.x) scode[i] = __ldg(a.code + pd.uop_off + i);
-        if (threadIdx.x == 0) scode[pd.uop_len] = 0u;  // prefetch pad of the forward loop
+        if (threadIdx.x == 0) scode[pd.uop_len] = scode[pd.uop_len + 1] = 0u;  // prefetch pads of the loops
         for (uint32_t i = threadIdx.x; i < pd.n_consts; i += blockDim.x) sconst[i] = __ldg(a.consts + pd.const_off + i);
         for (uint32_t k = 0; k < np; ++k) io.gacc[k * 32] = 0.0f;
         kahan[lane] = 0.0f;
@@ -565,14 +581,15 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
 }
 
 // ------------------------------------------------------------- launchers
-// Shared-memory layout (floats).  Block header: code (+1 pad) | constants |
+// Shared-memory layout (floats).  Block header: code (+2 pads) | constants |
 // meta (4 words) | cross-warp sums (warps x 33 doubles).  Per warp: tape |
-// stacks (per type) | adjoint stacks (per type) | gradient sums (one row of
-// 32 per parameter, at most 32) | Kahan state (2 x 32), each program's own sizes (the kernel lays the
-// region out per item); warp_floats is the largest region of the launch.
+// stacks (per type; the reverse sweep's adjoint stacks in the same slots) |
+// gradient sums (one row of 32 per parameter, at most 32) | Kahan state (2 x
+// 32), each program's own sizes (the kernel lays the region out per item);
+// warp_floats is the largest region of the launch.
 uint32_t adj_warp_floats(uint32_t tape_slots, const uint32_t *stack_depth, int P, uint32_t n_params) {
-    uint32_t slots = tape_slots;
-    for (int t = 0; t < N_STACKS; ++t) slots += 2u * stack_depth[t] * (uint32_t)kStackWidth[t];
+    uint32_t slots = tape_slots;  // + the stacks, whose slots the adjoints reuse
+    for (int t = 0; t < N_STACKS; ++t) slots += stack_depth[t] * (uint32_t)kStackWidth[t];
     const uint32_t np = n_params < kAdjParams ? n_params : kAdjParams;
     return (slots * 32u * (uint32_t)P + np * 32u + 2u * 32u + 3u) & ~3u;
 }
@@ -585,7 +602,7 @@ uint32_t adj_pack_depth(const uint32_t *stack_depth) {
 
 void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, LaunchArgs *a) {
     const uint32_t nw = kAdjThreads / 32;
-    a->block_hdr_floats = ((code_words + 1u + 3u) & ~3u) + ((const_floats + 3u) & ~3u) + 4u +
+    a->block_hdr_floats = ((code_words + 2u + 3u) & ~3u) + ((const_floats + 3u) & ~3u) + 4u +
                           2u * nw * (1u + kAdjParams);
     a->region_floats = warp_floats;
 }
@@ -599,7 +616,8 @@ size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t warp_
 template <int PROF, int P>
 static cudaError_t launch_adj_pp(const LaunchArgs &a, uint32_t grid, size_t smem, cudaStream_t st) {
     auto k = adj_eval_kernel<PROF, P>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin);
+    static std::atomic<uint64_t> limit_raised{0};
+    cudaError_t e = raise_smem_limit(k, limit_raised);
     if (e != cudaSuccess) return e;
     k<<<grid, kAdjThreads, smem, st>>>(a);
     return cudaGetLastError();

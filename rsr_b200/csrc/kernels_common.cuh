@@ -4,6 +4,10 @@
 #pragma once
 #include <stdint.h>
 
+#include <atomic>
+
+#include <cuda_runtime.h>
+
 #include "uops.h"
 #include "vm_ops.cuh"
 
@@ -44,6 +48,21 @@ struct LaunchArgs {
 // own size: the limit is per-function state shared by all host threads, and a
 // launch from one thread must not see it lowered by another thread.
 constexpr int kMaxDynSmemOptin = 227 * 1024;
+
+// Raises kernel k's dynamic shared-memory limit to kMaxDynSmemOptin once per
+// device: `done` (a static of the caller's instance) holds one bit per
+// device on which it is set, so later launches skip the driver call.
+template <typename K>
+__host__ inline cudaError_t raise_smem_limit(K k, std::atomic<uint64_t> &done) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin);
+    if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_release);
+    return e;
+}
 
 // Kahan-compensated single-precision running sum (one per lane).
 struct Kahan {

@@ -460,7 +460,8 @@ __global__ void finalize_grad_kernel(const ProgDesc *progs, const DatasetDesc *d
 template <int PROF, int P, bool NU>
 static cudaError_t launch_grad_p(const LaunchArgs &a, uint32_t wpb, size_t smem, cudaStream_t st) {
     auto k = grad_kernel<PROF, P, NU>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin);
+    static std::atomic<uint64_t> limit_raised{0};
+    cudaError_t e = raise_smem_limit(k, limit_raised);
     if (e != cudaSuccess) return e;
     k<<<(a.n_items + wpb - 1) / wpb, wpb * 32, smem, st>>>(a);
     return cudaGetLastError();

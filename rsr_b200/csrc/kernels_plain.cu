@@ -196,7 +196,8 @@ __global__ void finalize_mse_kernel(const ProgDesc *progs, const DatasetDesc *da
 template <int P>
 static cudaError_t launch_plain_p(const LaunchArgs &a, uint32_t warps_per_block, size_t smem, cudaStream_t st) {
     auto k = plain_eval_kernel<P>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin);
+    static std::atomic<uint64_t> limit_raised{0};
+    cudaError_t e = raise_smem_limit(k, limit_raised);
     if (e != cudaSuccess) return e;
     const uint32_t blocks = (a.n_items + warps_per_block - 1) / warps_per_block;
     k<<<blocks, warps_per_block * 32, smem, st>>>(a);

@@ -273,7 +273,8 @@ template <int PROF, int P, int OMIT>
 static cudaError_t launch_reg_pp(const LaunchArgs &a, uint32_t grid, cudaStream_t st) {
     auto k = reg_eval_kernel<PROF, P, OMIT>;
     const size_t smem = ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (kRegThreads / 32)) * 4u;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin);
+    static std::atomic<uint64_t> limit_raised{0};
+    cudaError_t e = raise_smem_limit(k, limit_raised);
     if (e != cudaSuccess) return e;
     k<<<grid, kRegThreads, smem, st>>>(a);
     return cudaGetLastError();
@@ -318,7 +319,8 @@ cudaError_t launch_reg(const LaunchArgs &a, int profile, int P, unsigned omit, u
 template <int PROF, int P, int OMIT>
 static cudaError_t preload_pp(const uint32_t *zero, cudaStream_t st) {
     auto k = reg_eval_kernel<PROF, P, OMIT>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin);
+    static std::atomic<uint64_t> limit_raised{0};
+    cudaError_t e = raise_smem_limit(k, limit_raised);
     if (e != cudaSuccess) return e;
     LaunchArgs none{};
     none.run_if = zero;

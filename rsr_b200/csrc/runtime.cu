@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <thread>
+#include <unordered_map>
 #include <numeric>
 
 #include "runtime.h"
@@ -135,8 +136,8 @@ static constexpr int kRegPathStride = 8;
 // 40 KB and 81.6 ms at 20 KB; the vector and matrix workloads' tapes fit
 // 40 KB at 4 points and do not change.
 static constexpr size_t kGradTapeBudget = 80 * 1024;
-// Register adjoint: shared memory a warp's tape, stacks, adjoint stacks and
-// gradient sums may take (4 warps per block: two blocks fit an SM), and the
+// Register adjoint: shared memory a warp's tape, stacks (which the adjoint
+// stacks reuse) and gradient sums may take (4 warps per block: two blocks fit an SM), and the
 // first path number of its launches in a gradient plan.
 static constexpr size_t kAdjWarpBudget = 24 * 1024;
 static constexpr int kAdjPathBase = 0;
@@ -255,7 +256,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         if (gradient && enc[i].adj_profile >= 0 && adj_supported(enc[i].adj_profile) &&
             !(ctx->opts.flags & RSR_OPT_SLOT_ADJOINT)) {
             // register adjoint: the most points per lane (8, 4, 2) whose warp
-            // region (tape, stacks, adjoint stacks, gradient sums) fits
+            // region (tape, stacks, gradient sums) fits
             // kAdjWarpBudget; launches by that region's size in steps of 4 KB,
             // so that a block's shared memory follows its own programs
             const EncodedProgram &E = enc[i];
@@ -571,6 +572,28 @@ int upload_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t st
     return RSR_OK;
 }
 
+// Blocks per SM of a register or register-adjoint instance at a shared-memory
+// size, from the occupancy API once per (device, instance, size): the query
+// costs the host more than the launch it sizes.
+static int blocks_per_sm(int device, int kind, int profile, int P, unsigned omit, size_t smem) {
+    static std::mutex mu;
+    static std::unordered_map<uint64_t, int> cache;
+    const uint64_t key = ((uint64_t)(device & 255) << 56) | ((uint64_t)(kind & 3) << 54) |
+                         ((uint64_t)(profile & 7) << 51) | ((uint64_t)(P & 15) << 47) | ((uint64_t)(omit & 3) << 45) |
+                         (uint64_t)(smem & ((1ull << 45) - 1));
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    const int n = kind == 1 ? reg_max_blocks_per_sm(profile, P, omit, smem) : adj_max_blocks_per_sm(profile, P, smem);
+    if (n > 0) {
+        std::lock_guard<std::mutex> lk(mu);
+        cache[key] = n;
+    }
+    return n;
+}
+
 int preload_eval_kernels(rsr_ctx *ctx) {
     if (ctx->kernels_loaded) return RSR_OK;
     cudaSetDevice(ctx->device);
@@ -653,7 +676,7 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             reg_layout(g.code_words, g.const_floats, g.stack_depth, g.P, g.G, a.stack_off, &a.acc_off, &a.region_floats,
                        &a.block_hdr_floats);
             const size_t smem = ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (kRegThreads / 32)) * 4u;
-            int bps = std::max(1, reg_max_blocks_per_sm(g.profile, g.P, g.omit, smem));
+            int bps = std::max(1, blocks_per_sm(ctx->device, 1, g.profile, g.P, g.omit, smem));
             uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)bps * ctx->num_sms, g.n_items);
             g.grid = std::max(1u, grid);
             g.smem = smem;
@@ -668,7 +691,7 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
                 return fail(RSR_EINVAL, "register adjoint launch needs " + std::to_string(smem) +
                                             " bytes of shared memory per block");
             }
-            const int bps = std::max(1, adj_max_blocks_per_sm(g.profile, g.P, smem));
+            const int bps = std::max(1, blocks_per_sm(ctx->device, 3, g.profile, g.P, 0, smem));
             g.grid = std::max(1u, (uint32_t)std::min<uint64_t>((uint64_t)bps * ctx->num_sms, g.n_items));
             g.smem = smem;
             g.warps_per_block = kAdjThreads / 32;

@@ -132,9 +132,15 @@ static constexpr int kMaxAccStack = 16;   // shared-memory stack slots per type
 // every PUSH to its own stack slot so that spilled values survive the
 // forward sweep), then R reverse entries of two words each, in the order the
 // reverse sweep runs them: the forward word of the micro-op being reversed,
-// and its tape slots (first | second << 16; which forward values they hold
-// depends on the kind, kernels_adj.cu).
+// and its tape references (first | second << 16; which forward values they
+// hold depends on the kind, kernels_adj.cu).  A reference is a tape slot
+// (below kTapeRefC), or, where the forward value was a plain feature or
+// constant load not changed since, that feature (kTapeRefX | index) or
+// constant (kTapeRefC | index), which the reverse sweep reads again instead
+// of a tape slot; a value of width W reads W consecutive slots, features or
+// constants.
 static constexpr int kAdjHeaderWords = 2;
+static constexpr uint32_t kTapeRefX = 0x8000u, kTapeRefC = 0x4000u, kTapeRefIndex = 0x3FFFu;
 
 // Program descriptor for the kernels (one per program in a launch).
 struct ProgDesc {

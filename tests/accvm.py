@@ -123,7 +123,7 @@ def transpose(m, n):
     return [m[n * (i % n) + i // n] for i in range(n * n)]
 
 
-def run(program, ds):
+def run(program, ds, alias_stacks=True):
     """Gradient of the MSE w.r.t. the first min(32, P) flat parameters and
     the MSE, by the register adjoint's code; (mse, grad[32])."""
     enc = E.encoding(program, ds.num_features, 5)
@@ -235,9 +235,17 @@ def run(program, ds):
     # reverse sweep
     G = [[zero] * WIDTH[t] for t in range(5)]
     G[SF] = [(f32(2) * diff).astype(f32)]
-    GS = [[None] * max(depth[t], 1) for t in range(5)]
+    # a spilled value's adjoint takes its forward slot: the one micro-op that
+    # pops the value reads it (in both sweeps) before its reverse writes the
+    # adjoint, and nothing reads the slot's forward value after that
+    GS = S if alias_stacks else [[None] * max(depth[t], 1) for t in range(5)]
     grad = np.zeros(32)
-    T = lambda s, w: [tape[s + c] for c in range(w)]
+    def T(ref, w):  # a tape slot, or a feature / constant reference (uops.h kTapeRefX, kTapeRefC)
+        if ref & 0x8000:
+            return [X[(ref & 0x3FFF) + c] for c in range(w)]
+        if ref & 0x4000:
+            return [C((ref & 0x3FFF) + c) for c in range(w)]
+        return [tape[ref + c] for c in range(w)]
 
     def to_const(arg, g, w):
         for c in range(w):
@@ -331,8 +339,11 @@ def run(program, ds):
                 send(t, k - kd, arg, [gf * a[c] for c in range(W)], W)
                 G[SF] = [zero]
             elif k == kn:
-                q = G[SF][0] / T(ta, 1)[0]
                 a = T(tb, W)
+                d = a[0] * a[0] + a[1] * a[1]   # the norm, recomputed in the forward's operation order
+                if W == 3:
+                    d = d + a[2] * a[2]
+                q = G[SF][0] / np.sqrt(d)
                 G[t] = [g[c] + q * a[c] for c in range(W)]
                 G[SF] = [zero]
             elif kn < k <= kn + W:

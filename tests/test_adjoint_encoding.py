@@ -57,6 +57,28 @@ def test_register_adjoint_code_gives_the_dual_gradients():
     assert all(checked[name] >= 10 for name, _, _ in CASES) and checked.get("inverse", 0) >= 3, checked
 
 
+def test_adjoint_stacks_can_share_the_forward_slots():
+    """The kernel keeps a spilled value's adjoint in the value's own stack
+    slot.  That is sound when the one micro-op that pops a value is the last
+    reader of its forward slot and the first writer of its adjoint: the
+    emulator with shared slots gives bit for bit the gradients of the one
+    with separate adjoint stacks."""
+    n = 0
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        for name, dsf, popf in CASES:
+            ds, pop = dsf(), popf()
+            for p in pop:
+                try:
+                    m1, g1 = accvm.run(p, ds, alias_stacks=True)
+                except ValueError:  # no register adjoint form
+                    continue
+                m2, g2 = accvm.run(p, ds, alias_stacks=False)
+                assert np.array_equal(g1, g2, equal_nan=True) and (m1 == m2 or (np.isnan(m1) and np.isnan(m2))), name
+                n += 1
+    assert n >= 100
+
+
 def test_register_adjoint_code_layout():
     """Header words, one reverse entry per non-TAPE forward micro-op, PUSH
     slots all distinct, tape slots inside the reported tape."""
@@ -71,6 +93,10 @@ def test_register_adjoint_code_layout():
         tapes = [w for w in fwd if (w & 255) in accvm.TAPE]
         assert nr == nf - len(tapes)
         assert all((w >> 8) < tape for w in tapes)
+        # reverse references: tape slots inside the tape, or features /
+        # constants (values the reverse sweep reads again instead of a tape)
+        refs = [r for i in range(nr) for r in (int(code[3 + nf + 2 * i]) & 0xFFFF, int(code[3 + nf + 2 * i]) >> 16)]
+        assert all(r < tape or r & 0xC000 for r in refs if r)
         pushes = {}
         for w in fwd:
             t = accvm.block(w & 255)
