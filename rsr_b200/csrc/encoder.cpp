@@ -562,8 +562,8 @@ class AccEmitter {
 };
 
 // Register-adjoint code (uops.h, kAdjHeaderWords) of a tree an AccEmitter
-// has analysed: the accumulator form's evaluation order without load
-// fusion, every PUSH to its own stack slot, TAPE micro-ops next to the ops
+// has analysed: the accumulator form's evaluation order, a load directly
+// after a PUSH fused into the PUSH's word, every PUSH to its own stack slot, TAPE micro-ops next to the ops
 // whose reverse rules read forward values, and one reverse entry per
 // micro-op.  An input value that is still a plain feature or constant load
 // is not taped: its reference names the feature or constant (kTapeRefX,
@@ -750,7 +750,10 @@ class AdjEmitter {
         tape += (uint32_t)kStackWidth[t];
         return s;
     }
-    void store(int t, uint32_t slot) { fwd.push_back(uop_word((uint32_t)kTapeKind[t], slot)); }
+    void store(int t, uint32_t slot) {
+        fwd.push_back(uop_word((uint32_t)kTapeKind[t], slot));
+        push_open_ = false;
+    }
     // Reference to the current value of accumulator t as an input of the next
     // op: the feature or constant it was loaded from when no op has changed
     // it since, else a new tape slot stored now.
@@ -761,16 +764,30 @@ class AdjEmitter {
         return s;
     }
     void op(int kind, uint32_t arg, uint32_t ta = 0, uint32_t tb = 0) {
-        fwd.push_back(uop_word((uint32_t)kind, arg));
-        rev.push_back(uop_word((uint32_t)kind, arg));
-        rev.push_back(ta | (tb << 16));
         const int t = kind_block(kind), k = kind - kBlockBase[t];
+        const bool load = k == KV_LDX || k == KV_LDC;
+        if (load && push_open_ && arg < (1u << 16)) {
+            // a load right after a PUSH joins the PUSH's word (push_load_arg),
+            // in the forward stream and in the PUSH's reverse entry, whose
+            // rule then also reverses the load
+            const uint32_t pw = fwd.back();
+            const uint32_t fused = uop_word(pw & 0xFFu, push_load_arg((pw >> 8) & 15u, (uint32_t)t + 1u,
+                                                                      k == KV_LDC ? 1u : 0u, arg));
+            fwd.back() = fused;
+            rev[rev.size() - 2] = fused;
+        } else {
+            fwd.push_back(uop_word((uint32_t)kind, arg));
+            rev.push_back(uop_word((uint32_t)kind, arg));
+            rev.push_back(ta | (tb << 16));
+        }
+        push_open_ = k == KV_PUSH && !load;
         const bool fits = arg + (uint32_t)kStackWidth[t] <= kTapeRefIndex;
         if (k == KV_LDX) plain_[t] = fits ? kTapeRefX | arg : 0u;
         else if (k == KV_LDC) plain_[t] = fits ? kTapeRefC | arg : 0u;
         else if (k != KV_PUSH) plain_[t] = plain_[SF] = 0u;  // the op's own type and A_F may change
     }
     uint32_t plain_[N_STACKS] = {0, 0, 0, 0, 0};
+    bool push_open_ = false;  // the last forward word is a PUSH without a load
     int push(int t) {
         const int slot = n_push[t]++;
         op(kBlockBase[t] + KV_PUSH, (uint32_t)slot);

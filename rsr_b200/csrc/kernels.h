@@ -59,8 +59,12 @@ uint32_t adj_warp_floats(uint32_t tape_slots, const uint32_t *stack_depth, int P
 uint32_t adj_pack_depth(const uint32_t *stack_depth);
 void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, LaunchArgs *a);
 size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats);
-cudaError_t launch_adj(const LaunchArgs &a, int profile, int P, uint32_t grid, size_t smem, cudaStream_t st);
-int adj_max_blocks_per_sm(int profile, int P, size_t smem);
+// Handler sets an instance may leave out (bit 0: unary Float ops; bit 1,
+// F+V3: mat-vec with a leaf or spilled matrix), as for the register kernel.
+unsigned adj_omittable(int profile);
+cudaError_t launch_adj(const LaunchArgs &a, int profile, int P, unsigned omit, uint32_t grid, size_t smem,
+                       cudaStream_t st);
+int adj_max_blocks_per_sm(int profile, int P, unsigned omit, size_t smem);
 
 // adjoint kernel (kernels_grad.cu)
 cudaError_t launch_grad(const LaunchArgs &a, int profile, bool no_unary, uint32_t warps_per_block, size_t smem,

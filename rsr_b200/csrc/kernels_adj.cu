@@ -5,8 +5,9 @@
 // and its one dual-number pass per flat parameter (eval_simd_dual,
 // evaluator.rs:228-388) for the programs the accumulator machine takes.
 // Per tile of 32*P points a warp runs
-//   forward  the accumulator form (acc_ops.cuh) without load fusion, every
-//            PUSH to its own stack slot, and TAPE micro-ops that store the
+//   forward  the accumulator form (acc_ops.cuh) with a load after a PUSH
+//            fused into the PUSH, every PUSH to its own stack slot, and
+//            TAPE micro-ops that store the
 //            forward values the reverse rules read into a per-warp tape in
 //            shared memory;
 //   seed     G_F = 2 (pred - y) on counted points (evaluator.rs:207);
@@ -133,6 +134,32 @@ __device__ __forceinline__ void mm_tn(const Vf<P> *A, const Vf<P> *G, Vf<P> *out
         }
 }
 
+// Reverse of a load into the accumulator of type t: a constant's adjoint
+// goes to the parameter sums, and the value the load overwrote is dead.
+template <int PROF, int P, int t>
+__device__ __forceinline__ void rev_load_t(Acc<PROF, P> &g, const RevIO<P> &io, uint32_t is_const, uint32_t off) {
+    if constexpr (((kProfileTypes[PROF] >> t) & 1u) != 0u) {
+        constexpr int W = kStackWidth[t];
+        Vf<P> *G = acc_of<PROF, P, t>(g);
+        if (is_const) {
+#pragma unroll
+            for (int c = 0; c < W; ++c) io.grad_add(off + c, G[c]);
+        }
+        zero_acc<P, W>(G);
+    }
+}
+template <int PROF, int P>
+__device__ __forceinline__ void rev_load_any(Acc<PROF, P> &g, const RevIO<P> &io, uint32_t t, uint32_t is_const,
+                                             uint32_t off) {
+    switch (t) {
+        case SF: rev_load_t<PROF, P, SF>(g, io, is_const, off); break;
+        case SV2: rev_load_t<PROF, P, SV2>(g, io, is_const, off); break;
+        case SV3: rev_load_t<PROF, P, SV3>(g, io, is_const, off); break;
+        case SM2: rev_load_t<PROF, P, SM2>(g, io, is_const, off); break;
+        default: rev_load_t<PROF, P, SM3>(g, io, is_const, off); break;
+    }
+}
+
 // Reverse of one micro-op of kind K: g holds the adjoints of the machine's
 // accumulators after the micro-op and is left holding those before it.
 template <int PROF, int P, int K>
@@ -151,8 +178,11 @@ __device__ __forceinline__ void rev_op(Acc<PROF, P> &g, const RevIO<P> &io, uint
             for (int c = 0; c < W; ++c) io.grad_add(arg + c, G[c]);
             zero_acc<P, W>(G);
         } else if constexpr (k == KV_PUSH) {
+            // a load fused into the PUSH ran after it: reverse it first
+            const uint32_t lt = (arg >> 4) & 7u, slot = arg & 15u;
+            if (lt) rev_load_any<PROF, P>(g, io, lt - 1u, (arg >> 7) & 1u, arg >> 8);
 #pragma unroll
-            for (int c = 0; c < W; ++c) G[c] = G[c] + io.template GS<W>(t, arg, c);
+            for (int c = 0; c < W; ++c) G[c] = G[c] + io.template GS<W>(t, slot, c);
         } else if constexpr (k >= KV_BIN && k < KV_BIN + 3 * nb) {
             constexpr int j = (k - KV_BIN) / 3, src = (k - KV_BIN) % 3;
             constexpr int op = bin_code<t, j>();
@@ -411,16 +441,35 @@ __device__ __forceinline__ void tape_store(Acc<PROF, P> &a, const RevIO<P> &io, 
 #define RSR_X27(M, K) RSR_X9(M, K) RSR_X9(M, K + 9) RSR_X9(M, K + 18)
 #define RSR_X34(M, K) RSR_X27(M, K) RSR_X4(M, K + 27) M(K + 31) M(K + 32) M(K + 33)
 // The kinds of each profile's blocks (F 0..26, V2 32..58, V3 64..97, M2
-// 104..130, M3 136..162): a profile's switch lists only its own.
-#define RSR_SWITCH(M, EXTRA)                                                                         \
-    if constexpr (PROF == P_F) {                                                                     \
-        switch (kind) { EXTRA RSR_X27(M, K_F) default: break; }                                      \
-    } else if constexpr (PROF == P_FV3) {                                                            \
-        switch (kind) { EXTRA RSR_X27(M, K_F) RSR_X34(M, K_V3) default: break; }                     \
-    } else if constexpr (PROF == P_FV2M2) {                                                          \
-        switch (kind) { EXTRA RSR_X27(M, K_F) RSR_X27(M, K_V2) RSR_X27(M, K_M2) default: break; }    \
-    } else {                                                                                         \
-        switch (kind) { EXTRA RSR_X27(M, K_F) RSR_X34(M, K_V3) RSR_X27(M, K_M3) default: break; }    \
+// 104..130, M3 136..162): a profile's switch lists only its own, and an
+// instance leaves out the handler sets its launch's programs do not use
+// (OMIT bit 0: the unary Float ops; bit 1, F+V3: the mat-vec products whose
+// matrix is a feature, a constant or a spilled value), as the register
+// kernel's instances do.
+#define RSR_ADJ_F(M) RSR_X27(M, K_F)
+#define RSR_ADJ_F_NU(M) RSR_X9(M, K_F) RSR_X9(M, K_F + 9) M(K_F + 18) M(K_F + 19) M(K_F + 20)
+#define RSR_ADJ_V3(M) RSR_X34(M, K_V3)
+#define RSR_ADJ_V3_NM(M) RSR_X27(M, K_V3) M(K_V3 + 27) M(K_V3 + 28) M(K_V3 + 29) M(K_V3 + 33)
+static_assert(kv_mulm(5, 3) == 29 && kv_make(5, 3) == 33, "Vec3 block: mat-vec kinds at 29..32");
+#define RSR_SWITCH(M, EXTRA)                                                                          \
+    if constexpr (PROF == P_F && (OMIT & 1)) {                                                        \
+        switch (kind) { EXTRA RSR_ADJ_F_NU(M) default: break; }                                       \
+    } else if constexpr (PROF == P_F) {                                                               \
+        switch (kind) { EXTRA RSR_ADJ_F(M) default: break; }                                          \
+    } else if constexpr (PROF == P_FV3 && (OMIT & 3) == 3) {                                          \
+        switch (kind) { EXTRA RSR_ADJ_F_NU(M) RSR_ADJ_V3_NM(M) default: break; }                      \
+    } else if constexpr (PROF == P_FV3 && (OMIT & 1)) {                                               \
+        switch (kind) { EXTRA RSR_ADJ_F_NU(M) RSR_ADJ_V3(M) default: break; }                         \
+    } else if constexpr (PROF == P_FV3 && (OMIT & 2)) {                                               \
+        switch (kind) { EXTRA RSR_ADJ_F(M) RSR_ADJ_V3_NM(M) default: break; }                         \
+    } else if constexpr (PROF == P_FV3) {                                                             \
+        switch (kind) { EXTRA RSR_ADJ_F(M) RSR_ADJ_V3(M) default: break; }                            \
+    } else if constexpr (PROF == P_FV2M2 && (OMIT & 1)) {                                             \
+        switch (kind) { EXTRA RSR_ADJ_F_NU(M) RSR_X27(M, K_V2) RSR_X27(M, K_M2) default: break; }     \
+    } else if constexpr (PROF == P_FV2M2) {                                                           \
+        switch (kind) { EXTRA RSR_ADJ_F(M) RSR_X27(M, K_V2) RSR_X27(M, K_M2) default: break; }        \
+    } else {                                                                                          \
+        switch (kind) { EXTRA RSR_ADJ_F(M) RSR_ADJ_V3(M) RSR_X27(M, K_M3) default: break; }           \
     }
 #define RSR_TAPES                                                            \
     case kTapeKind[SF]: tape_store<PROF, P, SF>(a, io, arg); break;          \
@@ -430,7 +479,7 @@ __device__ __forceinline__ void tape_store(Acc<PROF, P> &a, const RevIO<P> &io, 
     case kTapeKind[SM3]: tape_store<PROF, P, SM3>(a, io, arg); break;
 #define RSR_NONE
 
-template <int PROF, int P>
+template <int PROF, int P, int OMIT>
 __device__ __forceinline__ void run_forward(Acc<PROF, P> &a, const RevIO<P> &io, const uint32_t *code, uint32_t len) {
     uint32_t w = code[0];
     for (uint32_t pc = 0; pc < len; ++pc) {
@@ -443,7 +492,7 @@ __device__ __forceinline__ void run_forward(Acc<PROF, P> &a, const RevIO<P> &io,
 
 // The next entry is read while the current one runs (the code ends with two
 // pad words).
-template <int PROF, int P>
+template <int PROF, int P, int OMIT>
 __device__ __forceinline__ void run_reverse(Acc<PROF, P> &g, const RevIO<P> &io, const uint32_t *rev, uint32_t n) {
     uint32_t w0 = rev[0], w1 = rev[1];
     for (uint32_t i = 0; i < n; ++i) {
@@ -458,6 +507,10 @@ __device__ __forceinline__ void run_reverse(Acc<PROF, P> &g, const RevIO<P> &io,
 #undef RSR_NONE
 #undef RSR_TAPES
 #undef RSR_SWITCH
+#undef RSR_ADJ_F
+#undef RSR_ADJ_F_NU
+#undef RSR_ADJ_V3
+#undef RSR_ADJ_V3_NM
 #undef RSR_X34
 #undef RSR_X27
 #undef RSR_X9
@@ -469,7 +522,7 @@ __device__ __forceinline__ void run_reverse(Acc<PROF, P> &g, const RevIO<P> &io,
 // work item (one program on a chunk of points).  Shared memory: block
 // header (code | constants | meta | cross-warp sums), then one region per
 // warp: tape | stacks (then adjoint stacks) | gradient sums | Kahan state.
-template <int PROF, int P>
+template <int PROF, int P, int OMIT>
 __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchArgs a) {
     extern __shared__ __align__(16) float smem[];
     if (a.run_if && *a.run_if == 0u) return;
@@ -536,7 +589,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
             for (int q = 0; q < P; ++q) valid |= (t0 + lane_point<P>(lane, q) < ds.n_eval ? 1u : 0u) << q;
             io.valid = valid;
             Acc<PROF, P> acc;
-            run_forward<PROF, P>(acc, io, fwd, n_fwd);
+            run_forward<PROF, P, OMIT>(acc, io, fwd, n_fwd);
             const Vf<P> y = load_lane<P>(ds.y + p0);
             Acc<PROF, P> g;
             g.F[0] = splat<P>(0.0f);
@@ -556,7 +609,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
             }
             kahan[lane] = ks.s;
             kahan[32 + lane] = ks.c;
-            run_reverse<PROF, P>(g, io, rev, n_rev);
+            run_reverse<PROF, P, OMIT>(g, io, rev, n_rev);
         }
         // per-warp sums in f64, then across warps in a fixed order
         {
@@ -613,9 +666,9 @@ size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t warp_
     return ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (kAdjThreads / 32)) * 4u;
 }
 
-template <int PROF, int P>
+template <int PROF, int P, int OMIT>
 static cudaError_t launch_adj_pp(const LaunchArgs &a, uint32_t grid, size_t smem, cudaStream_t st) {
-    auto k = adj_eval_kernel<PROF, P>;
+    auto k = adj_eval_kernel<PROF, P, OMIT>;
     static std::atomic<uint64_t> limit_raised{0};
     cudaError_t e = raise_smem_limit(k, limit_raised);
     if (e != cudaSuccess) return e;
@@ -623,13 +676,22 @@ static cudaError_t launch_adj_pp(const LaunchArgs &a, uint32_t grid, size_t smem
     return cudaGetLastError();
 }
 
-template <int PROF, int P>
+template <int PROF, int P, int OMIT>
 static int adj_occ(size_t smem) {
-    auto k = adj_eval_kernel<PROF, P>;
+    auto k = adj_eval_kernel<PROF, P, OMIT>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin) != cudaSuccess) return 0;
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kAdjThreads, smem) != cudaSuccess) return 0;
     return n;
+}
+
+// Loads one instance ahead of its first real launch (an empty launch: run_if
+// points at a zero word, every thread returns at its first check).
+template <int PROF, int P, int OMIT>
+static cudaError_t adj_preload_pp(const uint32_t *zero, cudaStream_t st) {
+    LaunchArgs none{};
+    none.run_if = zero;
+    return launch_adj_pp<PROF, P, OMIT>(none, 1, 0, st);
 }
 
 bool adj_supported(int profile) { return profile >= P_F && profile <= P_FV3M3; }
@@ -637,58 +699,89 @@ bool adj_supported(int profile) { return profile >= P_F && profile <= P_FV3M3; }
 // P = 8 exists for the F and F+V3 profiles only (the others would spill).
 int adj_max_p(int profile) { return profile == P_F || profile == P_FV3 ? 8 : 4; }
 
-cudaError_t launch_adj(const LaunchArgs &a, int profile, int P, uint32_t grid, size_t smem, cudaStream_t st) {
+// The instances that exist: (profile, P) as above; OMIT 0..3 for F+V3,
+// 0..1 for F and F+V2+M2, 0 for F+V3+M3.  `what` picks the launcher, the
+// occupancy query or the preload of instance (PROF, P, omit).
+enum AdjWhat { ADJ_LAUNCH, ADJ_OCC, ADJ_PRELOAD };
+struct AdjCall {
+    AdjWhat what;
+    const LaunchArgs *a;
+    uint32_t grid;
+    size_t smem;
+    cudaStream_t st;
+    const uint32_t *zero;
+    int occ = 0;
+};
+
+template <int PROF, int P, int OMIT>
+static cudaError_t adj_do(AdjCall &c) {
+    if (c.what == ADJ_LAUNCH) return launch_adj_pp<PROF, P, OMIT>(*c.a, c.grid, c.smem, c.st);
+    if (c.what == ADJ_OCC) {
+        c.occ = adj_occ<PROF, P, OMIT>(c.smem);
+        return cudaSuccess;
+    }
+    return adj_preload_pp<PROF, P, OMIT>(c.zero, c.st);
+}
+
+template <int PROF, int P>
+static cudaError_t adj_do_omit(AdjCall &c, unsigned omit) {
+    if constexpr (PROF == P_FV3) {
+        switch (omit & 3u) {
+            case 3: return adj_do<PROF, P, 3>(c);
+            case 2: return adj_do<PROF, P, 2>(c);
+            case 1: return adj_do<PROF, P, 1>(c);
+            default: return adj_do<PROF, P, 0>(c);
+        }
+    } else if constexpr (PROF == P_F || PROF == P_FV2M2) {
+        return omit & 1u ? adj_do<PROF, P, 1>(c) : adj_do<PROF, P, 0>(c);
+    } else {
+        return adj_do<PROF, P, 0>(c);
+    }
+}
+
+static cudaError_t adj_dispatch(AdjCall &c, int profile, int P, unsigned omit) {
     if (P >= 8) {
-        if (profile == P_F) return launch_adj_pp<P_F, 8>(a, grid, smem, st);
-        if (profile == P_FV3) return launch_adj_pp<P_FV3, 8>(a, grid, smem, st);
+        if (profile == P_F) return adj_do_omit<P_F, 8>(c, omit);
+        if (profile == P_FV3) return adj_do_omit<P_FV3, 8>(c, omit);
         return cudaErrorInvalidValue;
     }
     switch (profile * 2 + (P >= 4 ? 1 : 0)) {
-        case 0: return launch_adj_pp<P_F, 2>(a, grid, smem, st);
-        case 1: return launch_adj_pp<P_F, 4>(a, grid, smem, st);
-        case 2: return launch_adj_pp<P_FV3, 2>(a, grid, smem, st);
-        case 3: return launch_adj_pp<P_FV3, 4>(a, grid, smem, st);
-        case 4: return launch_adj_pp<P_FV2M2, 2>(a, grid, smem, st);
-        case 5: return launch_adj_pp<P_FV2M2, 4>(a, grid, smem, st);
-        case 6: return launch_adj_pp<P_FV3M3, 2>(a, grid, smem, st);
-        case 7: return launch_adj_pp<P_FV3M3, 4>(a, grid, smem, st);
+        case 0: return adj_do_omit<P_F, 2>(c, omit);
+        case 1: return adj_do_omit<P_F, 4>(c, omit);
+        case 2: return adj_do_omit<P_FV3, 2>(c, omit);
+        case 3: return adj_do_omit<P_FV3, 4>(c, omit);
+        case 4: return adj_do_omit<P_FV2M2, 2>(c, omit);
+        case 5: return adj_do_omit<P_FV2M2, 4>(c, omit);
+        case 6: return adj_do_omit<P_FV3M3, 2>(c, omit);
+        case 7: return adj_do_omit<P_FV3M3, 4>(c, omit);
         default: return cudaErrorInvalidValue;
     }
 }
 
-// Loads one instance ahead of its first real launch (an empty launch: run_if
-// points at a zero word, every thread returns at its first check).
-template <int PROF, int P>
-static cudaError_t adj_preload_pp(const uint32_t *zero, cudaStream_t st) {
-    LaunchArgs none{};
-    none.run_if = zero;
-    return launch_adj_pp<PROF, P>(none, 1, 0, st);
+unsigned adj_omittable(int profile) {
+    return profile == P_FV3 ? 3u : profile == P_F || profile == P_FV2M2 ? 1u : 0u;
+}
+
+cudaError_t launch_adj(const LaunchArgs &a, int profile, int P, unsigned omit, uint32_t grid, size_t smem,
+                       cudaStream_t st) {
+    AdjCall c{ADJ_LAUNCH, &a, grid, smem, st, nullptr};
+    return adj_dispatch(c, profile, P, omit);
+}
+
+int adj_max_blocks_per_sm(int profile, int P, unsigned omit, size_t smem) {
+    AdjCall c{ADJ_OCC, nullptr, 0, smem, nullptr, nullptr};
+    return adj_dispatch(c, profile, P, omit) == cudaSuccess ? c.occ : 0;
 }
 
 cudaError_t preload_adj(const uint32_t *zero, cudaStream_t st) {
-    const cudaError_t r[] = {adj_preload_pp<P_F, 2>(zero, st),     adj_preload_pp<P_F, 4>(zero, st),
-                             adj_preload_pp<P_F, 8>(zero, st),     adj_preload_pp<P_FV3, 2>(zero, st),
-                             adj_preload_pp<P_FV3, 4>(zero, st),   adj_preload_pp<P_FV3, 8>(zero, st),
-                             adj_preload_pp<P_FV2M2, 2>(zero, st), adj_preload_pp<P_FV2M2, 4>(zero, st),
-                             adj_preload_pp<P_FV3M3, 2>(zero, st), adj_preload_pp<P_FV3M3, 4>(zero, st)};
-    for (cudaError_t e : r)
-        if (e != cudaSuccess) return e;
+    AdjCall c{ADJ_PRELOAD, nullptr, 0, 0, st, zero};
+    for (int profile = P_F; profile <= P_FV3M3; ++profile)
+        for (int P = 2; P <= adj_max_p(profile); P *= 2)
+            for (unsigned omit = 0; omit <= adj_omittable(profile); ++omit) {
+                const cudaError_t e = adj_dispatch(c, profile, P, omit);
+                if (e != cudaSuccess) return e;
+            }
     return cudaSuccess;
-}
-
-int adj_max_blocks_per_sm(int profile, int P, size_t smem) {
-    if (P >= 8) return profile == P_F ? adj_occ<P_F, 8>(smem) : profile == P_FV3 ? adj_occ<P_FV3, 8>(smem) : 0;
-    switch (profile * 2 + (P >= 4 ? 1 : 0)) {
-        case 0: return adj_occ<P_F, 2>(smem);
-        case 1: return adj_occ<P_F, 4>(smem);
-        case 2: return adj_occ<P_FV3, 2>(smem);
-        case 3: return adj_occ<P_FV3, 4>(smem);
-        case 4: return adj_occ<P_FV2M2, 2>(smem);
-        case 5: return adj_occ<P_FV2M2, 4>(smem);
-        case 6: return adj_occ<P_FV3M3, 2>(smem);
-        case 7: return adj_occ<P_FV3M3, 4>(smem);
-        default: return 0;
-    }
 }
 
 }  // namespace rsr

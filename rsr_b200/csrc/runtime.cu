@@ -234,7 +234,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                                 (uint32_t)(pop.param_off[i + 1] - p0), P.datasets[prog_ds[i]].num_features, &enc[i],
                                 &emsg[i], fuse, f);
     };
-    if (n >= 256) {
+    if (n >= 64) {  // a program takes ~2 us to encode; a pool run costs ~10 us
         std::unique_ptr<TaskPool> &pool = scratch ? scratch->pool : ctx->encoders;
         if (!pool)
             pool = std::make_unique<TaskPool>(std::max(
@@ -252,6 +252,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
     // path per program: <= -2 slot-file adjoint, -1 plain, >= 0 register
     // profile (MSE plans) or register adjoint (gradient plans)
     std::vector<int> path(n);
+    std::vector<uint8_t> adj_omit(n, 0);
     for (uint32_t i = 0; i < n; ++i) {
         if (gradient && enc[i].adj_profile >= 0 && adj_supported(enc[i].adj_profile) &&
             !(ctx->opts.flags & RSR_OPT_SLOT_ADJOINT)) {
@@ -267,6 +268,18 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             while (pc >= 0 && (size_t)adj_warp_floats(E.adj_tape, depth, 2 << pc, np) * 4u > kAdjWarpBudget) --pc;
             if (pc >= 0) {
                 const int bucket = (int)((adj_warp_floats(E.adj_tape, depth, 2 << pc, np) + 1023u) / 1024u);
+                // the handler sets the program does not use (forward words:
+                // the code after the two header words); a launch leaves out
+                // those none of its programs uses
+                const uint32_t mv = (uint32_t)(K_V3 + kv_mulm(kBinOps[SV3], 3));
+                unsigned omit = adj_omittable(E.adj_profile);
+                const uint32_t n_fwd = E.adj_code.empty() ? 0u : E.adj_code[0];
+                for (uint32_t q = 0; q < n_fwd; ++q) {
+                    const uint32_t kind = E.adj_code[kAdjHeaderWords + q] & 0xFFu;
+                    if (kind >= (uint32_t)K_F_UN && kind < (uint32_t)K_F_END) omit &= ~1u;
+                    if (kind >= mv + 1 && kind <= mv + 3) omit &= ~2u;
+                }
+                adj_omit[i] = (uint8_t)omit;
                 path[i] = kAdjPathBase + ((bucket * 3 + pc) * N_PROFILES + E.adj_profile);
                 continue;
             }
@@ -334,13 +347,20 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         }
     }
     // group programs by (path, dataset), each group sorted by descending code length
+    // (one 64-bit key per program: path, dataset, then longer code first and
+    // the caller's order among equals, as a stable sort by those would give)
     std::vector<uint32_t> order(n);
-    std::iota(order.begin(), order.end(), 0u);
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-        if (path[a] != path[b]) return path[a] < path[b];
-        if (prog_ds[a] != prog_ds[b]) return prog_ds[a] < prog_ds[b];
-        return enc[a].reg_code.size() + enc[a].slot_code.size() > enc[b].reg_code.size() + enc[b].slot_code.size();
-    });
+    {
+        std::vector<std::pair<uint64_t, uint32_t>> keyed(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint64_t len = enc[i].reg_code.size() + enc[i].slot_code.size();
+            const uint64_t key = ((uint64_t)(uint32_t)(path[i] + (1 << 20)) << 42) | ((uint64_t)prog_ds[i] << 22) |
+                                 ((1ull << 22) - 1 - std::min<uint64_t>(len, (1ull << 22) - 1));
+            keyed[i] = {key, i};
+        }
+        std::sort(keyed.begin(), keyed.end());
+        for (uint32_t i = 0; i < n; ++i) order[i] = keyed[i].second;
+    }
     P.progs.resize(n);
     P.orig = order;
     {
@@ -402,6 +422,10 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         g.profile = g.kind == 3 ? (pth - kAdjPathBase) % N_PROFILES
                   : pth >= 0 ? pth % kRegPathStride : pth <= -2 ? (-2 - pth) % N_PROFILES : -1;
         g.omit = g.kind == 1 ? (unsigned)(pth / kRegPathStride / 3) : 0u;
+        if (g.kind == 3) {
+            g.omit = 3u;
+            for (uint32_t j = li; j < end; ++j) g.omit &= adj_omit[order[j]];
+        }
         g.item_begin = (uint32_t)P.items.size();
         if (g.kind == 3) {
             g.G = 1;
@@ -491,6 +515,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             }
         }
         std::stable_sort(tail.begin(), tail.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+        g.item_work = std::max(full.empty() ? 0 : full[0].first, tail.empty() ? 0 : tail[0].first);
         size_t a = 0, b = 0;
         while (a < full.size() || b < tail.size())
             P.items.push_back(b == tail.size() || (a < full.size() && full[a].first >= tail[b].first) ? full[a++].second
@@ -505,6 +530,10 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         P.groups.push_back(g);
         li = end;
     }
+    // Launches run side by side (enqueue_plan): the one whose longest item
+    // takes longest goes first, so that it does not become the plan's tail.
+    std::stable_sort(P.groups.begin(), P.groups.end(),
+                     [](const Group &a, const Group &b) { return a.item_work > b.item_work; });
     return RSR_OK;
 }
 
@@ -586,7 +615,7 @@ static int blocks_per_sm(int device, int kind, int profile, int P, unsigned omit
         auto it = cache.find(key);
         if (it != cache.end()) return it->second;
     }
-    const int n = kind == 1 ? reg_max_blocks_per_sm(profile, P, omit, smem) : adj_max_blocks_per_sm(profile, P, smem);
+    const int n = kind == 1 ? reg_max_blocks_per_sm(profile, P, omit, smem) : adj_max_blocks_per_sm(profile, P, omit, smem);
     if (n > 0) {
         std::lock_guard<std::mutex> lk(mu);
         cache[key] = n;
@@ -691,11 +720,11 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
                 return fail(RSR_EINVAL, "register adjoint launch needs " + std::to_string(smem) +
                                             " bytes of shared memory per block");
             }
-            const int bps = std::max(1, blocks_per_sm(ctx->device, 3, g.profile, g.P, 0, smem));
+            const int bps = std::max(1, blocks_per_sm(ctx->device, 3, g.profile, g.P, g.omit, smem));
             g.grid = std::max(1u, (uint32_t)std::min<uint64_t>((uint64_t)bps * ctx->num_sms, g.n_items));
             g.smem = smem;
             g.warps_per_block = kAdjThreads / 32;
-            e = launch_adj(a, g.profile, g.P, g.grid, smem, gs);
+            e = launch_adj(a, g.profile, g.P, g.omit, g.grid, smem, gs);
         } else {
             const size_t per = grad_smem_per_warp(g.code_words, g.const_floats, g.slots, g.adj_slots, g.P);
             a.smem_adj_slots = g.adj_slots;
@@ -1268,7 +1297,7 @@ int rsr_batch_describe(rsr_ctx *ctx, rsr_batch *b, char *buf, size_t len) {
         const Group &g = b->plan.groups[i];
         const char *kn = g.kind == 0 ? "slot" : g.kind == 1 ? "register" : g.kind == 2 ? "adjoint" : "register_adjoint";
         s += (i ? ", " : "") + std::string("{\"kernel\": \"") + kn + "\", \"profile\": " + std::to_string(g.profile) +
-             ", \"no_unary\": " + ((g.kind == 1 ? (g.omit & 1u) != 0 : g.no_unary) ? "true" : "false") +
+             ", \"no_unary\": " + (((g.kind == 1 || g.kind == 3) ? (g.omit & 1u) != 0 : g.no_unary) ? "true" : "false") +
              ", \"no_matrix_operand\": " + ((g.kind == 1 && (g.omit & 2u)) ? "true" : "false") +
              ", \"points_per_thread\": " + std::to_string(g.P) + ", \"programs_per_warp\": " + std::to_string(g.G) +
              ", \"items\": " + std::to_string(g.n_items) + ", \"flops\": " + std::to_string(g.flops) +

@@ -115,6 +115,7 @@ struct Group {
     mutable uint32_t warps_per_block = 0;
     uint64_t flops = 0;           // algorithmic FP32 lane-ops of one run
     uint64_t program_points = 0;
+    uint64_t item_work = 0;       // code length x tiles of the group's longest item
 };
 
 // A population encoded and laid out for the device: what one launch of the

@@ -128,7 +128,8 @@ static constexpr int kMaxAccStack = 16;   // shared-memory stack slots per type
 
 // Register adjoint code of a program (EncodedProgram::adj_code): word 0 the
 // forward length F, word 1 the reverse length R, then F forward micro-op
-// words (accumulator form without load fusion, TAPE kinds between them,
+// words (accumulator form, a load after a PUSH fused into the PUSH's word
+// but no load fused into a unary op, TAPE kinds between them,
 // every PUSH to its own stack slot so that spilled values survive the
 // forward sweep), then R reverse entries of two words each, in the order the
 // reverse sweep runs them: the forward word of the micro-op being reversed,

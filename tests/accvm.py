@@ -165,7 +165,11 @@ def run(program, ds, alias_stacks=True):
         elif k == 1:
             A[t] = [C(arg + c) for c in range(W)]
         elif k == 2:
-            S[t][arg] = list(A[t])
+            S[t][arg & 15] = list(A[t])
+            lt = (arg >> 4) & 7   # a load fused into the PUSH (uops.h push_load_arg)
+            if lt:
+                off, W2 = arg >> 8, WIDTH[lt - 1]
+                A[lt - 1] = [C(off + c) if (arg >> 7) & 1 else X[off + c] for c in range(W2)]
         elif k < 3 + 3 * nb:
             j, src = (k - 3) // 3, (k - 3) % 3
             B = fetch(t, src, arg, W)
@@ -270,7 +274,13 @@ def run(program, ds, alias_stacks=True):
             to_const(arg, g, W)
             G[t] = [zero] * W
         elif k == 2:
-            G[t] = [g[c] + GS[t][arg][c] for c in range(W)]
+            lt = (arg >> 4) & 7
+            if lt:  # the fused load ran after the PUSH: reverse it first
+                if (arg >> 7) & 1:
+                    to_const(arg >> 8, G[lt - 1], WIDTH[lt - 1])
+                G[lt - 1] = [zero] * WIDTH[lt - 1]
+                g = G[t]
+            G[t] = [g[c] + GS[t][arg & 15][c] for c in range(W)]
         elif k < 3 + 3 * nb:
             j, src = (k - 3) // 3, (k - 3) % 3
             if j == 0:

@@ -101,6 +101,6 @@ def test_register_adjoint_code_layout():
         for w in fwd:
             t = accvm.block(w & 255)
             if (w & 255) - accvm.BASE[t] == 2:
-                pushes.setdefault(t, []).append(w >> 8)
+                pushes.setdefault(t, []).append((w >> 8) & 15)  # the slot; a fused load sits above it
         for t, slots in pushes.items():
             assert sorted(slots) == list(range(len(slots))) and len(slots) == depth[t]
