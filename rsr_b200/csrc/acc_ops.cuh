@@ -160,7 +160,7 @@ __device__ __forceinline__ void acc_op(Acc<PROF, P> &a, const AccIO<P> &io, uint
             const uint32_t slot = arg & 15u, lt = (arg >> 4) & 7u;
 #pragma unroll
             for (int c = 0; c < W; ++c) io.template put<W>(t, slot, c, A[c]);
-            if (lt) load_any<PROF, P>(a, io, lt - 1u, (arg >> 7) & 1u, arg >> 8);
+            if (lt) load_any<PROF, P>(a, io, lt - 1u, (arg >> 7) & 1u, (arg >> 8) & ((1u << kLdOffsetBits) - 1u));
         } else if constexpr (k >= KV_BIN && k < KV_BIN + 3 * nb) {
             constexpr int j = (k - KV_BIN) / 3, src = (k - KV_BIN) % 3;
             Vf<P> b[W];

@@ -563,9 +563,10 @@ class AccEmitter {
 
 // Register-adjoint code (uops.h, kAdjHeaderWords) of a tree an AccEmitter
 // has analysed: the accumulator form's evaluation order, a load directly
-// after a PUSH fused into the PUSH's word, every PUSH to its own stack slot, TAPE micro-ops next to the ops
-// whose reverse rules read forward values, and one reverse entry per
-// micro-op.  An input value that is still a plain feature or constant load
+// after a PUSH fused into the PUSH's word, every PUSH to its own stack slot,
+// tape stores of the forward values the reverse rules read (carried by the
+// op's own forward entry where the value is of the op's type, else a TAPE
+// entry), and one reverse entry per micro-op.  An input value that is still a plain feature or constant load
 // is not taped: its reference names the feature or constant (kTapeRefX,
 // kTapeRefC).  Tape references hold (first | second << 16):
 //   F MUL: A before; DIV: A after; RDIV: A before, A after;
@@ -620,7 +621,7 @@ class AdjEmitter {
                 if (before) ta = tape_in(t);
                 if (after) (before ? tb : ta) = take(t);
                 op(kind, arg, ta, tb);
-                if (after) store(t, before ? tb : ta);
+                if (after) store_after(t, before ? tb : ta);
                 break;
             }
             case C_DOT: {
@@ -651,7 +652,7 @@ class AdjEmitter {
                 const bool after = u == 2 || u == 4;
                 const uint32_t ta = after ? take(SF) : tape_in(SF);
                 op(K_F_UN + u, 0, ta);
-                if (after) store(SF, ta);
+                if (after) store_after(SF, ta);
                 break;
             }
             case C_NORM: case C_GET: {
@@ -683,7 +684,7 @@ class AdjEmitter {
                 } else {
                     const uint32_t tb = tape_in(t), ta = take(t);
                     op(kBlockBase[t] + KM_INVERSE, 0, ta, tb);
-                    store(t, ta);
+                    store_after(t, ta);
                 }
                 break;
             }
@@ -704,10 +705,10 @@ class AdjEmitter {
         }
     }
 
-    // The code: header, forward words, reverse entries in reverse order.
+    // The code: header, forward entries, reverse entries in reverse order.
     void finish(std::vector<uint32_t> *out) const {
         out->clear();
-        out->push_back((uint32_t)fwd.size());
+        out->push_back((uint32_t)(fwd.size() / 2));
         out->push_back((uint32_t)(rev.size() / 2));
         out->insert(out->end(), fwd.begin(), fwd.end());
         for (size_t i = rev.size(); i >= 2; i -= 2) {
@@ -750,33 +751,52 @@ class AdjEmitter {
         tape += (uint32_t)kStackWidth[t];
         return s;
     }
-    void store(int t, uint32_t slot) {
+    // A TAPE entry of its own: a store the op's entry cannot carry.
+    void tape_entry(int t, uint32_t slot) {
         fwd.push_back(uop_word((uint32_t)kTapeKind[t], slot));
+        fwd.push_back(kNoTapes);
         push_open_ = false;
+    }
+    // Tape store of accumulator t after the op just emitted: carried by that
+    // op's entry when it is the op's own type.
+    void store_after(int t, uint32_t slot) {
+        uint32_t &tapes = fwd.back();
+        if (kind_block((int)(fwd[fwd.size() - 2] & 0xFFu)) == t && (tapes >> 16) == kNoTape)
+            tapes = (tapes & 0xFFFFu) | (slot << 16);
+        else
+            tape_entry(t, slot);
     }
     // Reference to the current value of accumulator t as an input of the next
     // op: the feature or constant it was loaded from when no op has changed
-    // it since, else a new tape slot stored now.
+    // it since, else a new tape slot, stored before the op runs (by the op's
+    // entry, or by a TAPE entry for another type's accumulator).
     uint32_t tape_in(int t) {
         if (plain_[t]) return plain_[t];
         const uint32_t s = take(t);
-        store(t, s);
+        pending_[n_pending_++] = {t, s};
         return s;
     }
     void op(int kind, uint32_t arg, uint32_t ta = 0, uint32_t tb = 0) {
         const int t = kind_block(kind), k = kind - kBlockBase[t];
+        uint32_t before = kNoTape;
+        for (int q = 0; q < n_pending_; ++q) {
+            if (pending_[q].t == t && before == kNoTape) before = pending_[q].slot;
+            else tape_entry(pending_[q].t, pending_[q].slot);
+        }
+        n_pending_ = 0;
         const bool load = k == KV_LDX || k == KV_LDC;
-        if (load && push_open_ && arg < (1u << 16)) {
+        if (load && push_open_ && arg < (1u << kLdOffsetBits)) {
             // a load right after a PUSH joins the PUSH's word (push_load_arg),
             // in the forward stream and in the PUSH's reverse entry, whose
             // rule then also reverses the load
-            const uint32_t pw = fwd.back();
+            const uint32_t pw = fwd[fwd.size() - 2];
             const uint32_t fused = uop_word(pw & 0xFFu, push_load_arg((pw >> 8) & 15u, (uint32_t)t + 1u,
                                                                       k == KV_LDC ? 1u : 0u, arg));
-            fwd.back() = fused;
+            fwd[fwd.size() - 2] = fused;
             rev[rev.size() - 2] = fused;
         } else {
             fwd.push_back(uop_word((uint32_t)kind, arg));
+            fwd.push_back(before | (kNoTape << 16));
             rev.push_back(uop_word((uint32_t)kind, arg));
             rev.push_back(ta | (tb << 16));
         }
@@ -787,7 +807,10 @@ class AdjEmitter {
         else if (k != KV_PUSH) plain_[t] = plain_[SF] = 0u;  // the op's own type and A_F may change
     }
     uint32_t plain_[N_STACKS] = {0, 0, 0, 0, 0};
-    bool push_open_ = false;  // the last forward word is a PUSH without a load
+    bool push_open_ = false;  // the last forward entry is a PUSH without a load
+    struct Pending { int t; uint32_t slot; };
+    Pending pending_[2];      // tape stores before the next op (at most two: A-form scale / mat-vec)
+    int n_pending_ = 0;
     int push(int t) {
         const int slot = n_push[t]++;
         op(kBlockBase[t] + KV_PUSH, (uint32_t)slot);
@@ -798,9 +821,10 @@ class AdjEmitter {
     const AccEmitter &an_;
 };
 
-// Peephole pass over the accumulator form: a PUSH directly followed by a
-// load becomes part of the load, and a load directly followed by a unary op
-// on the loaded value becomes the load's post-op.
+// Peephole passes over the accumulator form: a load directly followed by a
+// unary op on the loaded value becomes the op's operand load; a PUSH
+// directly followed by a load carries the load; a PUSH directly followed by
+// a unary op that loads its operand carries both (the op as its post-op).
 int kind_block(int kind) { return kind >= K_M3 ? SM3 : kind >= K_M2 ? SM2 : kind >= K_V3 ? SV3 : kind >= K_V2 ? SV2 : SF; }
 
 int post_op_of(int kind, int t) {
@@ -819,7 +843,7 @@ int post_op_of(int kind, int t) {
 
 bool is_unary_kind(int kind, int t) { return post_op_of(kind, t) != 0; }
 
-// Both passes rewrite the code in place: a word is written at or before the
+// The passes rewrite the code in place: a word is written at or before the
 // position just read, after the words it depends on were read.
 void fuse_loads(std::vector<uint32_t> *code) {
     std::vector<uint32_t> &c = *code;
@@ -830,7 +854,7 @@ void fuse_loads(std::vector<uint32_t> *code) {
         const int t = kind_block(kind), k = kind - kBlockBase[t];
         if ((k == KV_LDX || k == KV_LDC) && i + 1 < c.size()) {
             const int kn = (int)(c[i + 1] & 0xFFu);
-            if (kind_block(kn) == t && is_unary_kind(kn, t)) {
+            if (kind_block(kn) == t && is_unary_kind(kn, t) && (c[i] >> 8) < (1u << kLdOffsetBits)) {
                 c[w++] = uop_word((uint32_t)kn, unary_load_arg(c[i] >> 8, k == KV_LDX ? 1u : 2u));
                 ++i;
                 continue;
@@ -846,9 +870,29 @@ void fuse_loads(std::vector<uint32_t> *code) {
         const int t = kind_block(kind), k = kind - kBlockBase[t];
         if (k == KV_PUSH && i + 1 < c.size()) {
             const int kn = (int)(c[i + 1] & 0xFFu), tn = kind_block(kn), kk = kn - kBlockBase[tn];
-            if (kk == KV_LDX || kk == KV_LDC) {
+            if ((kk == KV_LDX || kk == KV_LDC) && (c[i + 1] >> 8) < (1u << kLdOffsetBits)) {
                 c[w++] = uop_word((uint32_t)kind, push_load_arg(c[i] >> 8, (uint32_t)tn + 1u, kk == KV_LDC ? 1u : 0u,
                                                                c[i + 1] >> 8));
+                ++i;
+                continue;
+            }
+        }
+        c[w++] = c[i];
+    }
+    c.resize(w);
+    // 3. a PUSH without a load directly followed by a unary op that loads its
+    // operand: the PUSH carries the load and the op (its post-op)
+    w = 0;
+    for (size_t i = 0; i < c.size(); ++i) {
+        const int kind = (int)(c[i] & 0xFFu);
+        const int t = kind_block(kind), k = kind - kBlockBase[t];
+        if (k == KV_PUSH && ((c[i] >> 12) & 7u) == 0 && i + 1 < c.size()) {
+            const int kn = (int)(c[i + 1] & 0xFFu), tn = kind_block(kn);
+            const uint32_t an = c[i + 1] >> 8, src1 = (an >> 12) & 3u;
+            if (is_unary_kind(kn, tn) && src1 != 0) {
+                c[w++] = uop_word((uint32_t)kind, push_load_arg((c[i] >> 8) & 15u, (uint32_t)tn + 1u, src1 == 2 ? 1u : 0u,
+                                                               an & ((1u << kLdOffsetBits) - 1u),
+                                                               (uint32_t)post_op_of(kn, tn)));
                 ++i;
                 continue;
             }

@@ -6,10 +6,10 @@
 // evaluator.rs:228-388) for the programs the accumulator machine takes.
 // Per tile of 32*P points a warp runs
 //   forward  the accumulator form (acc_ops.cuh) with a load after a PUSH
-//            fused into the PUSH, every PUSH to its own stack slot, and
-//            TAPE micro-ops that store the
-//            forward values the reverse rules read into a per-warp tape in
-//            shared memory;
+//            fused into the PUSH and every PUSH to its own stack slot; the
+//            forward values the reverse rules read go to a per-warp tape in
+//            shared memory, stored by the op's own entry (before or after
+//            the op) or by a TAPE micro-op;
 //   seed     G_F = 2 (pred - y) on counted points (evaluator.rs:207);
 //   reverse  the reverse entries (uops.h, kAdjHeaderWords): each maps the
 //            adjoint accumulators G_t of the micro-op's output to those of
@@ -180,7 +180,7 @@ __device__ __forceinline__ void rev_op(Acc<PROF, P> &g, const RevIO<P> &io, uint
         } else if constexpr (k == KV_PUSH) {
             // a load fused into the PUSH ran after it: reverse it first
             const uint32_t lt = (arg >> 4) & 7u, slot = arg & 15u;
-            if (lt) rev_load_any<PROF, P>(g, io, lt - 1u, (arg >> 7) & 1u, arg >> 8);
+            if (lt) rev_load_any<PROF, P>(g, io, lt - 1u, (arg >> 7) & 1u, (arg >> 8) & ((1u << kLdOffsetBits) - 1u));
 #pragma unroll
             for (int c = 0; c < W; ++c) G[c] = G[c] + io.template GS<W>(t, slot, c);
         } else if constexpr (k >= KV_BIN && k < KV_BIN + 3 * nb) {
@@ -434,7 +434,17 @@ __device__ __forceinline__ void tape_store(Acc<PROF, P> &a, const RevIO<P> &io, 
     }
 }
 
-#define RSR_F(K) case (K): acc_op<PROF, P, (K)>(a, io, arg); break;
+// A forward entry: the op's type's accumulator stored to the tape before
+// and/or after the op (uops.h, kNoTape).
+template <int PROF, int P, int K>
+__device__ __forceinline__ void fwd_op(Acc<PROF, P> &a, const RevIO<P> &io, uint32_t arg, uint32_t tapes) {
+    constexpr int t = K >= K_M3 ? SM3 : K >= K_M2 ? SM2 : K >= K_V3 ? SV3 : K >= K_V2 ? SV2 : SF;
+    if ((tapes & kNoTape) != kNoTape) tape_store<PROF, P, t>(a, io, tapes & kNoTape);
+    acc_op<PROF, P, K>(a, io, arg);
+    if ((tapes >> 16) != kNoTape) tape_store<PROF, P, t>(a, io, tapes >> 16);
+}
+
+#define RSR_F(K) case (K): fwd_op<PROF, P, (K)>(a, io, arg, tapes); break;
 #define RSR_R(K) case (K): rev_op<PROF, P, (K)>(g, io, arg, w1); break;
 #define RSR_X4(M, K) M(K) M(K + 1) M(K + 2) M(K + 3)
 #define RSR_X9(M, K) RSR_X4(M, K) RSR_X4(M, K + 4) M(K + 8)
@@ -479,14 +489,17 @@ static_assert(kv_mulm(5, 3) == 29 && kv_make(5, 3) == 33, "Vec3 block: mat-vec k
     case kTapeKind[SM3]: tape_store<PROF, P, SM3>(a, io, arg); break;
 #define RSR_NONE
 
+// Forward entries are (word, tape stores); the next entry is read while the
+// current one runs.
 template <int PROF, int P, int OMIT>
-__device__ __forceinline__ void run_forward(Acc<PROF, P> &a, const RevIO<P> &io, const uint32_t *code, uint32_t len) {
-    uint32_t w = code[0];
-    for (uint32_t pc = 0; pc < len; ++pc) {
-        const uint32_t wn = code[pc + 1];
+__device__ __forceinline__ void run_forward(Acc<PROF, P> &a, const RevIO<P> &io, const uint32_t *code, uint32_t n) {
+    uint32_t w = code[0], tapes = code[1];
+    for (uint32_t pc = 0; pc < n; ++pc) {
+        const uint32_t wn = code[2 * pc + 2], tn = code[2 * pc + 3];
         const uint32_t arg = w >> 8, kind = w & 0xFFu;
         RSR_SWITCH(RSR_F, RSR_TAPES)
         w = wn;
+        tapes = tn;
     }
 }
 
@@ -579,7 +592,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
         const DatasetDesc ds = a.datasets[pd.dataset];
         io.stride = (uint32_t)ds.stride;
         const uint32_t n_fwd = scode[0], n_rev = scode[1];
-        const uint32_t *fwd = scode + kAdjHeaderWords, *rev = fwd + n_fwd;
+        const uint32_t *fwd = scode + kAdjHeaderWords, *rev = fwd + 2 * n_fwd;
         for (uint32_t tile = it.tile_begin + warp; tile < it.tile_end; tile += nw) {
             const uint64_t t0 = (uint64_t)tile * (32u * P);
             const uint64_t p0 = t0 + lane_point<P>(lane, 0);

@@ -268,14 +268,14 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             while (pc >= 0 && (size_t)adj_warp_floats(E.adj_tape, depth, 2 << pc, np) * 4u > kAdjWarpBudget) --pc;
             if (pc >= 0) {
                 const int bucket = (int)((adj_warp_floats(E.adj_tape, depth, 2 << pc, np) + 1023u) / 1024u);
-                // the handler sets the program does not use (forward words:
-                // the code after the two header words); a launch leaves out
+                // the handler sets the program does not use (forward entries:
+                // two words each after the header words); a launch leaves out
                 // those none of its programs uses
                 const uint32_t mv = (uint32_t)(K_V3 + kv_mulm(kBinOps[SV3], 3));
                 unsigned omit = adj_omittable(E.adj_profile);
                 const uint32_t n_fwd = E.adj_code.empty() ? 0u : E.adj_code[0];
                 for (uint32_t q = 0; q < n_fwd; ++q) {
-                    const uint32_t kind = E.adj_code[kAdjHeaderWords + q] & 0xFFu;
+                    const uint32_t kind = E.adj_code[kAdjHeaderWords + 2 * q] & 0xFFu;
                     if (kind >= (uint32_t)K_F_UN && kind < (uint32_t)K_F_END) omit &= ~1u;
                     if (kind >= mv + 1 && kind <= mv + 3) omit &= ~2u;
                 }
@@ -336,6 +336,10 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                     const uint32_t kind = w & 0xFFu;
                     if (kind >= (uint32_t)K_F_UN && kind < (uint32_t)K_F_END) omit &= ~1u;
                     if (kind >= mv + 1 && kind <= mv + 3) omit &= ~2u;
+                    // a PUSH carrying a unary Float op on a loaded value
+                    const int kt = kind_block_of((int)kind);
+                    if ((int)kind - kBlockBase[kt] == KV_PUSH && ((w >> 28) & 7u) != 0 && ((w >> 12) & 7u) == SF + 1u)
+                        omit &= ~1u;
                 }
                 path[i] = enc[i].profile + kRegPathStride * (cls + 3 * (int)omit);
             }

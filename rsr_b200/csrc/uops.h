@@ -86,6 +86,10 @@ static constexpr int kBinOps[5] = {6, 3, 5, 5, 5};
 // block's last kind; arg = first tape slot.  It stores the type's
 // accumulator to the tape, for the reverse rules that read forward values.
 static constexpr int kTapeKind[5] = {K_F + 27, K_V2 + 27, K_V3 + 34, K_M2 + 27, K_M3 + 27};
+// Value type of a micro-op kind's block.
+RSR_HD static constexpr int kind_block_of(int kind) {
+    return kind >= K_M3 ? SM3 : kind >= K_M2 ? SM2 : kind >= K_V3 ? SV3 : kind >= K_V2 ? SV2 : SF;
+}
 static constexpr int kBlockBase[5] = {K_F, K_V2, K_V3, K_M2, K_M3};
 // V-block offsets after the binary ops
 RSR_HD static constexpr int kv_scale(int nbin) { return KV_BIN + 3 * nbin; }       // 4 kinds: A X C S
@@ -102,11 +106,15 @@ RSR_HD static inline constexpr uint32_t uop_word(uint32_t kind, uint32_t arg) { 
 //               (0 none, 1 feature, 2 constant)
 //   PUSH arg:   bits 0-3 slot, bits 4-6 then load into accumulator type
 //               (0 none, 1 + type), bit 7 constant (else feature),
-//               bits 8-19 offset
+//               bits 8-19 offset, bits 20-22 then a unary op on the loaded
+//               value (register kernel only; 0 none, else 1 + its index
+//               in the type's block: F sin cos exp sqr sqrt ln; Vec norm,
+//               x, y, z; Mat det, trace, transpose, inverse)
 static constexpr uint32_t kLdOffsetBits = 12;
 RSR_HD static inline constexpr uint32_t unary_load_arg(uint32_t off, uint32_t src1) { return off | (src1 << 12); }
-RSR_HD static inline constexpr uint32_t push_load_arg(uint32_t slot, uint32_t type1, uint32_t is_const, uint32_t off) {
-    return slot | (type1 << 4) | (is_const << 7) | (off << 8);
+RSR_HD static inline constexpr uint32_t push_load_arg(uint32_t slot, uint32_t type1, uint32_t is_const, uint32_t off,
+                                                      uint32_t post = 0) {
+    return slot | (type1 << 4) | (is_const << 7) | (off << 8) | (post << 20);
 }
 
 // Tape value slot that stands for a feature column (adjoint kernel): the
@@ -127,21 +135,26 @@ static constexpr uint32_t kProfileTypes[N_PROFILES] = {
 static constexpr int kMaxAccStack = 16;   // shared-memory stack slots per type
 
 // Register adjoint code of a program (EncodedProgram::adj_code): word 0 the
-// forward length F, word 1 the reverse length R, then F forward micro-op
-// words (accumulator form, a load after a PUSH fused into the PUSH's word
-// but no load fused into a unary op, TAPE kinds between them,
-// every PUSH to its own stack slot so that spilled values survive the
-// forward sweep), then R reverse entries of two words each, in the order the
-// reverse sweep runs them: the forward word of the micro-op being reversed,
-// and its tape references (first | second << 16; which forward values they
-// hold depends on the kind, kernels_adj.cu).  A reference is a tape slot
-// (below kTapeRefC), or, where the forward value was a plain feature or
-// constant load not changed since, that feature (kTapeRefX | index) or
-// constant (kTapeRefC | index), which the reverse sweep reads again instead
-// of a tape slot; a value of width W reads W consecutive slots, features or
-// constants.
+// number F of forward entries, word 1 the number R of reverse entries, then
+// F forward entries of two words each -- the micro-op word (accumulator
+// form, a load after a PUSH fused into the PUSH's word but no load fused
+// into a unary op, every PUSH to its own stack slot so that spilled values
+// survive the forward sweep; TAPE kinds for the tape stores an op's entry
+// cannot carry) and its tape stores (kNoTape) -- then R reverse entries of
+// two words each, in the order the reverse sweep runs them: the forward word
+// of the micro-op being reversed, and its tape references (first | second
+// << 16; which forward values they hold depends on the kind,
+// kernels_adj.cu).  A reference is a tape slot (below kTapeRefC), or, where
+// the forward value was a plain feature or constant load not changed since,
+// that feature (kTapeRefX | index) or constant (kTapeRefC | index), which
+// the reverse sweep reads again instead of a tape slot; a value of width W
+// reads W consecutive slots, features or constants.
 static constexpr int kAdjHeaderWords = 2;
 static constexpr uint32_t kTapeRefX = 0x8000u, kTapeRefC = 0x4000u, kTapeRefIndex = 0x3FFFu;
+// Second word of a forward entry: the tape slot its op stores the op type's
+// accumulator to before running (low half) and after (high half), kNoTape
+// for none.
+static constexpr uint32_t kNoTape = 0xFFFFu, kNoTapes = 0xFFFFFFFFu;
 
 // Program descriptor for the kernels (one per program in a launch).
 struct ProgDesc {

@@ -132,8 +132,10 @@ def run(program, ds, alias_stacks=True):
     depth = [int(x) for x in enc[2:7]]
     code = enc[7:]
     n_fwd, n_rev = int(code[0]), int(code[1])
-    fwd = [int(w) for w in code[2:2 + n_fwd]]
-    rev = [(int(code[2 + n_fwd + 2 * i]), int(code[3 + n_fwd + 2 * i])) for i in range(n_rev)]
+    # forward entries: (micro-op word, tape stores before | after << 16)
+    fwd = [(int(code[2 + 2 * i]), int(code[3 + 2 * i])) for i in range(n_fwd)]
+    r0 = 2 + 2 * n_fwd
+    rev = [(int(code[r0 + 2 * i]), int(code[r0 + 1 + 2 * i])) for i in range(n_rev)]
     npts = ds.num_batches * 8
     ff = np.asarray(ds.feature_flat, f32).reshape(ds.num_batches, ds.num_features, 8)
     X = [ff[:, f, :].reshape(-1) for f in range(ds.num_features)]
@@ -152,14 +154,7 @@ def run(program, ds, alias_stacks=True):
             return [C(arg + c) for c in range(w)]
         return list(S[t][arg])
 
-    for word in fwd:
-        kind, arg = word & 0xFF, word >> 8
-        t = block(kind)
-        k, W, nb = kind - BASE[t], WIDTH[t], NBIN[t]
-        if kind == TAPE[t]:
-            for c in range(W):
-                tape[arg + c] = A[t][c]
-            continue
+    def forward_op(kind, arg, t, k, W, nb):
         if k == 0:
             A[t] = [X[arg + c] for c in range(W)]
         elif k == 1:
@@ -232,6 +227,23 @@ def run(program, ds, alias_stacks=True):
             elif k == 26:
                 cols = [S[tv][arg + c] for c in range(n - 1)] + [A[tv]]
                 A[t] = [cols[c][r] for c in range(n) for r in range(n)]
+
+    for word, tapes in fwd:
+        kind, arg = word & 0xFF, word >> 8
+        t = block(kind)
+        k, W, nb = kind - BASE[t], WIDTH[t], NBIN[t]
+        if kind == TAPE[t]:
+            for c in range(W):
+                tape[arg + c] = A[t][c]
+            continue
+        if tapes & 0xFFFF != 0xFFFF:   # the op's type's accumulator, stored before the op
+            for c in range(W):
+                tape[(tapes & 0xFFFF) + c] = A[t][c]
+        forward_op(kind, arg, t, k, W, nb)
+        if tapes >> 16 != 0xFFFF:      # and after it
+            for c in range(W):
+                tape[(tapes >> 16) + c] = A[t][c]
+
     pred = A[SF][0]
     valid = np.arange(npts) < ds.num_batches * 8
     diff = pred - y

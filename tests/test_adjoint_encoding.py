@@ -80,7 +80,7 @@ def test_adjoint_stacks_can_share_the_forward_slots():
 
 
 def test_register_adjoint_code_layout():
-    """Header words, one reverse entry per non-TAPE forward micro-op, PUSH
+    """Header words, one reverse entry per non-TAPE forward entry, PUSH
     slots all distinct, tape slots inside the reported tape."""
     for p in W.lorentz_population(30, seed=11) + W.inverse_population(30, seed=12):
         enc = E.encoding(p, 9, 5)
@@ -88,14 +88,20 @@ def test_register_adjoint_code_layout():
             continue
         tape, depth, code = int(enc[1]), [int(x) for x in enc[2:7]], enc[7:]
         nf, nr = int(code[0]), int(code[1])
-        assert len(code) == 2 + nf + 2 * nr
-        fwd = [int(w) for w in code[2:2 + nf]]
+        assert len(code) == 2 + 2 * nf + 2 * nr
+        fwd = [int(w) for w in code[2:2 + 2 * nf:2]]
+        stores = [int(w) for w in code[3:3 + 2 * nf:2]]
         tapes = [w for w in fwd if (w & 255) in accvm.TAPE]
         assert nr == nf - len(tapes)
         assert all((w >> 8) < tape for w in tapes)
+        # stores an entry carries: tape slots inside the tape, none on TAPE entries
+        for w, st in zip(fwd, stores):
+            for s in (st & 0xFFFF, st >> 16):
+                assert s == 0xFFFF or (s < tape and (w & 255) not in accvm.TAPE)
         # reverse references: tape slots inside the tape, or features /
         # constants (values the reverse sweep reads again instead of a tape)
-        refs = [r for i in range(nr) for r in (int(code[3 + nf + 2 * i]) & 0xFFFF, int(code[3 + nf + 2 * i]) >> 16)]
+        r0 = 2 + 2 * nf
+        refs = [r for i in range(nr) for r in (int(code[r0 + 1 + 2 * i]) & 0xFFFF, int(code[r0 + 1 + 2 * i]) >> 16)]
         assert all(r < tape or r & 0xC000 for r in refs if r)
         pushes = {}
         for w in fwd:
