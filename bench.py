@@ -282,7 +282,11 @@ def serving_light_bench(eng, jobs: int = 300, rate: float = 150.0, threads: int 
     MSE-only jobs of 64-1024 vector-workload programs (100k points) with
     Poisson arrivals at `rate` jobs/s in total, a load the device keeps up
     with, so latency is the jobs' own service time rather than queueing.
-    The server is warmed up with 16 jobs before the statistics start."""
+    The server is warmed up before the statistics start: 8 jobs of 1024
+    programs submitted 0.3 ms apart, so that each slot takes one while the
+    others are busy and grows its buffers to the largest job (a slot
+    allocates on its first job of a new size), then 16 of the stream's own
+    jobs."""
     from rsr_b200 import isa as I
     from rsr_b200 import workloads as W
     from rsr_b200.serving import Server
@@ -297,7 +301,15 @@ def serving_light_bench(eng, jobs: int = 300, rate: float = 150.0, threads: int 
     gaps = rng.exponential(threads / rate, jobs)
     srv = Server(eng, slots=4)
     # warm-up outside the statistics: a new server's slots allocate their
-    # device buffers and start their encoding threads on their first jobs
+    # device and pinned buffers and start their encoding threads on their
+    # first jobs, so every slot is given the largest job at least once
+    big = I.pack(progs)
+    warm = []
+    for _ in range(8):
+        warm.append(srv.submit(big, d, kind="mse"))
+        time.sleep(0.0003)
+    for t in warm:
+        srv.wait(t)
     for pk in plan[:16]:
         srv.wait(srv.submit(pk, d, kind="mse"))
     srv.stats(reset=True)

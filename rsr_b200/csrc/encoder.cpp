@@ -822,9 +822,8 @@ class AdjEmitter {
 };
 
 // Peephole passes over the accumulator form: a load directly followed by a
-// unary op on the loaded value becomes the op's operand load; a PUSH
-// directly followed by a load carries the load; a PUSH directly followed by
-// a unary op that loads its operand carries both (the op as its post-op).
+// unary op on the loaded value becomes the op's operand load, and a PUSH
+// directly followed by a load carries the load.
 int kind_block(int kind) { return kind >= K_M3 ? SM3 : kind >= K_M2 ? SM2 : kind >= K_V3 ? SV3 : kind >= K_V2 ? SV2 : SF; }
 
 int post_op_of(int kind, int t) {
@@ -873,26 +872,6 @@ void fuse_loads(std::vector<uint32_t> *code) {
             if ((kk == KV_LDX || kk == KV_LDC) && (c[i + 1] >> 8) < (1u << kLdOffsetBits)) {
                 c[w++] = uop_word((uint32_t)kind, push_load_arg(c[i] >> 8, (uint32_t)tn + 1u, kk == KV_LDC ? 1u : 0u,
                                                                c[i + 1] >> 8));
-                ++i;
-                continue;
-            }
-        }
-        c[w++] = c[i];
-    }
-    c.resize(w);
-    // 3. a PUSH without a load directly followed by a unary op that loads its
-    // operand: the PUSH carries the load and the op (its post-op)
-    w = 0;
-    for (size_t i = 0; i < c.size(); ++i) {
-        const int kind = (int)(c[i] & 0xFFu);
-        const int t = kind_block(kind), k = kind - kBlockBase[t];
-        if (k == KV_PUSH && ((c[i] >> 12) & 7u) == 0 && i + 1 < c.size()) {
-            const int kn = (int)(c[i + 1] & 0xFFu), tn = kind_block(kn);
-            const uint32_t an = c[i + 1] >> 8, src1 = (an >> 12) & 3u;
-            if (is_unary_kind(kn, tn) && src1 != 0) {
-                c[w++] = uop_word((uint32_t)kind, push_load_arg((c[i] >> 8) & 15u, (uint32_t)tn + 1u, src1 == 2 ? 1u : 0u,
-                                                               an & ((1u << kLdOffsetBits) - 1u),
-                                                               (uint32_t)post_op_of(kn, tn)));
                 ++i;
                 continue;
             }

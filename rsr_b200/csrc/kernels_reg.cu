@@ -20,49 +20,7 @@
 
 namespace rsr {
 
-// A PUSH may carry a load and a unary op on the loaded value (uops.h,
-// push_load_arg post-op): that op, of the loaded type t, on its accumulator.
-template <int PROF, int P, int OMIT>
-__device__ __forceinline__ void post_op(Acc<PROF, P> &a, const AccIO<P> &io, uint32_t t, uint32_t post) {
-    constexpr bool NU = (OMIT & 1) != 0;
-    switch (t * 8u + post) {
-        case SF * 8 + 1: if constexpr (!NU) acc_op<PROF, P, K_F_UN + 0>(a, io, 0u); break;
-        case SF * 8 + 2: if constexpr (!NU) acc_op<PROF, P, K_F_UN + 1>(a, io, 0u); break;
-        case SF * 8 + 3: if constexpr (!NU) acc_op<PROF, P, K_F_UN + 2>(a, io, 0u); break;
-        case SF * 8 + 4: if constexpr (!NU) acc_op<PROF, P, K_F_UN + 3>(a, io, 0u); break;
-        case SF * 8 + 5: if constexpr (!NU) acc_op<PROF, P, K_F_UN + 4>(a, io, 0u); break;
-        case SF * 8 + 6: if constexpr (!NU) acc_op<PROF, P, K_F_UN + 5>(a, io, 0u); break;
-        case SV2 * 8 + 1: acc_op<PROF, P, K_V2 + kv_norm(kBinOps[SV2]) + 0>(a, io, 0u); break;
-        case SV2 * 8 + 2: acc_op<PROF, P, K_V2 + kv_norm(kBinOps[SV2]) + 1>(a, io, 0u); break;
-        case SV2 * 8 + 3: acc_op<PROF, P, K_V2 + kv_norm(kBinOps[SV2]) + 2>(a, io, 0u); break;
-        case SV3 * 8 + 1: acc_op<PROF, P, K_V3 + kv_norm(kBinOps[SV3]) + 0>(a, io, 0u); break;
-        case SV3 * 8 + 2: acc_op<PROF, P, K_V3 + kv_norm(kBinOps[SV3]) + 1>(a, io, 0u); break;
-        case SV3 * 8 + 3: acc_op<PROF, P, K_V3 + kv_norm(kBinOps[SV3]) + 2>(a, io, 0u); break;
-        case SV3 * 8 + 4: acc_op<PROF, P, K_V3 + kv_norm(kBinOps[SV3]) + 3>(a, io, 0u); break;
-        case SM2 * 8 + 1: acc_op<PROF, P, K_M2 + KM_DET>(a, io, 0u); break;
-        case SM2 * 8 + 2: acc_op<PROF, P, K_M2 + KM_TRACE>(a, io, 0u); break;
-        case SM2 * 8 + 3: acc_op<PROF, P, K_M2 + KM_TRANSPOSE>(a, io, 0u); break;
-        case SM2 * 8 + 4: acc_op<PROF, P, K_M2 + KM_INVERSE>(a, io, 0u); break;
-        case SM3 * 8 + 1: acc_op<PROF, P, K_M3 + KM_DET>(a, io, 0u); break;
-        case SM3 * 8 + 2: acc_op<PROF, P, K_M3 + KM_TRACE>(a, io, 0u); break;
-        case SM3 * 8 + 3: acc_op<PROF, P, K_M3 + KM_TRANSPOSE>(a, io, 0u); break;
-        case SM3 * 8 + 4: acc_op<PROF, P, K_M3 + KM_INVERSE>(a, io, 0u); break;
-        default: break;
-    }
-}
-
-// One micro-op: the accumulator op, and a PUSH's post-op.
-template <int PROF, int P, int OMIT, int K>
-__device__ __forceinline__ void reg_op(Acc<PROF, P> &a, const AccIO<P> &io, uint32_t arg) {
-    acc_op<PROF, P, K>(a, io, arg);
-    constexpr int t = K >= K_M3 ? SM3 : K >= K_M2 ? SM2 : K >= K_V3 ? SV3 : K >= K_V2 ? SV2 : SF;
-    if constexpr (K - kBlockBase[t] == KV_PUSH && ((kProfileTypes[PROF] >> t) & 1u) != 0u) {
-        const uint32_t post = (arg >> 20) & 7u;
-        if (post) post_op<PROF, P, OMIT>(a, io, ((arg >> 4) & 7u) - 1u, post);
-    }
-}
-
-#define RSR_C(K) case (K): reg_op<PROF, P, OMIT, (K)>(a, io, arg); break;
+#define RSR_C(K) case (K): acc_op<PROF, P, (K)>(a, io, arg); break;
 #define RSR_C4(K) RSR_C(K) RSR_C(K + 1) RSR_C(K + 2) RSR_C(K + 3)
 #define RSR_C9(K) RSR_C4(K) RSR_C4(K + 4) RSR_C(K + 8)
 #define RSR_C27(K) RSR_C9(K) RSR_C9(K + 9) RSR_C9(K + 18)

@@ -336,10 +336,6 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                     const uint32_t kind = w & 0xFFu;
                     if (kind >= (uint32_t)K_F_UN && kind < (uint32_t)K_F_END) omit &= ~1u;
                     if (kind >= mv + 1 && kind <= mv + 3) omit &= ~2u;
-                    // a PUSH carrying a unary Float op on a loaded value
-                    const int kt = kind_block_of((int)kind);
-                    if ((int)kind - kBlockBase[kt] == KV_PUSH && ((w >> 28) & 7u) != 0 && ((w >> 12) & 7u) == SF + 1u)
-                        omit &= ~1u;
                 }
                 path[i] = enc[i].profile + kRegPathStride * (cls + 3 * (int)omit);
             }

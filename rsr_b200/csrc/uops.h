@@ -86,10 +86,6 @@ static constexpr int kBinOps[5] = {6, 3, 5, 5, 5};
 // block's last kind; arg = first tape slot.  It stores the type's
 // accumulator to the tape, for the reverse rules that read forward values.
 static constexpr int kTapeKind[5] = {K_F + 27, K_V2 + 27, K_V3 + 34, K_M2 + 27, K_M3 + 27};
-// Value type of a micro-op kind's block.
-RSR_HD static constexpr int kind_block_of(int kind) {
-    return kind >= K_M3 ? SM3 : kind >= K_M2 ? SM2 : kind >= K_V3 ? SV3 : kind >= K_V2 ? SV2 : SF;
-}
 static constexpr int kBlockBase[5] = {K_F, K_V2, K_V3, K_M2, K_M3};
 // V-block offsets after the binary ops
 RSR_HD static constexpr int kv_scale(int nbin) { return KV_BIN + 3 * nbin; }       // 4 kinds: A X C S
@@ -106,15 +102,11 @@ RSR_HD static inline constexpr uint32_t uop_word(uint32_t kind, uint32_t arg) { 
 //               (0 none, 1 feature, 2 constant)
 //   PUSH arg:   bits 0-3 slot, bits 4-6 then load into accumulator type
 //               (0 none, 1 + type), bit 7 constant (else feature),
-//               bits 8-19 offset, bits 20-22 then a unary op on the loaded
-//               value (register kernel only; 0 none, else 1 + its index
-//               in the type's block: F sin cos exp sqr sqrt ln; Vec norm,
-//               x, y, z; Mat det, trace, transpose, inverse)
+//               bits 8-19 offset
 static constexpr uint32_t kLdOffsetBits = 12;
 RSR_HD static inline constexpr uint32_t unary_load_arg(uint32_t off, uint32_t src1) { return off | (src1 << 12); }
-RSR_HD static inline constexpr uint32_t push_load_arg(uint32_t slot, uint32_t type1, uint32_t is_const, uint32_t off,
-                                                      uint32_t post = 0) {
-    return slot | (type1 << 4) | (is_const << 7) | (off << 8) | (post << 20);
+RSR_HD static inline constexpr uint32_t push_load_arg(uint32_t slot, uint32_t type1, uint32_t is_const, uint32_t off) {
+    return slot | (type1 << 4) | (is_const << 7) | (off << 8);
 }
 
 // Tape value slot that stands for a feature column (adjoint kernel): the

@@ -123,19 +123,35 @@ def transpose(m, n):
     return [m[n * (i % n) + i // n] for i in range(n * n)]
 
 
-def run(program, ds, alias_stacks=True):
+def _is_unary(t, k):
+    if t == SF:
+        return 21 <= k < 27
+    if t in (SV2, SV3):
+        return kv_norm(NBIN[t]) <= k <= kv_norm(NBIN[t]) + WIDTH[t]
+    return 22 <= k <= 25
+
+
+def run(program, ds, alias_stacks=True, form=5):
     """Gradient of the MSE w.r.t. the first min(32, P) flat parameters and
-    the MSE, by the register adjoint's code; (mse, grad[32])."""
-    enc = E.encoding(program, ds.num_features, 5)
-    if enc[0] == 0xFFFFFFFF:
-        raise ValueError("no register adjoint form")
-    depth = [int(x) for x in enc[2:7]]
-    code = enc[7:]
-    n_fwd, n_rev = int(code[0]), int(code[1])
-    # forward entries: (micro-op word, tape stores before | after << 16)
-    fwd = [(int(code[2 + 2 * i]), int(code[3 + 2 * i])) for i in range(n_fwd)]
-    r0 = 2 + 2 * n_fwd
-    rev = [(int(code[r0 + 2 * i]), int(code[r0 + 1 + 2 * i])) for i in range(n_rev)]
+    the MSE, by the register adjoint's code; (mse, grad[32]).  form=1 runs
+    the register kernel's accumulator form instead (fused loads,
+    no tape, no reverse sweep) and returns the MSE alone."""
+    if form == 1:
+        words = E.encoding(program, ds.num_features, 1)
+        if len(words) == 0:
+            raise ValueError("no accumulator form")
+        fwd = [(int(w), 0xFFFFFFFF) for w in words]
+        rev = []
+    else:
+        enc = E.encoding(program, ds.num_features, 5)
+        if enc[0] == 0xFFFFFFFF:
+            raise ValueError("no register adjoint form")
+        code = enc[7:]
+        n_fwd, n_rev = int(code[0]), int(code[1])
+        # forward entries: (micro-op word, tape stores before | after << 16)
+        fwd = [(int(code[2 + 2 * i]), int(code[3 + 2 * i])) for i in range(n_fwd)]
+        r0 = 2 + 2 * n_fwd
+        rev = [(int(code[r0 + 2 * i]), int(code[r0 + 1 + 2 * i])) for i in range(n_rev)]
     npts = ds.num_batches * 8
     ff = np.asarray(ds.feature_flat, f32).reshape(ds.num_batches, ds.num_features, 8)
     X = [ff[:, f, :].reshape(-1) for f in range(ds.num_features)]
@@ -144,7 +160,7 @@ def run(program, ds, alias_stacks=True):
     C = lambda i: np.full(npts, consts[i], f32)
     zero = np.zeros(npts, f32)
     A = [[zero] * WIDTH[t] for t in range(5)]
-    S = [[None] * max(depth[t], 1) for t in range(5)]
+    S = [dict() for _ in range(5)]
     tape = {}
 
     def fetch(t, src, arg, w):
@@ -155,6 +171,9 @@ def run(program, ds, alias_stacks=True):
         return list(S[t][arg])
 
     def forward_op(kind, arg, t, k, W, nb):
+        if _is_unary(t, k) and (arg >> 12) & 3:  # the operand's load, fused into the op (accumulator form)
+            src1, off = (arg >> 12) & 3, arg & 0xFFF
+            A[t] = [X[off + c] if src1 == 1 else C(off + c) for c in range(W)]
         if k == 0:
             A[t] = [X[arg + c] for c in range(W)]
         elif k == 1:
@@ -163,8 +182,9 @@ def run(program, ds, alias_stacks=True):
             S[t][arg & 15] = list(A[t])
             lt = (arg >> 4) & 7   # a load fused into the PUSH (uops.h push_load_arg)
             if lt:
-                off, W2 = arg >> 8, WIDTH[lt - 1]
+                off, W2 = (arg >> 8) & 0xFFF, WIDTH[lt - 1]
                 A[lt - 1] = [C(off + c) if (arg >> 7) & 1 else X[off + c] for c in range(W2)]
+
         elif k < 3 + 3 * nb:
             j, src = (k - 3) // 3, (k - 3) % 3
             B = fetch(t, src, arg, W)
@@ -248,13 +268,15 @@ def run(program, ds, alias_stacks=True):
     valid = np.arange(npts) < ds.num_batches * 8
     diff = pred - y
     sse = float(np.sum(diff.astype(np.float64) ** 2))
+    if form == 1:
+        return sse / ds.num_samples
     # reverse sweep
     G = [[zero] * WIDTH[t] for t in range(5)]
     G[SF] = [(f32(2) * diff).astype(f32)]
     # a spilled value's adjoint takes its forward slot: the one micro-op that
     # pops the value reads it (in both sweeps) before its reverse writes the
     # adjoint, and nothing reads the slot's forward value after that
-    GS = S if alias_stacks else [[None] * max(depth[t], 1) for t in range(5)]
+    GS = S if alias_stacks else [dict() for _ in range(5)]
     grad = np.zeros(32)
     def T(ref, w):  # a tape slot, or a feature / constant reference (uops.h kTapeRefX, kTapeRefC)
         if ref & 0x8000:

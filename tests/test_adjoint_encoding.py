@@ -57,6 +57,36 @@ def test_register_adjoint_code_gives_the_dual_gradients():
     assert all(checked[name] >= 10 for name, _, _ in CASES) and checked.get("inverse", 0) >= 3, checked
 
 
+def test_accumulator_form_mse_matches_the_oracle():
+    """The register kernel's code (accumulator form, form 1): loads fused
+    into unary ops and PUSHes.  Emulated on the CPU, every program's MSE
+    agrees with the FP64 oracle, and the fused forms occur."""
+    unary = fused = 0
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        for name, dsf, popf in CASES:
+            ds, pop = dsf(), popf()
+            n = 0
+            for p in pop:
+                words = E.encoding(p, ds.num_features, 1)
+                if len(words) == 0:
+                    continue
+                for w in (int(x) for x in words):
+                    t = accvm.block(w & 255)
+                    if (w & 255) - accvm.BASE[t] == 2:
+                        fused += ((w >> 12) & 7) != 0
+                    elif accvm._is_unary(t, (w & 255) - accvm.BASE[t]):
+                        unary += ((w >> 20) & 3) != 0
+                m = accvm.run(p, ds, form=1)
+                m64 = O.mse_f64(p, ds)
+                if not (np.isfinite(m64) and m64 < 1e30):
+                    continue
+                assert abs(m - m64) <= 1e-5 * max(abs(m64), 1e-6), (name, m, m64)
+                n += 1
+            assert n >= 10, name
+    assert unary > 0 and fused > 0, (unary, fused)
+
+
 def test_adjoint_stacks_can_share_the_forward_slots():
     """The kernel keeps a spilled value's adjoint in the value's own stack
     slot.  That is sound when the one micro-op that pops a value is the last
