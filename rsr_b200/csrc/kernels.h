@@ -11,7 +11,6 @@ namespace rsr {
 constexpr int kPlainThreads = 128;  // 4 warps per block, one work item per warp
 constexpr int kRegThreads = 256;  // 8 warps share one work item
 constexpr int kGradThreads = 32;  // one warp per block, one item per warp
-constexpr int kAdjThreads = 128;  // register adjoint: 4 warps share one work item
 
 cudaError_t launch_plain(const LaunchArgs &a, int P, uint32_t warps_per_block, size_t smem, cudaStream_t st);
 size_t plain_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t slots, int P);
@@ -52,19 +51,22 @@ int reg_max_blocks_per_sm(int profile, int P, unsigned omit, size_t smem);
 // P (points per lane) 2, 4, or 8 up to adj_max_p(profile)
 bool adj_supported(int profile);
 int adj_max_p(int profile);
-// floats of a warp's region for a program (tape | stacks, shared by the
-// adjoint stacks | gradient sums | Kahan state), and its stack depths packed
-// for ProgDesc
-uint32_t adj_warp_floats(uint32_t tape_slots, const uint32_t *stack_depth, int P, uint32_t n_params);
+// floats of a warp's shared-memory region for a program (stacks, shared by
+// the adjoint stacks | gradient sums | Kahan state), and its stack depths
+// packed for ProgDesc
+uint32_t adj_warp_floats(const uint32_t *stack_depth, int P, uint32_t n_params);
 uint32_t adj_pack_depth(const uint32_t *stack_depth);
-void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, LaunchArgs *a);
-size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats);
+// shared-memory layout of a block of nw warps; the tensor-memory columns
+// of each warp's tape (512 / (nw / 4)) go to a->tmem_cols
+void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, int nw, LaunchArgs *a);
+size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, int nw);
+// warps of a block of instance (profile, P), one block per SM (a multiple of 4)
+int adj_block_warps(int profile, int P);
 // Handler sets an instance may leave out (bit 0: unary Float ops; bit 1,
 // F+V3: mat-vec with a leaf or spilled matrix), as for the register kernel.
 unsigned adj_omittable(int profile);
 cudaError_t launch_adj(const LaunchArgs &a, int profile, int P, unsigned omit, uint32_t grid, size_t smem,
                        cudaStream_t st);
-int adj_max_blocks_per_sm(int profile, int P, unsigned omit, size_t smem);
 
 // adjoint kernel (kernels_grad.cu)
 cudaError_t launch_grad(const LaunchArgs &a, int profile, bool no_unary, uint32_t warps_per_block, size_t smem,

@@ -35,15 +35,79 @@ namespace rsr {
 
 constexpr uint32_t kAdjParams = 32;
 
+// ------------------------------------------------ tensor memory (the tape)
+// The tape lives in tensor memory: one block per SM allocates all 512
+// columns of its SM's 128 lanes; warp w owns lanes 32 (w % 4) .. +31, one
+// lane per thread, and the (w / 4)-th run of a.tmem_cols columns (512 /
+// (warps / 4)); a tape slot is P consecutive columns of the thread's lane.
+// Stores are asynchronous (waited for before the reverse sweep reads),
+// loads are waited for at once.  The launch pads each block's shared memory
+// to more than half an SM's (enqueue_plan), so no two blocks that allocate
+// share an SM and the allocation never waits.
+__device__ __forceinline__ void tm_alloc(uint32_t *dst_smem, uint32_t ncols) {
+    const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(dst_smem));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(ncols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tm_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tm_fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tm_fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tm_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+template <int P>
+__device__ __forceinline__ void tm_st(uint32_t addr, const Vf<P> &v) {
+    if constexpr (P == 2) {
+        asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(addr), "r"(__float_as_uint(v.v[0])),
+                     "r"(__float_as_uint(v.v[1])) : "memory");
+    } else if constexpr (P == 4) {
+        asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr),
+                     "r"(__float_as_uint(v.v[0])), "r"(__float_as_uint(v.v[1])), "r"(__float_as_uint(v.v[2])),
+                     "r"(__float_as_uint(v.v[3])) : "memory");
+    } else {
+        static_assert(P == 8, "tape slots of 2, 4 or 8 columns");
+        asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(addr),
+                     "r"(__float_as_uint(v.v[0])), "r"(__float_as_uint(v.v[1])), "r"(__float_as_uint(v.v[2])),
+                     "r"(__float_as_uint(v.v[3])), "r"(__float_as_uint(v.v[4])), "r"(__float_as_uint(v.v[5])),
+                     "r"(__float_as_uint(v.v[6])), "r"(__float_as_uint(v.v[7])) : "memory");
+    }
+}
+
+// The wait names the loaded registers, so no use of them is scheduled
+// before it.
+template <int P>
+__device__ __forceinline__ Vf<P> tm_ld(uint32_t addr) {
+    uint32_t r[P];
+    if constexpr (P == 2) {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(addr) : "memory");
+        asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r[0]), "+r"(r[1])::"memory");
+    } else if constexpr (P == 4) {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(addr) : "memory");
+        asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3])::"memory");
+    } else {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                     : "r"(addr) : "memory");
+        asm volatile("tcgen05.wait::ld.sync.aligned;"
+                     : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7])::"memory");
+    }
+    Vf<P> v;
+#pragma unroll
+    for (int j = 0; j < P; ++j) v.v[j] = __uint_as_float(r[j]);
+    return v;
+}
+
 // Reverse-sweep access: the forward machine's operand fetches (features,
 // constants, forward stack values), the adjoint stacks, the tape and the
 // lane's gradient sums.
 template <int P>
 struct RevIO : AccIO<P> {
-    // adjoint stacks and tape in the interleaved lane layout (blocks of 32*P
-    // floats), at this lane's first value
+    // adjoint stacks in the interleaved lane layout (blocks of 32*P floats),
+    // at this lane's first value
     float *gstk[N_STACKS];  // adjoint stacks, block (slot*W + c)
-    float *tape;            // tape, block slot
+    uint32_t tm;            // tensor-memory tape: this warp's lanes, column 0
     float *gacc;            // this lane's f32 gradient sums: gacc[k*32]
     uint32_t valid;         // bit q: value q of the lane is a counted point
     // a tape reference (uops.h, kTapeRefX): a tape slot, or the feature or
@@ -51,10 +115,10 @@ struct RevIO : AccIO<P> {
     __device__ __forceinline__ Vf<P> T(uint32_t ref) const {
         if (ref & kTapeRefX) return this->X(ref & kTapeRefIndex);
         if (ref & kTapeRefC) return this->C(ref & kTapeRefIndex);
-        return lds_lane<P>(tape + ref * 32u * P);
+        return tm_ld<P>(tm + ref * (uint32_t)P);
     }
     __device__ __forceinline__ void put_tape(uint32_t slot, const Vf<P> &v) const {
-        sts_lane<P>(tape + slot * 32u * P, v);
+        tm_st<P>(tm + slot * (uint32_t)P, v);
     }
     template <int W>
     __device__ __forceinline__ Vf<P> GS(int t, uint32_t slot, int c) const {
@@ -531,24 +595,45 @@ __device__ __forceinline__ void run_reverse(Acc<PROF, P> &g, const RevIO<P> &io,
 #undef RSR_R
 #undef RSR_F
 
-// Block-cooperative persistent kernel: a block's warps take the tiles of one
-// work item (one program on a chunk of points).  Shared memory: block
-// header (code | constants | meta | cross-warp sums), then one region per
-// warp: tape | stacks (then adjoint stacks) | gradient sums | Kahan state.
+// Block-cooperative persistent kernel, one block per SM: its warps take the
+// tiles of one work item (one program on a chunk of points).  Shared
+// memory: block header (code | constants | meta | cross-warp sums), then
+// one region per warp: stacks (then adjoint stacks) | gradient sums | Kahan
+// state.  The tape is in tensor memory, a.tmem_cols columns per warp.
+// Warps of a block of instance (PROF, P), one block per SM: a multiple of
+// 4, at most 16.  More warps than the instance's registers allow unspilled
+// pay: the extra warps hide more of the dispatch latency than the spill
+// costs.  F+V3 at 8 points per lane: 168 registers at 12 warps, 128 with
+// ~250 bytes of spill at 16 (vector workload gradient 17.7 ms against 22.4
+// ms); F+V2+M2 and F+V3+M3 at 4 points likewise at 16 and 12 warps (matrix
+// workload 17.0 against 18.7 ms).
+template <int PROF, int P>
+__host__ __device__ constexpr int adj_warps() {
+    if constexpr (PROF == P_FV3M3) return P >= 4 ? 12 : 16;
+    else return 16;
+}
+
 template <int PROF, int P, int OMIT>
-__global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchArgs a) {
+__global__ void __launch_bounds__(adj_warps<PROF, P>() * 32, 1) adj_eval_kernel(const LaunchArgs a) {
     extern __shared__ __align__(16) float smem[];
     if (a.run_if && *a.run_if == 0u) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nw = blockDim.x >> 5;
     uint32_t *scode = reinterpret_cast<uint32_t *>(smem);
     float *sconst = smem + ((a.smem_code_words + 2u + 3u) & ~3u);  // code and its two pad words
-    uint32_t *meta = reinterpret_cast<uint32_t *>(sconst + ((a.smem_const_floats + 3u) & ~3u));  // [0] item
+    uint32_t *meta = reinterpret_cast<uint32_t *>(sconst + ((a.smem_const_floats + 3u) & ~3u));  // [0] item, [1] tape
     double *red = reinterpret_cast<double *>(meta + 4);  // [warp][1 + kAdjParams]
     float *wbase = smem + a.block_hdr_floats + (size_t)warp * a.region_floats;
 
+    // the block takes all of the SM's tensor memory; warp w owns lanes
+    // 32 (w % 4) .. +31 (its quadrant) and the (w / 4)-th share of columns
+    if (warp == 0) tm_alloc(&meta[1], 512u);
+    tm_fence_before_sync();
+    __syncthreads();
+    tm_fence_after_sync();
     RevIO<P> io;
     io.consts = sconst;
+    io.tm = meta[1] + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(warp >> 2) * a.tmem_cols;
 
     for (;;) {
         if (threadIdx.x == 0) meta[0] = atomicAdd(a.item_counter, 1u);
@@ -561,13 +646,12 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
             continue;
         }
         const ProgDesc pd = a.progs[it.prog_begin];
-        // this program's warp region: tape | stacks | sums
-        // (n_slots: tape slots; n_tape: stack depths, 5 bits per type); the
-        // launch's region_floats is the largest of its programs'
+        // this program's warp region: stacks | sums (n_tape: stack depths,
+        // 5 bits per type); the launch's region_floats is the largest of its
+        // programs'
         {
             const uint32_t l0 = lane_point<P>(lane, 0);
-            uint32_t off = pd.n_slots * 32u * P;
-            io.tape = wbase + l0;
+            uint32_t off = 0;
             // A spilled value's adjoint takes the value's own slot: the one
             // micro-op that pops the value reads it into registers (in both
             // sweeps) before its reverse writes the adjoint, and no later
@@ -603,6 +687,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
             io.valid = valid;
             Acc<PROF, P> acc;
             run_forward<PROF, P, OMIT>(acc, io, fwd, n_fwd);
+            tm_wait_st();  // the tape stores land before the reverse sweep reads them
             const Vf<P> y = load_lane<P>(ds.y + p0);
             Acc<PROF, P> g;
             g.F[0] = splat<P>(0.0f);
@@ -644,17 +729,22 @@ __global__ void __launch_bounds__(kAdjThreads, 2) adj_eval_kernel(const LaunchAr
         }
         __syncthreads();
     }
+    // every thread left the loop together (after the item fetch's barrier)
+    tm_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tm_dealloc(meta[1], 512u);
 }
 
 // ------------------------------------------------------------- launchers
 // Shared-memory layout (floats).  Block header: code (+2 pads) | constants |
-// meta (4 words) | cross-warp sums (warps x 33 doubles).  Per warp: tape |
-// stacks (per type; the reverse sweep's adjoint stacks in the same slots) |
+// meta (4 words) | cross-warp sums (warps x 33 doubles).  Per warp: stacks
+// (per type; the reverse sweep's adjoint stacks in the same slots) |
 // gradient sums (one row of 32 per parameter, at most 32) | Kahan state (2 x
 // 32), each program's own sizes (the kernel lays the region out per item);
-// warp_floats is the largest region of the launch.
-uint32_t adj_warp_floats(uint32_t tape_slots, const uint32_t *stack_depth, int P, uint32_t n_params) {
-    uint32_t slots = tape_slots;  // + the stacks, whose slots the adjoints reuse
+// warp_floats is the largest region of the launch.  The tape is in tensor
+// memory (a.tmem_cols columns a warp).
+uint32_t adj_warp_floats(const uint32_t *stack_depth, int P, uint32_t n_params) {
+    uint32_t slots = 0;  // the stacks, whose slots the adjoints reuse
     for (int t = 0; t < N_STACKS; ++t) slots += stack_depth[t] * (uint32_t)kStackWidth[t];
     const uint32_t np = n_params < kAdjParams ? n_params : kAdjParams;
     return (slots * 32u * (uint32_t)P + np * 32u + 2u * 32u + 3u) & ~3u;
@@ -666,17 +756,17 @@ uint32_t adj_pack_depth(const uint32_t *stack_depth) {
     return v;
 }
 
-void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, LaunchArgs *a) {
-    const uint32_t nw = kAdjThreads / 32;
+void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, int nw, LaunchArgs *a) {
     a->block_hdr_floats = ((code_words + 2u + 3u) & ~3u) + ((const_floats + 3u) & ~3u) + 4u +
-                          2u * nw * (1u + kAdjParams);
+                          2u * (uint32_t)nw * (1u + kAdjParams);
     a->region_floats = warp_floats;
+    a->tmem_cols = 512u / ((uint32_t)nw / 4u);
 }
 
-size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats) {
+size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, int nw) {
     LaunchArgs a{};
-    adj_layout(code_words, const_floats, warp_floats, &a);
-    return ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (kAdjThreads / 32)) * 4u;
+    adj_layout(code_words, const_floats, warp_floats, nw, &a);
+    return ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (uint32_t)nw) * 4u;
 }
 
 template <int PROF, int P, int OMIT>
@@ -685,17 +775,8 @@ static cudaError_t launch_adj_pp(const LaunchArgs &a, uint32_t grid, size_t smem
     static std::atomic<uint64_t> limit_raised{0};
     cudaError_t e = raise_smem_limit(k, limit_raised);
     if (e != cudaSuccess) return e;
-    k<<<grid, kAdjThreads, smem, st>>>(a);
+    k<<<grid, adj_warps<PROF, P>() * 32, smem, st>>>(a);
     return cudaGetLastError();
-}
-
-template <int PROF, int P, int OMIT>
-static int adj_occ(size_t smem) {
-    auto k = adj_eval_kernel<PROF, P, OMIT>;
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemOptin) != cudaSuccess) return 0;
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kAdjThreads, smem) != cudaSuccess) return 0;
-    return n;
 }
 
 // Loads one instance ahead of its first real launch (an empty launch: run_if
@@ -714,8 +795,8 @@ int adj_max_p(int profile) { return profile == P_F || profile == P_FV3 ? 8 : 4; 
 
 // The instances that exist: (profile, P) as above; OMIT 0..3 for F+V3,
 // 0..1 for F and F+V2+M2, 0 for F+V3+M3.  `what` picks the launcher, the
-// occupancy query or the preload of instance (PROF, P, omit).
-enum AdjWhat { ADJ_LAUNCH, ADJ_OCC, ADJ_PRELOAD };
+// block size or the preload of instance (PROF, P, omit).
+enum AdjWhat { ADJ_LAUNCH, ADJ_WARPS, ADJ_PRELOAD };
 struct AdjCall {
     AdjWhat what;
     const LaunchArgs *a;
@@ -723,14 +804,14 @@ struct AdjCall {
     size_t smem;
     cudaStream_t st;
     const uint32_t *zero;
-    int occ = 0;
+    int occ = 0;  // ADJ_WARPS: the instance's warps per block
 };
 
 template <int PROF, int P, int OMIT>
 static cudaError_t adj_do(AdjCall &c) {
     if (c.what == ADJ_LAUNCH) return launch_adj_pp<PROF, P, OMIT>(*c.a, c.grid, c.smem, c.st);
-    if (c.what == ADJ_OCC) {
-        c.occ = adj_occ<PROF, P, OMIT>(c.smem);
+    if (c.what == ADJ_WARPS) {
+        c.occ = adj_warps<PROF, P>();
         return cudaSuccess;
     }
     return adj_preload_pp<PROF, P, OMIT>(c.zero, c.st);
@@ -781,9 +862,9 @@ cudaError_t launch_adj(const LaunchArgs &a, int profile, int P, unsigned omit, u
     return adj_dispatch(c, profile, P, omit);
 }
 
-int adj_max_blocks_per_sm(int profile, int P, unsigned omit, size_t smem) {
-    AdjCall c{ADJ_OCC, nullptr, 0, smem, nullptr, nullptr};
-    return adj_dispatch(c, profile, P, omit) == cudaSuccess ? c.occ : 0;
+int adj_block_warps(int profile, int P) {
+    AdjCall c{ADJ_WARPS, nullptr, 0, 0, nullptr, nullptr};
+    return adj_dispatch(c, profile, P, 0u) == cudaSuccess ? c.occ : 0;
 }
 
 cudaError_t preload_adj(const uint32_t *zero, cudaStream_t st) {

@@ -41,6 +41,7 @@ struct LaunchArgs {
     uint32_t block_hdr_floats;
     uint32_t acc_off;
     uint32_t stack_off[N_STACKS];
+    uint32_t tmem_cols;       // register adjoint: tensor-memory columns of a block's tapes
 };
 
 // Opt-in dynamic shared-memory limit of one block on sm_100 (227 KB).  Every

@@ -136,10 +136,11 @@ static constexpr int kRegPathStride = 8;
 // 40 KB and 81.6 ms at 20 KB; the vector and matrix workloads' tapes fit
 // 40 KB at 4 points and do not change.
 static constexpr size_t kGradTapeBudget = 80 * 1024;
-// Register adjoint: shared memory a warp's tape, stacks (which the adjoint
-// stacks reuse) and gradient sums may take (4 warps per block: two blocks fit an SM), and the
-// first path number of its launches in a gradient plan.
-static constexpr size_t kAdjWarpBudget = 24 * 1024;
+// Register adjoint: shared memory the warps' stacks (which the adjoint
+// stacks reuse) and gradient sums may take in a block (one block per SM,
+// the rest of the 227 KB for code, constants and sums), and the first path
+// number of its launches in a gradient plan.
+static constexpr size_t kAdjRegionBudget = 200 * 1024;
 static constexpr int kAdjPathBase = 0;
 // Points per work-item chunk (all P).  8192 measured slower on every kernel
 // (vector register 4.32 ms against 4.30, matrix register 4.84 against 4.69,
@@ -256,18 +257,24 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
     for (uint32_t i = 0; i < n; ++i) {
         if (gradient && enc[i].adj_profile >= 0 && adj_supported(enc[i].adj_profile) &&
             !(ctx->opts.flags & RSR_OPT_SLOT_ADJOINT)) {
-            // register adjoint: the most points per lane (8, 4, 2) whose warp
-            // region (tape, stacks, gradient sums) fits
-            // kAdjWarpBudget; launches by that region's size in steps of 4 KB,
-            // so that a block's shared memory follows its own programs
+            // register adjoint: the most points per lane (8, 4, 2) whose tape
+            // fits a warp's share of the SM's tensor memory (512 columns / (warps
+            // / 4), P columns a slot) and whose stacks and sums fit the block's
+            // shared memory; launches by points per lane and profile
             const EncodedProgram &E = enc[i];
             uint32_t depth[N_STACKS];
             for (int t = 0; t < N_STACKS; ++t) depth[t] = (uint32_t)E.adj_depth[t];
-            int pc = adj_max_p(E.adj_profile) >= 8 ? 2 : 1;  // points per lane 2 << pc: the most that fits
             const uint32_t np = (uint32_t)E.consts.size();
-            while (pc >= 0 && (size_t)adj_warp_floats(E.adj_tape, depth, 2 << pc, np) * 4u > kAdjWarpBudget) --pc;
+            int pc = adj_max_p(E.adj_profile) >= 8 ? 2 : 1;  // points per lane 2 << pc
+            for (; pc >= 0; --pc) {
+                const int P = 2 << pc, nw = adj_block_warps(E.adj_profile, P);
+                const uint32_t cols = 512u / (uint32_t)(nw / 4);
+                if (E.adj_tape * (uint32_t)P <= cols &&
+                    (size_t)adj_warp_floats(depth, P, np) * 4u * (size_t)nw <= kAdjRegionBudget)
+                    break;
+            }
             if (pc >= 0) {
-                const int bucket = (int)((adj_warp_floats(E.adj_tape, depth, 2 << pc, np) + 1023u) / 1024u);
+                const int bucket = 0;
                 // the handler sets the program does not use (forward entries:
                 // two words each after the header words); a launch leaves out
                 // those none of its programs uses
@@ -469,8 +476,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                 if (g.kind == 3) {  // slots: the largest warp region (floats)
                     uint32_t depth[N_STACKS];
                     for (int t = 0; t < N_STACKS; ++t) depth[t] = (uint32_t)enc[order[q]].adj_depth[t];
-                    sl = std::max(sl, adj_warp_floats(enc[order[q]].adj_tape, depth, g.P,
-                                                      (uint32_t)enc[order[q]].consts.size()));
+                    sl = std::max(sl, adj_warp_floats(depth, g.P, (uint32_t)enc[order[q]].consts.size()));
                 }
             }
             g.code_words = std::max(g.code_words, cw);
@@ -615,7 +621,8 @@ static int blocks_per_sm(int device, int kind, int profile, int P, unsigned omit
         auto it = cache.find(key);
         if (it != cache.end()) return it->second;
     }
-    const int n = kind == 1 ? reg_max_blocks_per_sm(profile, P, omit, smem) : adj_max_blocks_per_sm(profile, P, omit, smem);
+    (void)kind;
+    const int n = reg_max_blocks_per_sm(profile, P, omit, smem);
     if (n > 0) {
         std::lock_guard<std::mutex> lk(mu);
         cache[key] = n;
@@ -712,18 +719,25 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             g.warps_per_block = kRegThreads / 32;
             e = launch_reg(a, g.profile, g.P, g.omit, g.grid, gs);
         } else if (g.kind == 3) {
-            adj_layout(g.code_words, g.const_floats, g.slots, &a);
-            const size_t smem = adj_smem_bytes(g.code_words, g.const_floats, g.slots);
-            if (smem > (size_t)kMaxDynSmemOptin) {
+            const int nw = adj_block_warps(g.profile, g.P);
+            adj_layout(g.code_words, g.const_floats, g.slots, nw, &a);
+            g.tmem_cols = a.tmem_cols;
+            // One block per SM: it allocates all of the SM's tensor memory,
+            // and its shared memory is padded past half the SM's so that no
+            // second such block, of this launch or one beside it, shares the
+            // SM and waits for the columns.
+            const size_t half = ctx->smem_per_sm / 2 + 16;
+            const size_t pad = half > ctx->smem_reserved ? half - ctx->smem_reserved : 0;
+            const size_t smem = std::max(adj_smem_bytes(g.code_words, g.const_floats, g.slots, nw), pad);
+            if (nw < 4 || smem > (size_t)kMaxDynSmemOptin) {
                 e = cudaErrorInvalidValue;
                 join_side_streams(dev, st, forked);
                 return fail(RSR_EINVAL, "register adjoint launch needs " + std::to_string(smem) +
                                             " bytes of shared memory per block");
             }
-            const int bps = std::max(1, blocks_per_sm(ctx->device, 3, g.profile, g.P, g.omit, smem));
-            g.grid = std::max(1u, (uint32_t)std::min<uint64_t>((uint64_t)bps * ctx->num_sms, g.n_items));
+            g.grid = std::max(1u, (uint32_t)std::min<uint64_t>((uint64_t)ctx->num_sms, g.n_items));
             g.smem = smem;
-            g.warps_per_block = kAdjThreads / 32;
+            g.warps_per_block = (uint32_t)nw;
             e = launch_adj(a, g.profile, g.P, g.omit, g.grid, smem, gs);
         } else {
             const size_t per = grad_smem_per_warp(g.code_words, g.const_floats, g.slots, g.adj_slots, g.P);
@@ -974,6 +988,8 @@ int rsr_ctx_create(int device, const rsr_options *opts, rsr_ctx **out) {
     auto *ctx = new rsr_ctx();
     ctx->device = device;
     ctx->num_sms = prop.multiProcessorCount;
+    ctx->smem_per_sm = prop.sharedMemPerMultiprocessor;
+    ctx->smem_reserved = prop.reservedSharedMemPerBlock;
     rsr_options_default(&ctx->opts);
     if (opts) memcpy(&ctx->opts, opts, std::min<size_t>(sizeof(rsr_options), opts->struct_size ? opts->struct_size : sizeof(rsr_options)));
     if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
@@ -1298,7 +1314,8 @@ int rsr_batch_describe(rsr_ctx *ctx, rsr_batch *b, char *buf, size_t len) {
         const char *kn = g.kind == 0 ? "slot" : g.kind == 1 ? "register" : g.kind == 2 ? "adjoint" : "register_adjoint";
         s += (i ? ", " : "") + std::string("{\"kernel\": \"") + kn + "\", \"profile\": " + std::to_string(g.profile) +
              ", \"no_unary\": " + (((g.kind == 1 || g.kind == 3) ? (g.omit & 1u) != 0 : g.no_unary) ? "true" : "false") +
-             ", \"no_matrix_operand\": " + ((g.kind == 1 && (g.omit & 2u)) ? "true" : "false") +
+             ", \"no_matrix_operand\": " + (((g.kind == 1 || g.kind == 3) && (g.omit & 2u)) ? "true" : "false") +
+             ", \"tmem_cols\": " + std::to_string(g.tmem_cols) +
              ", \"points_per_thread\": " + std::to_string(g.P) + ", \"programs_per_warp\": " + std::to_string(g.G) +
              ", \"items\": " + std::to_string(g.n_items) + ", \"flops\": " + std::to_string(g.flops) +
              ", \"program_points\": " + std::to_string(g.program_points) + ", \"grid\": " + std::to_string(g.grid) +

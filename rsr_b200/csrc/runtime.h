@@ -113,6 +113,7 @@ struct Group {
     mutable uint32_t grid = 0;
     mutable size_t smem = 0;
     mutable uint32_t warps_per_block = 0;
+    mutable uint32_t tmem_cols = 0;     // register adjoint: tensor-memory columns of a warp's tape
     uint64_t flops = 0;           // algorithmic FP32 lane-ops of one run
     uint64_t program_points = 0;
     uint64_t item_work = 0;       // code length x tiles of the group's longest item
@@ -187,6 +188,8 @@ struct DevicePlan {
 struct rsr_ctx {
     int device = 0;
     int num_sms = 0;
+    size_t smem_per_sm = 0;    // shared memory of an SM (bytes)
+    size_t smem_reserved = 0;  // shared memory the system reserves per block
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;  // odd chunks of a chunked one-shot call
     rsr_options opts{};
