@@ -48,8 +48,9 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 # DRAM bytes (read + write) of the dominant kernel's launches in one step of
-# this workload (three spill-depth classes, P=8 G=4), from one ncu capture
-# (profiles/launch_list_bench_vector_4096x100k.md, "DRAM traffic"):
+# this workload (three spill-depth classes, P=8 G=4), from one ncu capture of
+# `bench.py --case --workload vector --programs 4096 --kernel register --runs 3
+# --points-per-thread 8 --programs-per-warp 4` (dram__bytes_read/write.sum):
 # 4,711,424 + 4,775,680 + 4,116,736 read, 512 written.  ncu replays each launch
 # with cold caches, so each re-reads the 4 MB dataset; in a step the second
 # and third launches find it in L2.
