@@ -26,9 +26,9 @@ end-to-end, serving and search legs.
 image) on all host cores, on bounded samples of the same workload.
 
 `--case` runs one fixed evaluation case for profilers instead (`--workload`,
-`--programs`, `--points`, `--kernel register|plain|adjoint`, `--runs`,
-`--points-per-thread`, `--programs-per-warp`): the commands under profiles/
-use it.
+`--programs`, `--points`, `--kernel register|plain|adjoint|slot-adjoint`,
+`--runs`, `--points-per-thread`, `--programs-per-warp`), a small case for an
+ncu capture.
 """
 from __future__ import annotations
 
