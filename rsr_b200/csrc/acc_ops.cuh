@@ -11,6 +11,7 @@
 // by the encoder), or another type's accumulator.
 #pragma once
 #include "kernels_common.cuh"
+#include "tmem.cuh"
 
 namespace rsr {
 
