@@ -2,12 +2,12 @@
 // 32-bit loads and stores of P consecutive columns of a thread's own lane
 // (shape 32x32b: a warp reaches the 32 lanes of its quadrant, warp w of a
 // block lanes 32 (w % 4) .. +31).  The register adjoint keeps its tape
-// here, the register kernel its tiles of features.  Stores are
-// asynchronous (tm_wait_st before a load reads them); tm_ld waits for its
-// own load, and the wait names the loaded registers so that no use of them
-// is scheduled before it.  A block allocates with tm_alloc (one warp, which
-// also gives up the right to allocate again), fences around the barrier
-// that publishes the address, and frees with tm_dealloc before it exits.
+// here.  Stores are asynchronous (tm_wait_st before a load reads them);
+// tm_ld waits for its own load, and the wait names the loaded registers so
+// that no use of them is scheduled before it.  A block allocates with
+// tm_alloc (one warp, which also gives up the right to allocate again),
+// fences around the barrier that publishes the address, and frees with
+// tm_dealloc before it exits.
 #pragma once
 #include <stdint.h>
 
