@@ -146,6 +146,14 @@ static constexpr int kAdjPathBase = 0;
 // (vector register 4.32 ms against 4.30, matrix register 4.84 against 4.69,
 // vector adjoint 6.68 against 5.90): coarser items balance worse.
 static constexpr uint64_t kChunkPoints = 4096;
+// Points per work-item chunk of the register adjoint, whose block is the
+// SM's only one: between items the SM waits for the item's code and the
+// cross-warp sums, so its chunks are four rounds of 16 warps at eight
+// points per lane.  A dataset's last chunk takes the remainder (one to two
+// chunks' worth), so no item is a few tiles on an otherwise idle block.
+static constexpr uint64_t kAdjChunkPoints = 16384;
+// Points per lane of a register-adjoint path (its launch's P).
+static int adj_path_p(int pth) { return 2 << (((pth - kAdjPathBase) / N_PROFILES) % 3); }
 static constexpr uint64_t kStrideAlign = 1024;   // dataset column padding
 static constexpr int kGradSlotDoubles = 33;      // sse + 32 gradient sums
 
@@ -406,7 +414,12 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                   (E.differentiable ? PF_DIFFERENTIABLE : 0u);
         d.dataset = prog_ds[i];
         const uint64_t n_eval = P.datasets[d.dataset].n_eval;
-        d.n_parts = (uint32_t)std::max<uint64_t>(1, (n_eval + kChunkPoints - 1) / kChunkPoints);
+        if (reg_adj) {
+            const uint64_t tile_pts = 32ull * (uint64_t)adj_path_p(path[i]);
+            d.n_parts = (uint32_t)std::max<uint64_t>(1, ((n_eval + tile_pts - 1) / tile_pts) / (kAdjChunkPoints / tile_pts));
+        } else {
+            d.n_parts = (uint32_t)std::max<uint64_t>(1, (n_eval + kChunkPoints - 1) / kChunkPoints);
+        }
         d.part_off = part;
         if (reg_adj) {
             uint32_t depth[N_STACKS];
@@ -444,7 +457,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
         g.item_begin = (uint32_t)P.items.size();
         if (g.kind == 3) {
             g.G = 1;
-            g.P = 2 << (((pth - kAdjPathBase) / N_PROFILES) % 3);
+            g.P = adj_path_p(pth);
         } else if (g.kind == 1) {
             // P and G are per profile and dataset size; one launch uses one P,
             // the largest dataset's choice.
@@ -504,14 +517,16 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             while (Pp > 1 && plain_smem_per_warp(g.code_words, g.const_floats, g.slots, Pp) > 110 * 1024) Pp >>= 1;
             g.P = Pp;
         }
-        // Expand each item into chunks of kChunkPoints and order them longest
-        // first (persistent kernels pull items in this order; any order
-        // gives the same sums).  A chunk's work is its programs' code length
-        // times its tiles: every chunk but an item's last has the same tile
-        // count whatever the dataset, so the items sorted by code length give
-        // the full chunks in order, and the short last chunks are merged in.
+        // Expand each item into chunks of kChunkPoints (kAdjChunkPoints for
+        // the register adjoint, whose last chunk takes the remainder) and
+        // order them longest first (persistent kernels pull items in this
+        // order; any order gives the same sums).  A chunk's work is its
+        // programs' code length times its tiles: every chunk but an item's
+        // last has the same tile count whatever the dataset, so the items
+        // sorted by code length give the full chunks in order, and the last
+        // chunks are merged in.  The chunk count is the programs' n_parts.
         const uint64_t tile_pts = 32ull * g.P;
-        const uint64_t tpc = kChunkPoints / tile_pts;
+        const uint64_t tpc = (g.kind == 3 ? kAdjChunkPoints : kChunkPoints) / tile_pts;
         std::stable_sort(items.begin(), items.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
         full.clear();
         tail.clear();
@@ -519,10 +534,11 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             const WorkItem &w = pr.second;
             const uint64_t n_eval = P.datasets[P.progs[w.prog_begin].dataset].n_eval;
             const uint64_t n_tiles = (n_eval + tile_pts - 1) / tile_pts;
-            for (uint64_t c = 0, t = 0; t < n_tiles; ++c, t += tpc) {
+            const uint64_t n_parts = n_tiles ? P.progs[w.prog_begin].n_parts : 0;
+            for (uint64_t c = 0, t = 0; c < n_parts; ++c, t += tpc) {
                 WorkItem it = w;
                 it.tile_begin = (uint32_t)t;
-                it.tile_end = (uint32_t)std::min(n_tiles, t + tpc);
+                it.tile_end = (uint32_t)(c + 1 == n_parts ? n_tiles : std::min(n_tiles, t + tpc));
                 it.chunk = (uint32_t)c;
                 const uint64_t tiles = it.tile_end - it.tile_begin;
                 (tiles == tpc ? full : tail).emplace_back(pr.first * tiles, it);
