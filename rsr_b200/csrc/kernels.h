@@ -11,6 +11,12 @@ namespace rsr {
 constexpr int kPlainThreads = 128;  // 4 warps per block, one work item per warp
 constexpr int kRegThreads = 256;  // 8 warps share one work item
 constexpr int kGradThreads = 32;  // one warp per block, one item per warp
+// Points per partial sum: a program's MSE (and gradient) is the sum, in
+// order, of its per-part sums, each part 4096 consecutive points of its
+// dataset.  A work item covers one part (the register adjoint: up to
+// kAdjMaxParts), so results do not depend on how a batch is cut into items.
+constexpr uint32_t kPartPoints = 4096;
+constexpr uint32_t kAdjMaxParts = 5;
 
 cudaError_t launch_plain(const LaunchArgs &a, int P, uint32_t warps_per_block, size_t smem, cudaStream_t st);
 size_t plain_smem_per_warp(uint32_t code_words, uint32_t const_floats, uint32_t slots, int P);
@@ -56,10 +62,12 @@ int adj_max_p(int profile);
 // packed for ProgDesc
 uint32_t adj_warp_floats(const uint32_t *stack_depth, int P, uint32_t n_params);
 uint32_t adj_pack_depth(const uint32_t *stack_depth);
-// shared-memory layout of a block of nw warps; the tensor-memory columns
-// of each warp's tape (512 / (nw / 4)) go to a->tmem_cols
-void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, int nw, LaunchArgs *a);
-size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, int nw);
+// shared-memory layout of a block of nw warps whose items cover at most
+// `parts` parts; the tensor-memory columns of each warp's tape (512 / (nw /
+// 4)) go to a->tmem_cols
+void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, int nw, uint32_t parts,
+                LaunchArgs *a);
+size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, int nw, uint32_t parts);
 // warps of a block of instance (profile, P), one block per SM (a multiple of 4)
 int adj_block_warps(int profile, int P);
 // Handler sets an instance may leave out (bit 0: unary Float ops; bit 1,

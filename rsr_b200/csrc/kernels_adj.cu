@@ -566,7 +566,7 @@ __global__ void __launch_bounds__(adj_warps<PROF, P>() * 32, 1) adj_eval_kernel(
     uint32_t *scode = reinterpret_cast<uint32_t *>(smem);
     float *sconst = smem + ((a.smem_code_words + 2u + 3u) & ~3u);  // code and its two pad words
     uint32_t *meta = reinterpret_cast<uint32_t *>(sconst + ((a.smem_const_floats + 3u) & ~3u));  // [0] item, [1] tape
-    double *red = reinterpret_cast<double *>(meta + 4);  // [warp][1 + kAdjParams]
+    double *red = reinterpret_cast<double *>(meta + 4);  // [part][warp][1 + kAdjParams]
     float *wbase = smem + a.block_hdr_floats + (size_t)warp * a.region_floats;
 
     // the block takes all of the SM's tensor memory; warp w owns lanes
@@ -621,55 +621,72 @@ __global__ void __launch_bounds__(adj_warps<PROF, P>() * 32, 1) adj_eval_kernel(
         io.stride = (uint32_t)ds.stride;
         const uint32_t n_fwd = scode[0], n_rev = scode[1];
         const uint32_t *fwd = scode + kAdjHeaderWords, *rev = fwd + 2 * n_fwd;
-        for (uint32_t tile = it.tile_begin + warp; tile < it.tile_end; tile += nw) {
-            const uint64_t t0 = (uint64_t)tile * (32u * P);
-            const uint64_t p0 = t0 + lane_point<P>(lane, 0);
-            io.xl = ds.x + p0;
-            uint32_t valid = 0;
+        // The item's parts (kPartPoints points each) one after another; a
+        // warp takes the same tiles of a part, and sums them the same way,
+        // whatever the item's size, so a program's partial sums do not
+        // depend on how its batch was cut into items.
+        constexpr uint32_t part_tiles = kPartPoints / (32u * P);
+        const uint32_t n_parts = (it.tile_end - it.tile_begin + part_tiles - 1) / part_tiles;
+        for (uint32_t part = 0; part < n_parts; ++part) {
+            const uint32_t part_end = min(it.tile_end, it.tile_begin + (part + 1) * part_tiles);
+            for (uint32_t tile = it.tile_begin + part * part_tiles + warp; tile < part_end; tile += nw) {
+                const uint64_t t0 = (uint64_t)tile * (32u * P);
+                const uint64_t p0 = t0 + lane_point<P>(lane, 0);
+                io.xl = ds.x + p0;
+                uint32_t valid = 0;
 #pragma unroll
-            for (int q = 0; q < P; ++q) valid |= (t0 + lane_point<P>(lane, q) < ds.n_eval ? 1u : 0u) << q;
-            io.valid = valid;
-            Acc<PROF, P> acc;
-            run_forward<PROF, P, OMIT>(acc, io, fwd, n_fwd);
-            tm_wait_st();  // the tape stores land before the reverse sweep reads them
-            const Vf<P> y = load_lane<P>(ds.y + p0);
-            Acc<PROF, P> g;
-            g.F[0] = splat<P>(0.0f);
-            if constexpr (Types<PROF>::V2) zero_acc<P, 2>(g.V2);
-            if constexpr (Types<PROF>::V3) zero_acc<P, 3>(g.V3);
-            if constexpr (Types<PROF>::M2) zero_acc<P, 4>(g.M2);
-            if constexpr (Types<PROF>::M3) zero_acc<P, 9>(g.M3);
-            Kahan ks;
-            ks.s = kahan[lane];
-            ks.c = kahan[32 + lane];
+                for (int q = 0; q < P; ++q) valid |= (t0 + lane_point<P>(lane, q) < ds.n_eval ? 1u : 0u) << q;
+                io.valid = valid;
+                Acc<PROF, P> acc;
+                run_forward<PROF, P, OMIT>(acc, io, fwd, n_fwd);
+                tm_wait_st();  // the tape stores land before the reverse sweep reads them
+                const Vf<P> y = load_lane<P>(ds.y + p0);
+                Acc<PROF, P> g;
+                g.F[0] = splat<P>(0.0f);
+                if constexpr (Types<PROF>::V2) zero_acc<P, 2>(g.V2);
+                if constexpr (Types<PROF>::V3) zero_acc<P, 3>(g.V3);
+                if constexpr (Types<PROF>::M2) zero_acc<P, 4>(g.M2);
+                if constexpr (Types<PROF>::M3) zero_acc<P, 9>(g.M3);
+                Kahan ks;
+                ks.s = kahan[lane];
+                ks.c = kahan[32 + lane];
 #pragma unroll
-            for (int q = 0; q < P; ++q) {
-                const bool ok = (valid >> q) & 1u;
-                const float d = acc.F[0].v[q] - y.v[q];
-                if (ok) ks.add(d * d);
-                g.F[0].v[q] = ok ? 2.0f * d : 0.0f;  // d(diff^2)/d pred, as in evaluator.rs:207
+                for (int q = 0; q < P; ++q) {
+                    const bool ok = (valid >> q) & 1u;
+                    const float d = acc.F[0].v[q] - y.v[q];
+                    if (ok) ks.add(d * d);
+                    g.F[0].v[q] = ok ? 2.0f * d : 0.0f;  // d(diff^2)/d pred, as in evaluator.rs:207
+                }
+                kahan[lane] = ks.s;
+                kahan[32 + lane] = ks.c;
+                run_reverse<PROF, P, OMIT>(g, io, rev, n_rev);
             }
-            kahan[lane] = ks.s;
-            kahan[32 + lane] = ks.c;
-            run_reverse<PROF, P, OMIT>(g, io, rev, n_rev);
-        }
-        // per-warp sums in f64, then across warps in a fixed order
-        {
-            Kahan ks;
-            ks.s = kahan[lane];
-            ks.c = kahan[32 + lane];
-            const double s = warp_sum(ks.value());
-            if (lane == 0) red[warp * (1 + kAdjParams)] = s;
-            for (uint32_t k = 0; k < kAdjParams; ++k) {
-                const double gk = k < np ? warp_sum((double)io.gacc[k * 32]) : 0.0;
-                if (lane == 0) red[warp * (1 + kAdjParams) + 1 + k] = gk;
+            // the warp's sums of this part in f64, then a fresh start for the next
+            {
+                double *wred = red + ((size_t)part * nw + warp) * (1 + kAdjParams);
+                Kahan ks;
+                ks.s = kahan[lane];
+                ks.c = kahan[32 + lane];
+                const double s = warp_sum(ks.value());
+                if (lane == 0) wred[0] = s;
+                for (uint32_t k = 0; k < np; ++k) {
+                    const double gk = warp_sum((double)io.gacc[k * 32]);
+                    if (lane == 0) wred[1 + k] = gk;
+                    io.gacc[k * 32] = 0.0f;
+                }
+                kahan[lane] = 0.0f;
+                kahan[32 + lane] = 0.0f;
             }
         }
+        // each part's sums across warps in a fixed order (the sums of the
+        // parameters past the program's own are 0)
         __syncthreads();
-        if (threadIdx.x < 1 + kAdjParams) {
+        for (uint32_t t = threadIdx.x; t < n_parts * (1 + kAdjParams); t += blockDim.x) {
+            const uint32_t part = t / (1 + kAdjParams), k = t % (1 + kAdjParams);
             double s = 0.0;
-            for (int w = 0; w < nw; ++w) s += red[w * (1 + kAdjParams) + threadIdx.x];
-            a.partials[(size_t)(pd.part_off + it.chunk) * (1 + kAdjParams) + threadIdx.x] = s;
+            if (k <= np)
+                for (int w = 0; w < nw; ++w) s += red[((size_t)part * nw + w) * (1 + kAdjParams) + k];
+            a.partials[(size_t)(pd.part_off + it.chunk + part) * (1 + kAdjParams) + k] = s;
         }
         __syncthreads();
     }
@@ -681,7 +698,7 @@ __global__ void __launch_bounds__(adj_warps<PROF, P>() * 32, 1) adj_eval_kernel(
 
 // ------------------------------------------------------------- launchers
 // Shared-memory layout (floats).  Block header: code (+2 pads) | constants |
-// meta (4 words) | cross-warp sums (warps x 33 doubles).  Per warp: stacks
+// meta (4 words) | cross-warp sums (parts x warps x 33 doubles).  Per warp: stacks
 // (per type; the reverse sweep's adjoint stacks in the same slots) |
 // gradient sums (one row of 32 per parameter, at most 32) | Kahan state (2 x
 // 32), each program's own sizes (the kernel lays the region out per item);
@@ -700,16 +717,17 @@ uint32_t adj_pack_depth(const uint32_t *stack_depth) {
     return v;
 }
 
-void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, int nw, LaunchArgs *a) {
+void adj_layout(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, int nw, uint32_t parts,
+                LaunchArgs *a) {
     a->block_hdr_floats = ((code_words + 2u + 3u) & ~3u) + ((const_floats + 3u) & ~3u) + 4u +
-                          2u * (uint32_t)nw * (1u + kAdjParams);
+                          2u * parts * (uint32_t)nw * (1u + kAdjParams);
     a->region_floats = warp_floats;
     a->tmem_cols = 512u / ((uint32_t)nw / 4u);
 }
 
-size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, int nw) {
+size_t adj_smem_bytes(uint32_t code_words, uint32_t const_floats, uint32_t warp_floats, int nw, uint32_t parts) {
     LaunchArgs a{};
-    adj_layout(code_words, const_floats, warp_floats, nw, &a);
+    adj_layout(code_words, const_floats, warp_floats, nw, parts, &a);
     return ((size_t)a.block_hdr_floats + (size_t)a.region_floats * (uint32_t)nw) * 4u;
 }
 

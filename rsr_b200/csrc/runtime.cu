@@ -145,13 +145,25 @@ static constexpr int kAdjPathBase = 0;
 // Points per work-item chunk (all P).  8192 measured slower on every kernel
 // (vector register 4.32 ms against 4.30, matrix register 4.84 against 4.69,
 // vector adjoint 6.68 against 5.90): coarser items balance worse.
-static constexpr uint64_t kChunkPoints = 4096;
-// Points per work-item chunk of the register adjoint, whose block is the
-// SM's only one: between items the SM waits for the item's code and the
-// cross-warp sums, so its chunks are four rounds of 16 warps at eight
-// points per lane.  A dataset's last chunk takes the remainder (one to two
-// chunks' worth), so no item is a few tiles on an otherwise idle block.
-static constexpr uint64_t kAdjChunkPoints = 16384;
+static constexpr uint64_t kChunkPoints = kPartPoints;
+// Work items of the register adjoint cover several parts: its block is the
+// SM's only one, and between items the SM waits for the next item's code
+// and for the item's cross-warp sums.  A launch takes the most parts an
+// item (about 4, 2 or 1) that still leave it kAdjItemsPerSm items an SM, so
+// that a small batch keeps short items and its launch does not end on a few
+// long ones, and whose cross-warp sums fit the block's shared memory.  A
+// dataset's parts are spread evenly over floor(parts / k) items of at most
+// k + 1 parts (25 parts: one item of 5 and five of 4), so that no item is a
+// few tiles on an otherwise idle block.  The kernel sums every part on its
+// own, so the sums do not depend on the items.
+static constexpr uint64_t kAdjItemsPerSm = 8;
+
+// Items a dataset of n_parts parts is cut into, at about k parts an item
+// and at most k + 1 (k = 1: one part an item).
+static uint64_t adj_items(uint64_t n_parts, uint32_t k) {
+    if (k <= 1) return n_parts;
+    return std::max<uint64_t>({1, n_parts / k, (n_parts + k) / (k + 1)});
+}
 // Points per lane of a register-adjoint path (its launch's P).
 static int adj_path_p(int pth) { return 2 << (((pth - kAdjPathBase) / N_PROFILES) % 3); }
 static constexpr uint64_t kStrideAlign = 1024;   // dataset column padding
@@ -414,12 +426,7 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
                   (E.differentiable ? PF_DIFFERENTIABLE : 0u);
         d.dataset = prog_ds[i];
         const uint64_t n_eval = P.datasets[d.dataset].n_eval;
-        if (reg_adj) {
-            const uint64_t tile_pts = 32ull * (uint64_t)adj_path_p(path[i]);
-            d.n_parts = (uint32_t)std::max<uint64_t>(1, ((n_eval + tile_pts - 1) / tile_pts) / (kAdjChunkPoints / tile_pts));
-        } else {
-            d.n_parts = (uint32_t)std::max<uint64_t>(1, (n_eval + kChunkPoints - 1) / kChunkPoints);
-        }
+        d.n_parts = (uint32_t)std::max<uint64_t>(1, (n_eval + kChunkPoints - 1) / kChunkPoints);
         d.part_off = part;
         if (reg_adj) {
             uint32_t depth[N_STACKS];
@@ -517,16 +524,29 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             while (Pp > 1 && plain_smem_per_warp(g.code_words, g.const_floats, g.slots, Pp) > 110 * 1024) Pp >>= 1;
             g.P = Pp;
         }
-        // Expand each item into chunks of kChunkPoints (kAdjChunkPoints for
-        // the register adjoint, whose last chunk takes the remainder) and
-        // order them longest first (persistent kernels pull items in this
-        // order; any order gives the same sums).  A chunk's work is its
-        // programs' code length times its tiles: every chunk but an item's
-        // last has the same tile count whatever the dataset, so the items
-        // sorted by code length give the full chunks in order, and the last
-        // chunks are merged in.  The chunk count is the programs' n_parts.
+        // register adjoint: parts per work item
+        if (g.kind == 3) {
+            const int nw = adj_block_warps(g.profile, g.P);
+            uint32_t k = kAdjMaxParts - 1;
+            for (; k > 1; k >>= 1) {
+                uint64_t n_items = 0;
+                for (uint32_t q = li; q < end; ++q) n_items += adj_items(P.progs[q].n_parts, k);
+                if (n_items >= kAdjItemsPerSm * (uint64_t)ctx->num_sms &&
+                    adj_smem_bytes(g.code_words, g.const_floats, g.slots, nw, k + 1) <= (size_t)kMaxDynSmemOptin)
+                    break;
+            }
+            g.parts = k;
+        }
+        // Expand each item into chunks of kChunkPoints (g.parts of them for
+        // the register adjoint) and order them longest first (persistent
+        // kernels pull items in this order; any order gives the same sums).
+        // A chunk's work is its programs' code length times its tiles: every
+        // chunk but an item's last has the same tile count whatever the
+        // dataset, so the items sorted by code length give the full chunks in
+        // order, and the short last chunks are merged in.
         const uint64_t tile_pts = 32ull * g.P;
-        const uint64_t tpc = (g.kind == 3 ? kAdjChunkPoints : kChunkPoints) / tile_pts;
+        const uint64_t part_tiles = kChunkPoints / tile_pts;
+        const uint64_t tpc = g.parts * part_tiles;
         std::stable_sort(items.begin(), items.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
         full.clear();
         tail.clear();
@@ -534,11 +554,23 @@ int build_plan(rsr_ctx *ctx, const rsr_population &pop, const uint64_t *ds_per_p
             const WorkItem &w = pr.second;
             const uint64_t n_eval = P.datasets[P.progs[w.prog_begin].dataset].n_eval;
             const uint64_t n_tiles = (n_eval + tile_pts - 1) / tile_pts;
-            const uint64_t n_parts = n_tiles ? P.progs[w.prog_begin].n_parts : 0;
-            for (uint64_t c = 0, t = 0; c < n_parts; ++c, t += tpc) {
+            if (g.kind == 3) {  // parts spread evenly over the items
+                const uint64_t n_parts = P.progs[w.prog_begin].n_parts, m = n_tiles ? adj_items(n_parts, g.parts) : 0;
+                for (uint64_t c = 0; c < m; ++c) {
+                    WorkItem it = w;
+                    const uint64_t p0 = c * n_parts / m, p1 = (c + 1) * n_parts / m;
+                    it.tile_begin = (uint32_t)(p0 * part_tiles);
+                    it.tile_end = (uint32_t)std::min(n_tiles, p1 * part_tiles);
+                    it.chunk = (uint32_t)p0;  // the item's first part
+                    const uint64_t tiles = it.tile_end - it.tile_begin;
+                    (tiles == tpc ? full : tail).emplace_back(pr.first * tiles, it);
+                }
+                continue;
+            }
+            for (uint64_t c = 0, t = 0; t < n_tiles; ++c, t += tpc) {
                 WorkItem it = w;
                 it.tile_begin = (uint32_t)t;
-                it.tile_end = (uint32_t)(c + 1 == n_parts ? n_tiles : std::min(n_tiles, t + tpc));
+                it.tile_end = (uint32_t)std::min(n_tiles, t + tpc);
                 it.chunk = (uint32_t)c;
                 const uint64_t tiles = it.tile_end - it.tile_begin;
                 (tiles == tpc ? full : tail).emplace_back(pr.first * tiles, it);
@@ -744,7 +776,7 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             e = launch_reg(a, g.profile, g.P, g.omit, g.grid, gs);
         } else if (g.kind == 3) {
             const int nw = adj_block_warps(g.profile, g.P);
-            adj_layout(g.code_words, g.const_floats, g.slots, nw, &a);
+            adj_layout(g.code_words, g.const_floats, g.slots, nw, g.parts + (g.parts > 1), &a);
             g.tmem_cols = a.tmem_cols;
             // One block per SM: it allocates all of the SM's tensor memory,
             // and its shared memory is padded past half the SM's so that no
@@ -752,7 +784,8 @@ int enqueue_plan(rsr_ctx *ctx, const Plan &plan, DevicePlan *dev, cudaStream_t s
             // SM and waits for the columns.
             const size_t half = ctx->smem_per_sm / 2 + 16;
             const size_t pad = half > ctx->smem_reserved ? half - ctx->smem_reserved : 0;
-            const size_t smem = std::max(adj_smem_bytes(g.code_words, g.const_floats, g.slots, nw), pad);
+            const size_t smem =
+                std::max(adj_smem_bytes(g.code_words, g.const_floats, g.slots, nw, g.parts + (g.parts > 1)), pad);
             if (nw < 4 || smem > (size_t)kMaxDynSmemOptin) {
                 e = cudaErrorInvalidValue;
                 join_side_streams(dev, st, forked);
@@ -1339,7 +1372,7 @@ int rsr_batch_describe(rsr_ctx *ctx, rsr_batch *b, char *buf, size_t len) {
         s += (i ? ", " : "") + std::string("{\"kernel\": \"") + kn + "\", \"profile\": " + std::to_string(g.profile) +
              ", \"no_unary\": " + (((g.kind == 1 || g.kind == 3) ? (g.omit & 1u) != 0 : g.no_unary) ? "true" : "false") +
              ", \"no_matrix_operand\": " + (((g.kind == 1 || g.kind == 3) && (g.omit & 2u)) ? "true" : "false") +
-             ", \"tmem_cols\": " + std::to_string(g.tmem_cols) +
+             ", \"tmem_cols\": " + std::to_string(g.tmem_cols) + ", \"parts_per_item\": " + std::to_string(g.parts) +
              ", \"points_per_thread\": " + std::to_string(g.P) + ", \"programs_per_warp\": " + std::to_string(g.G) +
              ", \"items\": " + std::to_string(g.n_items) + ", \"flops\": " + std::to_string(g.flops) +
              ", \"program_points\": " + std::to_string(g.program_points) + ", \"grid\": " + std::to_string(g.grid) +

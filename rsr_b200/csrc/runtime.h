@@ -108,6 +108,7 @@ struct Group {
     uint32_t item_begin = 0, n_items = 0;  // into the plan's item array
     uint32_t code_words = 0, const_floats = 0, slots = 0;  // per-warp staging maxima
     uint32_t adj_slots = 0;                                  // adjoint kernel: adjoint slots
+    uint32_t parts = 1;   // register adjoint: about this many parts (kPartPoints points) an item, at most one more
     uint32_t stack_depth[N_STACKS] = {0, 0, 0, 0, 0};       // register kernel: spill slots per type
     // launch shape of the last enqueue (filled in by enqueue_plan)
     mutable uint32_t grid = 0;

@@ -232,6 +232,18 @@ def test_alone_and_in_the_mix_identical(engine):
     assert np.array_equal(alone, mix[30:30 + len(popa)])
 
 
+def test_gradient_alone_and_in_a_large_batch_identical(engine):
+    """A large batch's register-adjoint items cover several 4096-point parts
+    and a small batch's one part each; every part is summed on its own, so a
+    program's MSE and gradient are the same bits either way."""
+    ds = engine.upload(W.lorentz_dataset(100_000, seed=2))
+    pop = W.lorentz_population(2048, seed=12)
+    mse_all, g_all = engine.compute_mse_grad_batch(pop, ds)
+    mse_sub, g_sub = engine.compute_mse_grad_batch(pop[100:116], ds)
+    assert same_bits(mse_sub, mse_all[100:116])
+    assert same_bits(g_sub, g_all[100:116])
+
+
 def test_multi_dataset_batch(engine):
     sizes = [400, 1000, 2500, 7000]
     dss = [W.inverse_dataset(n, seed=60 + i) for i, n in enumerate(sizes)]
