@@ -28,7 +28,9 @@ image) on all host cores, on bounded samples of the same workload.
 `--case` runs one fixed evaluation case for profilers instead (`--workload`,
 `--programs`, `--points`, `--kernel register|plain|adjoint|slot-adjoint`,
 `--runs`, `--points-per-thread`, `--programs-per-warp`), a small case for an
-ncu capture.
+ncu capture.  Given to the benchmark itself, `--points-per-thread` and
+`--programs-per-warp` fix the register kernel's shape in place of the
+autotuner (whose timings under ncu are not the bench's).
 """
 from __future__ import annotations
 
