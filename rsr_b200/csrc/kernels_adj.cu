@@ -663,17 +663,29 @@ __global__ void __launch_bounds__(adj_warps<PROF, P>() * 32, 1) adj_eval_kernel(
             }
             // the warp's sums of this part in f64, then a fresh start for the next
             {
+                // sums 0 (squared errors) .. np (gradient), four warp sums
+                // at a time, each as warp_sum adds
                 double *wred = red + ((size_t)part * nw + warp) * (1 + kAdjParams);
                 Kahan ks;
                 ks.s = kahan[lane];
                 ks.c = kahan[32 + lane];
-                const double s = warp_sum(ks.value());
-                if (lane == 0) wred[0] = s;
-                for (uint32_t k = 0; k < np; ++k) {
-                    const double gk = warp_sum((double)io.gacc[k * 32]);
-                    if (lane == 0) wred[1 + k] = gk;
-                    io.gacc[k * 32] = 0.0f;
+                for (uint32_t i0 = 0; i0 <= np; i0 += 4) {
+                    double v[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const uint32_t i = i0 + j;
+                        v[j] = i == 0 ? (double)ks.value() : i <= np ? (double)io.gacc[(i - 1) * 32] : 0.0;
+                    }
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) v[j] += __shfl_xor_sync(0xffffffffu, v[j], o);
+                    if (lane == 0)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j)
+                            if (i0 + j <= np) wred[i0 + j] = v[j];
                 }
+                for (uint32_t k = 0; k < np; ++k) io.gacc[k * 32] = 0.0f;
                 kahan[lane] = 0.0f;
                 kahan[32 + lane] = 0.0f;
             }
